@@ -1,0 +1,221 @@
+"""Generate the golden fixtures in tests/golden/*.npz from the reference itself.
+
+Runs the unmodified reference package (dakling/jax-spectral-dns, read from
+/root/reference) in FP64 on NumPy through the stand-in `jax` in
+tests/golden/jax_shim, on seeded inputs built with the product's own seed
+helper (jax_spectral_dns/seeds.py, loaded by file path so the reference's
+package of the same name stays the one imported). Only this script reads
+/root/reference; the fixtures it writes are small .npz files that travel with
+the repository.
+
+    python tests/golden/make_golden.py [case ...]
+
+Each fixture stores the seeded input, the reference outputs after the listed
+step counts, the energy history and the run parameters.
+"""
+from __future__ import annotations
+
+import importlib.util
+import math
+import os
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REFERENCE = os.environ.get("JSD_REFERENCE", "/root/reference")
+
+sys.path.insert(0, os.path.join(HERE, "jax_shim"))
+sys.path.insert(1, REFERENCE)
+
+_spec = importlib.util.spec_from_file_location(
+    "jsd_seeds", os.path.join(REPO, "jax-spectral-dns_b200", "jax_spectral_dns", "seeds.py"))
+seeds = importlib.util.module_from_spec(_spec)
+_spec.loader.exec_module(seeds)
+
+# the reference writes ./fields and ./plots; keep that out of the repository
+os.chdir(tempfile.mkdtemp(prefix="jsd_golden_"))
+
+import jax.numpy as jnp  # noqa: E402  (the shim)
+from jax_spectral_dns.equation import Equation  # noqa: E402
+from jax_spectral_dns.domain import PhysicalDomain  # noqa: E402
+from jax_spectral_dns.field import FourierField, VectorField  # noqa: E402
+from jax_spectral_dns.navier_stokes import NavierStokesVelVort  # noqa: E402
+from jax_spectral_dns.navier_stokes_perturbation import NavierStokesVelVortPerturbation  # noqa: E402
+from jax_spectral_dns.navier_stokes_perturbation_dual import NavierStokesVelVortPerturbationDual  # noqa: E402
+
+Equation.initialize()
+Equation.verbosity_level = 0
+
+
+def _domain(shape, lx, lz):
+    return PhysicalDomain.create(shape, (True, False, True), scale_factors=(lx, 1.0, lz), aliasing=3 / 2)
+
+
+def _vf(dom, data):
+    return VectorField.FromData(FourierField, dom, jnp.asarray(data), name="velocity_hat")
+
+
+def _energy(dom, data):
+    return float(_vf(dom, data).no_hat().energy())
+
+
+def _run_forward(nse, dom, u0, dpdx0, n_steps, keep, energy_every=1):
+    """Step the reference's perform_time_step by hand, recording states and E."""
+    u = jnp.asarray(u0)
+    dpdx = dpdx0
+    states = {}
+    dpdxs = [dpdx]
+    energies = [_energy(dom, u)]
+    for t in range(n_steps):
+        u, dpdx = nse.perform_time_step(u, dpdx, t)
+        dpdxs.append(float(dpdx))
+        if (t + 1) % energy_every == 0:
+            energies.append(_energy(dom, u))
+        if (t + 1) in keep:
+            states[t + 1] = np.asarray(u).copy()
+    return states, np.array(energies), np.array(dpdxs)
+
+
+def _save(name, **arrays):
+    path = os.path.join(HERE, name + ".npz")
+    np.savez_compressed(path, **arrays)
+    print("wrote", path, round(os.path.getsize(path) / 1024), "KiB", flush=True)
+
+
+def case_lin_pert():
+    """Linearised perturbation, pseudo-2D (Nz=4, Lz=2*pi*1e-3), Re=3000, dt=0.01,
+    only kx=+-1, kz=0 populated, E0=1e-6 (the 9x65x5-mode pseudo-2D case)."""
+    shape, lx, lz = (8, 65, 4), 2 * math.pi, 2 * math.pi * 1e-3
+    re, dt, n = 3000.0, 0.01, 100
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (1, 0), 1e-6, seed=0)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=True)
+    nse.activate_jit()
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={1, 10, 100})
+    _save("lin_pert_9x65x5", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt,
+          u0=u0, u1=states[1], u10=states[10], u100=states[100], energy=en)
+
+
+def case_lin_pert_gain():
+    """Same pseudo-2D linearised case run to T=15 (1500 steps): energy every
+    10 steps and the final gain."""
+    shape, lx, lz = (8, 65, 4), 2 * math.pi, 2 * math.pi * 1e-3
+    re, dt, n = 3000.0, 0.01, 1500
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (1, 0), 1e-6, seed=0)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=True)
+    nse.activate_jit()
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={n}, energy_every=10)
+    _save("lin_pert_gain_9x65x5", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt,
+          n_steps=n, energy_every10=en, u_final=states[n])
+
+
+def case_nonlin_pert():
+    """Nonlinear perturbation about Poiseuille flow, Re=5000, Lx=2pi, Lz=pi,
+    9x33x9 modes with every mode populated (exercises the max-mode handling),
+    E0=1e-3, dt=0.005."""
+    shape, lx, lz = (8, 33, 8), 2 * math.pi, math.pi
+    re, dt, n = 5000.0, 0.005, 20
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (4, 4), 1e-3, seed=1)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=False)
+    nse.activate_jit()
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={1, 20})
+    _save("nonlin_pert_9x33x9", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt,
+          u0=u0, u1=states[1], u20=states[20], energy=en)
+
+
+def case_nonlin_pert_odd():
+    """Nonlinear perturbation on an uneven box: 7x24x11 modes (even Ny),
+    Re=2000, Lx=3, Lz=5, E0=1e-2, dt=0.01."""
+    shape, lx, lz = (6, 24, 10), 3.0, 5.0
+    re, dt, n = 2000.0, 0.01, 5
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (3, 5), 1e-2, seed=2)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=False)
+    nse.activate_jit()
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={1, 5})
+    _save("nonlin_pert_7x24x11", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt,
+          u0=u0, u1=states[1], u5=states[5], energy=en)
+
+
+def case_ns_cmf():
+    """Full Navier-Stokes, constant mass flux, Re_tau=180, box 4pi x 2 x 4pi/3,
+    9x33x9 modes, Reichardt mean profile + 10% perturbation, dt=0.002."""
+    shape, lx, lz = (8, 33, 8), 4 * math.pi, 4 * math.pi / 3
+    re_tau, dt, n = 180.0, 0.002, 10
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.turbulent_channel_hat(shape, (lx, lz), re_tau, (4, 4), seed=3)
+    nse = NavierStokesVelVort(_vf(dom, u0), Re_tau=re_tau, dt=dt, end_time=n * dt, constant_mass_flux=True)
+    nse.activate_jit()
+    dpdx0 = float(nse.dPdx)
+    flow_rate = float(nse.flow_rate)
+    states, en, dps = _run_forward(nse, dom, u0, dpdx0, n, keep={1, 10})
+    _save("ns_cmf_9x33x9", shape=np.array(shape), lengths=np.array([lx, lz]), re_tau=re_tau, dt=dt,
+          u0=u0, u1=states[1], u10=states[10], energy=en, dpdx=dps, flow_rate=flow_rate)
+
+
+def case_ns_cpg():
+    """Full Navier-Stokes with a constant pressure gradient dPdx=-1,
+    Re_tau=180, same box and seed family as the constant-mass-flux case."""
+    shape, lx, lz = (8, 33, 8), 4 * math.pi, 4 * math.pi / 3
+    re_tau, dt, n = 180.0, 0.002, 10
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.turbulent_channel_hat(shape, (lx, lz), re_tau, (4, 4), seed=4)
+    nse = NavierStokesVelVort(_vf(dom, u0), Re_tau=re_tau, dt=dt, end_time=n * dt, constant_mass_flux=False)
+    nse.activate_jit()
+    states, en, dps = _run_forward(nse, dom, u0, -1.0, n, keep={1, 10})
+    _save("ns_cpg_9x33x9", shape=np.array(shape), lengths=np.array([lx, lz]), re_tau=re_tau, dt=dt,
+          u0=u0, u1=states[1], u10=states[10], energy=en, dpdx=dps)
+
+
+def _dual_case(name, shape, lx, lz, re, dt, n, kmax, e0, seed, linearise):
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), kmax, e0, seed=seed)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=linearise)
+    nse.activate_jit()
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse, checkpointing=False)
+    t0 = time.time()
+    grad = np.asarray(dual.get_grad()).copy()
+    gain = float(dual.gain)
+    uT = np.asarray(nse.get_latest_field("velocity_hat").get_data()).copy()
+    print(name, "dual seconds", round(time.time() - t0, 1), "gain", gain, flush=True)
+    _save(name, shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n,
+          u0=u0, uT=uT, grad=grad, gain=gain)
+
+
+def case_dual_lin():
+    """Reference continuous-adjoint gradient, linearised, 5x33x5 pseudo-2D,
+    Re=3000, T=0.2 (20 steps)."""
+    _dual_case("dual_lin_5x33x5", (4, 33, 4), 2 * math.pi, 2 * math.pi * 1e-3, 3000.0, 0.01, 20,
+               (1, 0), 1e-6, 5, True)
+
+
+def case_dual_nonlin():
+    """Reference continuous-adjoint gradient, nonlinear, 9x33x9, Re=3000,
+    Lx=2pi, Lz=pi, E0=1e-4, T=0.05 (5 steps)."""
+    _dual_case("dual_nonlin_9x33x9", (8, 33, 8), 2 * math.pi, math.pi, 3000.0, 0.01, 5,
+               (4, 4), 1e-4, 6, False)
+
+
+CASES = {
+    "lin_pert": case_lin_pert,
+    "lin_pert_gain": case_lin_pert_gain,
+    "nonlin_pert": case_nonlin_pert,
+    "nonlin_pert_odd": case_nonlin_pert_odd,
+    "ns_cmf": case_ns_cmf,
+    "ns_cpg": case_ns_cpg,
+    "dual_lin": case_dual_lin,
+    "dual_nonlin": case_dual_nonlin,
+}
+
+if __name__ == "__main__":
+    names = sys.argv[1:] or list(CASES)
+    for nm in names:
+        t = time.time()
+        CASES[nm]()
+        print(nm, "done in", round(time.time() - t, 1), "s", flush=True)
