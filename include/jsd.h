@@ -1,0 +1,152 @@
+/*
+ * jsd.h -- C ABI of the B200 velocity-vorticity channel-flow step.
+ *
+ * The reference (dakling/jax-spectral-dns) is pure Python/JAX and has no FFI;
+ * this ABI is the boundary under its equation classes. Each entry point names
+ * the reference call it replaces (paths inside the reference package).
+ *
+ * Conventions
+ *  - All arrays passed to the step functions are DEVICE pointers owned by the
+ *    caller. A state is 3 spectral fields (u, v, w), each Ny x Mx x Mz complex
+ *    doubles stored as interleaved (re, im), plane by plane:
+ *        element (c, y, ix, iz) at ((c * Ny + y) * Mx + ix) * Mz + iz
+ *    kx, kz in FFT order [0..K, -K..-1]; y index 0 is y = +1. Coefficients use
+ *    the reference normalisation: ortho FFT on the reference's physical grid
+ *    (Px_ref x Pz_ref) divided by s = Lx Lz / (4 pi^2).
+ *  - Host pointers in jsd_desc are copied at plan creation.
+ *  - Every function returns 0 on success or a negative JSD_ERR_* code; the
+ *    message of the last error on the calling thread is jsd_last_error().
+ *  - A plan owns its device workspace and launches on the stream passed to
+ *    each call. Plans are not thread-safe; distinct plans may run concurrently.
+ */
+#ifndef JSD_H
+#define JSD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JSD_ABI_VERSION 1
+
+enum jsd_status {
+  JSD_OK = 0,
+  JSD_ERR_ARG = -1,      /* invalid argument or unsupported configuration */
+  JSD_ERR_CUDA = -2,     /* CUDA runtime error (message has the detail) */
+  JSD_ERR_NOMEM = -3,    /* device allocation failed */
+  JSD_ERR_STATE = -4     /* call out of order (e.g. dual step without history) */
+};
+
+enum jsd_kind {
+  JSD_KIND_NS = 0,            /* NavierStokesVelVort            (navier_stokes.py:310) */
+  JSD_KIND_PERTURBATION = 1,  /* NavierStokesVelVortPerturbation (navier_stokes_perturbation.py:341) */
+  JSD_KIND_DUAL = 2           /* NavierStokesVelVortPerturbationDual (navier_stokes_perturbation_dual.py:376) */
+};
+
+/* Discretisation and operator tables. The tables are the FP64 quantities the
+ * host builds once per box (Chebyshev matrix D, the eigen-decomposition
+ * D2_int = V diag(lam) V^-1 of the interior second-derivative matrix, and the
+ * reference's (0,0) mean-flow matrices); see jax_spectral_dns/_ops.py. */
+typedef struct jsd_desc {
+  int mx, ny, mz;          /* Fourier modes in x and z (odd), Chebyshev points */
+  int px_ref, pz_ref;      /* reference physical grid (normalisation, Domain.create, domain.py:201-317) */
+  int px_fft, pz_fft;      /* device FFT lengths, >= 3*(m/2)+1 with factors 2,3,5,7 */
+  double lx, lz;           /* box lengths */
+  int kind;                /* enum jsd_kind */
+  int linearise;           /* drop the quadratic term (perturbation / dual) */
+  int constant_mass_flux;  /* navier_stokes.py:1205-1214 */
+  double re_tau;           /* Reynolds number of the implicit operators */
+  double dt;               /* time step of the implicit operators */
+  double dt_explicit;      /* time step multiplying the explicit terms (-dt for the dual) */
+  double flow_rate_target; /* Q0 for the constant-mass-flux correction */
+  const double* base_u;    /* [ny] base profile U(y) (perturbation / dual) or NULL */
+  const double* base_du;   /* [ny] dU/dy or NULL */
+  const double* D;         /* [ny*ny] Chebyshev first-derivative matrix, row-major */
+  const double* V;         /* [(ny-2)^2] eigenvectors of D2[1:-1,1:-1] (columns) */
+  const double* Vinv;      /* [(ny-2)^2] */
+  const double* lam;       /* [ny-2] eigenvalues */
+  const double* sgn;       /* [ny-2] parity of each eigenvector under y -> -y (+1/-1) */
+  const double* c0;        /* [ny-2] Vinv @ D2[1:-1, 0] */
+  const double* cN;        /* [ny-2] Vinv @ D2[1:-1, -1] */
+  const double* w0;        /* [ny-2] D[0, 1:-1] @ V */
+  const double* wN;        /* [ny-2] D[-1, 1:-1] @ V */
+  const double* y_weights; /* [ny] Chebyshev integration weights (field.py:2618-2650) */
+  const double* rhs_ns;    /* [3*(2ny)^2] (0,0) explicit matrices per RK stage (navier_stokes.py:1000-1022) */
+  const double* lhs_inv_ns;/* [3*(2ny)^2] (0,0) implicit inverses per RK stage */
+} jsd_desc;
+
+typedef struct jsd_plan jsd_plan;
+
+/* Builds the device operators, FFT tables and workspace.
+ * Replaces NavierStokesVelVort.assemble_matrices / prepare_assemble_rk_matrices
+ * (navier_stokes.py:437-502, 920-1022) and FourierDomain.assemble_poisson_matrix
+ * (domain.py:857-889). */
+int jsd_plan_create(const jsd_desc* desc, jsd_plan** plan);
+
+int jsd_plan_destroy(jsd_plan* plan);
+
+/* Advances `state` in place by n_steps RK3/Crank-Nicolson steps on `stream`.
+ * dpdx is a device double (mean pressure gradient), read and, with constant
+ * mass flux, updated. first_step is the global index of the first step (used
+ * by the dual to select the forward state).
+ * Replaces NavierStokesVelVort.perform_time_step / perform_runge_kutta_step
+ * (navier_stokes.py:1778-1813, 1219-1775). */
+int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* stream);
+
+/* Dual equations: register the forward trajectory u_0 .. u_{n_states-1}
+ * (device, n_states consecutive states). Dual step t uses u_{n_states-1-t}
+ * for all three stages (navier_stokes_perturbation_dual.py:591-602). */
+int jsd_set_history(jsd_plan* plan, const void* states, int n_states);
+
+/* Constant-mass-flux correction of the streamwise field: Q is the flow rate of
+ * state's u, u <- hat(no_hat(u) - (Q - Q0)/2) (walls included) and, when dpdx
+ * is not NULL, dpdx += (Q - Q0)/dt_explicit.
+ * Replaces update_pressure_gradient + update_velocity_field_data
+ * (navier_stokes.py:724-805; perturbation variant navier_stokes_perturbation.py:420-466). */
+int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* stream);
+
+/* Kinetic energy E = 1/(2V) int |u|^2 / 2 of a state, written to the device
+ * double `out`. Replaces VectorField.no_hat().energy() (field.py:607-611,
+ * 1468-1474). */
+int jsd_energy(jsd_plan* plan, const void* state, double* out, void* stream);
+
+/* Flow rate Q = int u(x=0, y, z=0) dy of the streamwise component, written to
+ * the device double `out`. Replaces NavierStokesVelVort.get_flow_rate
+ * (navier_stokes.py:709-722). */
+int jsd_flow_rate(jsd_plan* plan, const void* u_field, double* out, void* stream);
+
+/* Nonlinear-term hook: h_v, h_g (spectral, Ny x Mx x Mz each) of `state` at
+ * forward step t. Replaces nonlinear_update_fn's (h_v, h_g) outputs
+ * (navier_stokes.py:324-332, 48-73). */
+int jsd_nonlinear_terms(jsd_plan* plan, const void* state, int time_step, void* h_v, void* h_g, void* stream);
+
+/* Bytes of device workspace the plan holds. */
+size_t jsd_workspace_bytes(const jsd_plan* plan);
+
+/* Number of kernel launches one call of jsd_step issues per time step. */
+int jsd_launches_per_step(const jsd_plan* plan);
+
+/* Optional timing of kernel classes with CUDA events (no effect unless
+ * enabled). jsd_profile_read returns and clears, for one class, the summed
+ * device time (ms), the number of launches and the summed algorithmic work
+ * (FLOPs for JSD_PROF_GEMM, bytes for the others). No reference counterpart. */
+enum jsd_prof_class {
+  JSD_PROF_GEMM = 0,    /* FP64 y-contractions (DMMA) */
+  JSD_PROF_ZINV = 1,    /* inverse z transforms */
+  JSD_PROF_XMID = 2,    /* x transforms + products */
+  JSD_PROF_ZFWD = 3,    /* forward z transforms + truncation */
+  JSD_PROF_EIGEN = 4,   /* eigenbasis update + influence correction */
+  JSD_PROF_LINEAR = 5   /* linearised terms */
+};
+int jsd_profile_enable(jsd_plan* plan, int enable);
+int jsd_profile_read(jsd_plan* plan, int kernel_class, double* total_ms, long long* launches, double* work);
+
+const char* jsd_last_error(void);
+int jsd_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JSD_H */

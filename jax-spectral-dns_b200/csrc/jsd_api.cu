@@ -1,0 +1,678 @@
+// Plan management and the C ABI (include/jsd.h) of the velocity-vorticity step.
+//
+// One RK3/Crank-Nicolson step = 3 stages; each stage launches:
+//   1  k_dgemm          D applied to the fields the nonlinear term needs
+//   2  k_zinv + k_xmid + k_zfwd   (full / nonlinear equations), or
+//      k_linear_terms            (linearised equations)
+//   3  k_omega          omega_y of the current state
+//   4  k_dgemm          eigenbasis transforms (V^-1 D q, V^-1 [H1, h_g, v, omega])
+//   5  k_eigen_update   diagonal solves + influence-matrix correction
+//   6  k_mean_flow      (0,0) mean-flow block system
+//   7  k_dgemm          back-transform: v, dv/dy, omega_y
+//   8  k_reconstruct    u, w from continuity, walls
+// and, with constant mass flux, 3 more launches and one copy per step.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/jsd.h"
+#include "jsd_common.cuh"
+#include "jsd_fft.cuh"
+#include "jsd_gemm.cuh"
+#include "jsd_spectral.cuh"
+
+using namespace jsd;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define JSD_CUDA(call)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(JSD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));        \
+  } while (0)
+
+#define JSD_LAUNCHED(name)                                                                  \
+  do {                                                                                      \
+    cudaError_t e_ = cudaGetLastError();                                                    \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(JSD_ERR_CUDA, std::string("launch ") + name + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+constexpr double kAlpha[3] = {29.0 / 96.0, -3.0 / 40.0, 1.0 / 6.0};
+constexpr double kBeta[3] = {37.0 / 160.0, 5.0 / 24.0, 1.0 / 6.0};
+constexpr double kGamma[3] = {8.0 / 15.0, 5.0 / 12.0, 3.0 / 4.0};
+constexpr double kXi[3] = {0.0, -17.0 / 60.0, -5.0 / 12.0};
+
+constexpr int kXmidZB = 4;
+
+bool smooth_radix(int n) {
+  for (int p : {2, 3, 5, 7})
+    while (n % p == 0) n /= p;
+  return n == 1;
+}
+
+int choose_fft_size(int m) {
+  int n = 3 * (m / 2) + 1;
+  while (!smooth_radix(n)) ++n;
+  return n;
+}
+
+// Factor n into supported radices and build the forward twiddle table.
+bool build_fft(int n, FftDesc& d, std::vector<double2>& tw) {
+  std::vector<int> rs;
+  int m = n;
+  while (m % 8 == 0) { rs.push_back(8); m /= 8; }
+  if (m % 4 == 0) { rs.push_back(4); m /= 4; }
+  if (m % 2 == 0) { rs.push_back(2); m /= 2; }
+  for (int p : {7, 5, 3})
+    while (m % p == 0) { rs.push_back(p); m /= p; }
+  if (m != 1 || (int)rs.size() > kMaxFftPasses) return false;
+  d.n = n;
+  d.passes = (int)rs.size();
+  tw.clear();
+  int ls = 1;
+  for (int p = 0; p < d.passes; ++p) {
+    const int r = rs[p];
+    d.radix[p] = r;
+    d.ls[p] = ls;
+    d.twoff[p] = (int)tw.size();
+    for (int k = 0; k < ls; ++k)
+      for (int t = 1; t < r; ++t) {
+        const long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)(t * k) /
+                                (long double)(ls * r);
+        tw.push_back(make_double2((double)cosl(ang), (double)sinl(ang)));
+      }
+    ls *= r;
+  }
+  if ((int)tw.size() != n - 1) return false;
+  if (tw.empty()) tw.push_back(make_double2(1.0, 0.0));
+  return true;
+}
+
+}  // namespace
+
+struct jsd_plan {
+  jsd_desc desc;
+  Geo g;
+  FftDesc fx, fz;
+  int lda;             // padded leading dimension of the operator matrices
+  size_t fdoubles;     // doubles per spectral field (2 ny nk)
+  size_t edoubles;     // doubles per eigen-space field (2 (ny-2) nk)
+  double dpdx_scale;
+  // device operator tables
+  double2 *twx = nullptr, *twz = nullptr;
+  double *Dm = nullptr, *VinvD = nullptr, *Vinv = nullptr, *Vfull = nullptr, *DVfull = nullptr;
+  double *lam = nullptr, *sgn = nullptr, *c0 = nullptr, *cN = nullptr, *w0 = nullptr, *wN = nullptr;
+  double *yw = nullptr, *rhs_ns = nullptr, *lhs_inv_ns = nullptr, *ub = nullptr, *dub = nullptr;
+  // workspace
+  double2 *Dfld = nullptr;     // 3 fields: D u, D v, D w
+  double2 *inter = nullptr;    // 9 z-transformed lines per (y, kx >= 0)
+  double2 *out3 = nullptr;     // 3 x-transformed products per (y, kx >= 0)
+  double2 *q = nullptr, *H1 = nullptr, *hg = nullptr, *om = nullptr, *dvn = nullptr, *tmp = nullptr;
+  double2 *conv = nullptr;     // 3 stages x 2 ny
+  double2 *uw00 = nullptr;     // 2 ny
+  double *X1 = nullptr, *T = nullptr, *hv_old = nullptr, *hg_old = nullptr, *vnt = nullptr, *omnt = nullptr;
+  double *partial = nullptr, *scal = nullptr;
+  size_t ws_bytes = 0;
+  std::vector<void*> allocs;
+  const double2* history = nullptr;
+  int n_history = 0;
+  // optional per-kernel-class timing with CUDA events (jsd_profile_*)
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_free;
+  struct Rec { int cls; cudaEvent_t a, b; double work; };
+  std::vector<Rec> recs;
+};
+
+namespace {
+
+int dev_alloc(jsd_plan* p, void** ptr, size_t bytes) {
+  cudaError_t e = cudaMalloc(ptr, bytes);
+  if (e != cudaSuccess) return fail(JSD_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  p->allocs.push_back(*ptr);
+  p->ws_bytes += bytes;
+  return 0;
+}
+
+template <typename T>
+int upload(jsd_plan* p, T** dst, const T* src, size_t count) {
+  int rc = dev_alloc(p, (void**)dst, count * sizeof(T));
+  if (rc) return rc;
+  JSD_CUDA(cudaMemcpy(*dst, src, count * sizeof(T), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// rows x cols host matrix (row-major) -> device with leading dimension lda, zero padded
+int upload_padded(jsd_plan* p, double** dst, const double* src, int rows, int cols, int lda) {
+  std::vector<double> buf((size_t)rows * lda, 0.0);
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < cols; ++c) buf[(size_t)r * lda + c] = src[(size_t)r * cols + c];
+  return upload(p, dst, buf.data(), buf.size());
+}
+
+cudaEvent_t take_event(jsd_plan* p) {
+  if (!p->ev_free.empty()) {
+    cudaEvent_t e = p->ev_free.back();
+    p->ev_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+// Brackets one launch of kernel class `cls` with events when profiling.
+struct ProfScope {
+  jsd_plan* p;
+  int cls;
+  double work;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  ProfScope(jsd_plan* p_, int cls_, double work_, cudaStream_t s_) : p(p_), cls(cls_), work(work_), s(s_) {
+    if (p->profiling) {
+      a = take_event(p);
+      cudaEventRecord(a, s);
+    }
+  }
+  ~ProfScope() {
+    if (p->profiling) {
+      cudaEvent_t b = take_event(p);
+      cudaEventRecord(b, s);
+      p->recs.push_back({cls, a, b, work});
+    }
+  }
+};
+
+double gemm_flops(const GemmBatch& b) {
+  double f = 0;
+  for (int i = 0; i < b.count; ++i) f += 2.0 * b.e[i].M * (double)b.e[i].K * b.N;
+  return f;
+}
+
+int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, cudaStream_t s) {
+  ProfScope ps(const_cast<jsd_plan*>(p), JSD_PROF_GEMM, gemm_flops(b), s);
+  // pick the row tile that wastes least
+  const int t48 = (max_m + 47) / 48 * 48, t64 = (max_m + 63) / 64 * 64;
+  const dim3 block(128);
+  if (t48 < t64) {
+    const dim3 grid((b.N + 63) / 64, (max_m + 47) / 48, b.count);
+    k_dgemm<48><<<grid, block, GemmSmem<48>::BYTES, s>>>(b);
+  } else {
+    const dim3 grid((b.N + 63) / 64, (max_m + 63) / 64, b.count);
+    k_dgemm<64><<<grid, block, GemmSmem<64>::BYTES, s>>>(b);
+  }
+  JSD_LAUNCHED("k_dgemm");
+  return 0;
+}
+
+GemmBatch gemm_batch(const jsd_plan* p) {
+  GemmBatch b;
+  memset(&b, 0, sizeof(b));
+  b.N = 2 * p->g.nk;
+  b.lda = p->lda;
+  b.ldb = b.N;
+  b.ldc = b.N;
+  return b;
+}
+
+void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M, int K, double alpha = 1.0) {
+  GemmEntry& e = b.e[b.count++];
+  e.A = A;
+  e.B = B;
+  e.C = C;
+  e.M = M;
+  e.K = K;
+  e.alpha = alpha;
+}
+
+int grid_for(size_t total, int block) {
+  size_t g = (total + block - 1) / block;
+  if (g > 148 * 32) g = 148 * 32;
+  return (int)(g < 1 ? 1 : g);
+}
+
+// h_v = -D q - k^2 H1 (only for the nonlinear-term hook)
+__global__ void k_assemble_hv(Geo g, const double2* __restrict__ dq, const double2* __restrict__ h1,
+                              double2* __restrict__ hv) {
+  const size_t total = (size_t)g.ny * g.nk;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(t % g.nk);
+    const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+    const double kx = kx_of(g, ix), kz = kz_of(g, iz);
+    const double k2 = kx * kx + kz * kz;
+    hv[t] = make_double2(-dq[t].x - k2 * h1[t].x, -dq[t].y - k2 * h1[t].y);
+  }
+}
+
+// nonlinear terms of `state` into p->q, p->H1, p->hg and conv00 slot `stage`
+int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage, cudaStream_t s) {
+  const Geo& g = p->g;
+  const size_t fs = (size_t)g.ny * g.nk;
+  const double2* u = state;
+  const double2* v = state + fs;
+  const double2* w = state + 2 * fs;
+  const int ny = g.ny;
+  double2* conv = p->conv + (size_t)stage * 2 * ny;
+  const bool linear = p->desc.linearise && p->desc.kind != JSD_KIND_NS;
+  if (p->desc.kind == JSD_KIND_DUAL && !linear) {
+    (void)uhist;
+    return fail(JSD_ERR_ARG, "the nonlinear dual step is not available in this build");
+  }
+  if (linear) {
+    GemmBatch b = gemm_batch(p);
+    add_entry(b, p->Dm, (const double*)v, (double*)(p->Dfld + fs), ny, ny);
+    int rc = launch_gemm(p, b, ny, s);
+    if (rc) return rc;
+    const int blk = 256;
+    ProfScope ps(p, JSD_PROF_LINEAR, sizeof(double2) * 7.0 * fs, s);
+    if (p->desc.kind == JSD_KIND_PERTURBATION)
+      k_linear_terms<kPerturbation><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, p->Dfld + fs, p->ub, p->dub,
+                                                                      p->q, p->H1, p->hg, conv);
+    else
+      k_linear_terms<kDual><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, p->Dfld + fs, p->ub, p->dub, p->q,
+                                                              p->H1, p->hg, conv);
+    JSD_LAUNCHED("k_linear_terms");
+    return 0;
+  }
+  GemmBatch b = gemm_batch(p);
+  for (int c = 0; c < 3; ++c) add_entry(b, p->Dm, (const double*)(state + c * fs), (double*)(p->Dfld + c * fs), ny, ny);
+  int rc = launch_gemm(p, b, ny, s);
+  if (rc) return rc;
+  const int K1 = g.kx_max + 1;
+  {
+    const size_t sm = sizeof(double2) * ((size_t)g.pz + 2 * kZinvLines * (size_t)g.pz);
+    const double bytes = sizeof(double2) * (6.0 * fs + (double)kZinvLines * ny * K1 * g.pz);
+    ProfScope ps(p, JSD_PROF_ZINV, bytes, s);
+    k_zinv<<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, p->twz, u, v, w, p->Dfld, p->Dfld + fs, p->Dfld + 2 * fs,
+                                         p->inter);
+    JSD_LAUNCHED("k_zinv");
+  }
+  {
+    const size_t sm = XmidSmem<kXmidZB>::bytes(g);
+    ProfScope ps(p, JSD_PROF_XMID, sizeof(double2) * (double)(kZinvLines + 3) * ny * K1 * g.pz, s);
+    const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
+    const bool pert = p->desc.kind == JSD_KIND_PERTURBATION;
+    k_xmid<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), 256, sm, s>>>(
+        g, p->fx, p->twx, p->inter, p->out3, pert ? p->ub : nullptr, pert ? p->dub : nullptr, lam);
+    JSD_LAUNCHED("k_xmid");
+  }
+  {
+    const size_t sm = sizeof(double2) * 7 * (size_t)g.pz;
+    ProfScope ps(p, JSD_PROF_ZFWD, sizeof(double2) * (3.0 * ny * K1 * g.pz + 3.0 * fs), s);
+    k_zfwd<<<dim3(K1, ny), 128, sm, s>>>(g, p->fz, p->twz, p->out3, p->q, p->H1, p->hg, conv);
+    JSD_LAUNCHED("k_zfwd");
+  }
+  return 0;
+}
+
+int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cudaStream_t s) {
+  const Geo& g = p->g;
+  const size_t fs = (size_t)g.ny * g.nk;
+  const int ny = g.ny, ni = g.ny - 2;
+  double2* u = state;
+  double2* v = state + fs;
+  double2* w = state + 2 * fs;
+  const double2* uhist = nullptr;
+  if (p->desc.kind == JSD_KIND_DUAL && !p->desc.linearise) {
+    if (!p->history) return fail(JSD_ERR_STATE, "dual step needs jsd_set_history first");
+    const int idx = p->n_history - 1 - time_step;
+    if (idx < 0) return fail(JSD_ERR_ARG, "dual time step beyond the registered forward history");
+    uhist = p->history + (size_t)idx * 3 * fs;
+  }
+  int rc = nonlinear(p, state, uhist, st, s);
+  if (rc) return rc;
+  const int blk = 256;
+  k_omega<<<grid_for(fs, blk), blk, 0, s>>>(g, u, w, p->om);
+  JSD_LAUNCHED("k_omega");
+  // eigenbasis transforms
+  {
+    GemmBatch b = gemm_batch(p);
+    const size_t E = p->edoubles;
+    const size_t rowd = 2 * (size_t)g.nk;  // doubles per y-row
+    add_entry(b, p->VinvD, (const double*)p->q, p->X1, ni, ny);
+    add_entry(b, p->Vinv, (const double*)p->H1 + rowd, p->T + 0 * E, ni, ni);
+    add_entry(b, p->Vinv, (const double*)p->hg + rowd, p->T + 1 * E, ni, ni);
+    add_entry(b, p->Vinv, (const double*)v + rowd, p->T + 2 * E, ni, ni);
+    add_entry(b, p->Vinv, (const double*)p->om + rowd, p->T + 3 * E, ni, ni);
+    rc = launch_gemm(p, b, ni, s);
+    if (rc) return rc;
+  }
+  {
+    EigTables t{p->lam, p->c0, p->cN, p->sgn, p->w0, p->wN};
+    StageCoef sc{kAlpha[st], kBeta[st], kGamma[st], kXi[st], p->desc.dt, p->desc.dt_explicit, p->desc.re_tau,
+                 st == 0 ? 1 : 0};
+    const int N = 2 * g.nk;
+    const size_t E = p->edoubles;
+    // reads X1, 4 transformed fields, 2 old terms; writes 2 old terms, v~ twice, om~
+    ProfScope ps(p, JSD_PROF_EIGEN, sizeof(double) * 13.0 * (double)E, s);
+    k_eigen_update<<<(N + 127) / 128, 128, 0, s>>>(g, t, sc, p->X1, p->T, p->T + E, p->T + 2 * E, p->T + 3 * E,
+                                                   (const double*)v, p->hv_old, p->hg_old, p->vnt, p->omnt);
+    JSD_LAUNCHED("k_eigen_update");
+  }
+  {
+    const size_t n2 = 2 * (size_t)ny;
+    const double* rns = p->rhs_ns + (size_t)st * n2 * n2;
+    const double* lns = p->lhs_inv_ns + (size_t)st * n2 * n2;
+    const double2* conv = p->conv + (size_t)st * 2 * ny;
+    const double2* conv_old = st == 0 ? nullptr : p->conv + (size_t)(st - 1) * 2 * ny;
+    const double dte = p->desc.dt_explicit;
+    k_mean_flow<<<1, 256, sizeof(double2) * 2 * n2, s>>>(g, rns, lns, u, w, conv, conv_old, dpdx, p->dpdx_scale,
+                                                        dte * kGamma[st], dte * kXi[st], p->uw00);
+    JSD_LAUNCHED("k_mean_flow");
+  }
+  {
+    GemmBatch b = gemm_batch(p);
+    add_entry(b, p->Vfull, p->vnt, (double*)v, ny, ni);
+    add_entry(b, p->DVfull, p->vnt, (double*)p->dvn, ny, ni);
+    add_entry(b, p->Vfull, p->omnt, (double*)p->om, ny, ni);
+    rc = launch_gemm(p, b, ny, s);
+    if (rc) return rc;
+  }
+  k_reconstruct<<<grid_for(fs, blk), blk, 0, s>>>(g, p->dvn, p->om, p->uw00, u, v, w);
+  JSD_LAUNCHED("k_reconstruct");
+  return 0;
+}
+
+int mass_flux(jsd_plan* p, double2* state, double* dpdx, cudaStream_t s) {
+  const Geo& g = p->g;
+  const size_t fs = (size_t)g.ny * g.nk;
+  k_plane_sums<<<g.ny, 256, 0, s>>>(g, state, 1, 1, p->partial);
+  JSD_LAUNCHED("k_plane_sums");
+  k_mass_flux_scalar<<<1, 32, 0, s>>>(g.ny, p->yw, p->partial, g.c_inv, p->desc.flow_rate_target,
+                                      p->desc.dt_explicit, dpdx, p->scal);
+  JSD_LAUNCHED("k_mass_flux_scalar");
+  k_roundtrip_shift<<<grid_for(fs, 256), 256, 0, s>>>(g, state, p->scal, p->tmp);
+  JSD_LAUNCHED("k_roundtrip_shift");
+  JSD_CUDA(cudaMemcpyAsync(state, p->tmp, fs * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  return 0;
+}
+
+int set_smem_limits() {
+  static bool done = false;
+  if (done) return 0;
+  const int big = 200 * 1024;
+  JSD_CUDA(cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_xmid<kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_dgemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<48>::BYTES));
+  JSD_CUDA(cudaFuncSetAttribute(k_dgemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<64>::BYTES));
+  JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  done = true;
+  return 0;
+}
+
+void destroy(jsd_plan* p) {
+  if (!p) return;
+  for (auto& r : p->recs) {
+    cudaEventDestroy(r.a);
+    cudaEventDestroy(r.b);
+  }
+  for (cudaEvent_t e : p->ev_free) cudaEventDestroy(e);
+  for (void* a : p->allocs) cudaFree(a);
+  delete p;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jsd_abi_version(void) { return JSD_ABI_VERSION; }
+
+int jsd_profile_enable(jsd_plan* plan, int enable) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  plan->profiling = enable != 0;
+  return 0;
+}
+
+int jsd_profile_read(jsd_plan* plan, int kernel_class, double* total_ms, long long* launches, double* work) {
+  if (!plan || !total_ms || !launches || !work) return fail(JSD_ERR_ARG, "null argument");
+  double ms = 0, w = 0;
+  long long n = 0;
+  std::vector<jsd_plan::Rec> keep;
+  for (auto& r : plan->recs) {
+    if (r.cls != kernel_class) {
+      keep.push_back(r);
+      continue;
+    }
+    float t = 0;
+    JSD_CUDA(cudaEventSynchronize(r.b));
+    JSD_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    ms += t;
+    w += r.work;
+    ++n;
+    plan->ev_free.push_back(r.a);
+    plan->ev_free.push_back(r.b);
+  }
+  plan->recs.swap(keep);
+  *total_ms = ms;
+  *launches = n;
+  *work = w;
+  return 0;
+}
+
+const char* jsd_last_error(void) { return g_last_error.c_str(); }
+
+size_t jsd_workspace_bytes(const jsd_plan* plan) { return plan ? plan->ws_bytes : 0; }
+
+int jsd_launches_per_step(const jsd_plan* plan) {
+  if (!plan) return 0;
+  const bool linear = plan->desc.linearise && plan->desc.kind != JSD_KIND_NS;
+  const int per_stage = linear ? 8 : 10;
+  return 3 * per_stage + (plan->desc.constant_mass_flux ? 3 : 0);
+}
+
+int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
+  if (!d || !out) return fail(JSD_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (d->mx < 3 || d->mz < 3 || (d->mx % 2) == 0 || (d->mz % 2) == 0)
+    return fail(JSD_ERR_ARG, "mx and mz must be odd and >= 3");
+  if (d->ny < 4) return fail(JSD_ERR_ARG, "ny must be >= 4");
+  if (d->kind < 0 || d->kind > 2) return fail(JSD_ERR_ARG, "unknown equation kind");
+  if (!d->D || !d->V || !d->Vinv || !d->lam || !d->sgn || !d->c0 || !d->cN || !d->w0 || !d->wN ||
+      !d->y_weights || !d->rhs_ns || !d->lhs_inv_ns)
+    return fail(JSD_ERR_ARG, "operator tables missing");
+  if (d->kind != JSD_KIND_NS && (!d->base_u || !d->base_du))
+    return fail(JSD_ERR_ARG, "perturbation and dual equations need the base profile");
+  if (d->re_tau == 0.0 || d->dt == 0.0 || d->dt_explicit == 0.0) return fail(JSD_ERR_ARG, "zero Re or dt");
+  int rc = set_smem_limits();
+  if (rc) return rc;
+
+  jsd_plan* p = new jsd_plan();
+  p->desc = *d;
+  Geo& g = p->g;
+  g.mx = d->mx;
+  g.ny = d->ny;
+  g.mz = d->mz;
+  g.kx_max = d->mx / 2;
+  g.kz_max = d->mz / 2;
+  g.px = d->px_fft > 0 ? d->px_fft : choose_fft_size(d->mx);
+  g.pz = d->pz_fft > 0 ? d->pz_fft : choose_fft_size(d->mz);
+  g.nk = d->mx * d->mz;
+  const double two_pi = 2.0 * M_PI;
+  g.ax = two_pi / d->lx;
+  g.az = two_pi / d->lz;
+  const double s = (d->lx / two_pi) * (d->lz / two_pi);
+  g.c_inv = s / std::sqrt((double)d->px_ref * (double)d->pz_ref);
+  g.c_fwd = std::sqrt((double)d->px_ref * (double)d->pz_ref) / (s * (double)g.px * (double)g.pz);
+  p->dpdx_scale = std::sqrt(((double)d->px_ref * (two_pi / d->lx) * (two_pi / d->lx)) *
+                            ((double)d->pz_ref * (two_pi / d->lz) * (two_pi / d->lz)));
+  if (g.px < 3 * g.kx_max + 1 || g.pz < 3 * g.kz_max + 1) {
+    destroy(p);
+    return fail(JSD_ERR_ARG, "FFT length below 3K+1 would alias the quadratic products");
+  }
+  std::vector<double2> twx, twz;
+  if (!build_fft(g.px, p->fx, twx) || !build_fft(g.pz, p->fz, twz)) {
+    destroy(p);
+    return fail(JSD_ERR_ARG, "FFT length must factor into 2, 3, 5, 7");
+  }
+  const int ny = d->ny, ni = ny - 2;
+  p->lda = (ny + 15) / 16 * 16;
+  p->fdoubles = 2 * (size_t)ny * g.nk;
+  p->edoubles = 2 * (size_t)ni * g.nk;
+  const size_t fs = (size_t)ny * g.nk;
+  const size_t n2 = 2 * (size_t)ny;
+
+  std::vector<double> VinvD((size_t)ni * ny, 0.0), Vfull((size_t)ny * ni, 0.0), DVfull((size_t)ny * ni, 0.0);
+  for (int i = 0; i < ni; ++i)
+    for (int c = 0; c < ny; ++c) {
+      long double acc = 0;
+      for (int j = 0; j < ni; ++j) acc += (long double)d->Vinv[(size_t)i * ni + j] * d->D[(size_t)(j + 1) * ny + c];
+      VinvD[(size_t)i * ny + c] = (double)acc;
+    }
+  for (int r = 0; r < ni; ++r)
+    for (int c = 0; c < ni; ++c) Vfull[(size_t)(r + 1) * ni + c] = d->V[(size_t)r * ni + c];
+  for (int r = 0; r < ny; ++r)
+    for (int c = 0; c < ni; ++c) {
+      long double acc = 0;
+      for (int j = 0; j < ni; ++j) acc += (long double)d->D[(size_t)r * ny + j + 1] * d->V[(size_t)j * ni + c];
+      DVfull[(size_t)r * ni + c] = (double)acc;
+    }
+
+#define JSD_TRY(x)        \
+  do {                    \
+    int rc_ = (x);        \
+    if (rc_) {            \
+      destroy(p);         \
+      return rc_;         \
+    }                     \
+  } while (0)
+
+  JSD_TRY(upload(p, &p->twx, twx.data(), twx.size()));
+  JSD_TRY(upload(p, &p->twz, twz.data(), twz.size()));
+  JSD_TRY(upload_padded(p, &p->Dm, d->D, ny, ny, p->lda));
+  JSD_TRY(upload_padded(p, &p->VinvD, VinvD.data(), ni, ny, p->lda));
+  JSD_TRY(upload_padded(p, &p->Vinv, d->Vinv, ni, ni, p->lda));
+  JSD_TRY(upload_padded(p, &p->Vfull, Vfull.data(), ny, ni, p->lda));
+  JSD_TRY(upload_padded(p, &p->DVfull, DVfull.data(), ny, ni, p->lda));
+  JSD_TRY(upload(p, &p->lam, d->lam, ni));
+  JSD_TRY(upload(p, &p->sgn, d->sgn, ni));
+  JSD_TRY(upload(p, &p->c0, d->c0, ni));
+  JSD_TRY(upload(p, &p->cN, d->cN, ni));
+  JSD_TRY(upload(p, &p->w0, d->w0, ni));
+  JSD_TRY(upload(p, &p->wN, d->wN, ni));
+  JSD_TRY(upload(p, &p->yw, d->y_weights, ny));
+  JSD_TRY(upload(p, &p->rhs_ns, d->rhs_ns, 3 * n2 * n2));
+  JSD_TRY(upload(p, &p->lhs_inv_ns, d->lhs_inv_ns, 3 * n2 * n2));
+  if (d->base_u) JSD_TRY(upload(p, &p->ub, d->base_u, ny));
+  if (d->base_du) JSD_TRY(upload(p, &p->dub, d->base_du, ny));
+
+  const bool linear = d->linearise && d->kind != JSD_KIND_NS;
+  const size_t K1 = g.kx_max + 1;
+  JSD_TRY(dev_alloc(p, (void**)&p->Dfld, 3 * fs * sizeof(double2)));
+  if (!linear) {
+    JSD_TRY(dev_alloc(p, (void**)&p->inter, kZinvLines * (size_t)ny * K1 * g.pz * sizeof(double2)));
+    JSD_TRY(dev_alloc(p, (void**)&p->out3, 3 * (size_t)ny * K1 * g.pz * sizeof(double2)));
+  }
+  for (double2** f : {&p->q, &p->H1, &p->hg, &p->om, &p->dvn, &p->tmp})
+    JSD_TRY(dev_alloc(p, (void**)f, fs * sizeof(double2)));
+  JSD_TRY(dev_alloc(p, (void**)&p->conv, 3 * n2 * sizeof(double2)));
+  JSD_TRY(dev_alloc(p, (void**)&p->uw00, n2 * sizeof(double2)));
+  JSD_TRY(dev_alloc(p, (void**)&p->X1, p->edoubles * sizeof(double)));
+  JSD_TRY(dev_alloc(p, (void**)&p->T, 4 * p->edoubles * sizeof(double)));
+  for (double** f : {&p->hv_old, &p->hg_old, &p->vnt, &p->omnt})
+    JSD_TRY(dev_alloc(p, (void**)f, p->edoubles * sizeof(double)));
+  JSD_TRY(dev_alloc(p, (void**)&p->partial, (size_t)ny * sizeof(double)));
+  JSD_TRY(dev_alloc(p, (void**)&p->scal, 8 * sizeof(double)));
+  // conv entries are only written at (0,0); clear once so every read is defined
+  JSD_CUDA(cudaMemset(p->conv, 0, 3 * n2 * sizeof(double2)));
+#undef JSD_TRY
+  *out = p;
+  return 0;
+}
+
+int jsd_plan_destroy(jsd_plan* plan) {
+  destroy(plan);
+  return 0;
+}
+
+int jsd_set_history(jsd_plan* plan, const void* states, int n_states) {
+  if (!plan || (!states && n_states > 0) || n_states < 0) return fail(JSD_ERR_ARG, "bad history");
+  plan->history = static_cast<const double2*>(states);
+  plan->n_history = n_states;
+  return 0;
+}
+
+int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* stream) {
+  if (!plan || !state || !dpdx || n_steps < 0) return fail(JSD_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double2* st = static_cast<double2*>(state);
+  for (int t = 0; t < n_steps; ++t) {
+    for (int k = 0; k < 3; ++k) {
+      int rc = stage(plan, st, dpdx, k, first_step + t, s);
+      if (rc) return rc;
+    }
+    if (plan->desc.constant_mass_flux) {
+      int rc = mass_flux(plan, st, dpdx, s);
+      if (rc) return rc;
+    }
+  }
+  return 0;
+}
+
+int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* stream) {
+  if (!plan || !state) return fail(JSD_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* dp = dpdx ? dpdx : plan->scal + 1;  // a scratch slot when the caller keeps no pressure gradient
+  return mass_flux(plan, static_cast<double2*>(state), dp, s);
+}
+
+int jsd_energy(jsd_plan* plan, const void* state, double* out, void* stream) {
+  if (!plan || !state || !out) return fail(JSD_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Geo& g = plan->g;
+  k_plane_sums<<<g.ny, 256, 0, s>>>(g, static_cast<const double2*>(state), 3, 0, plan->partial);
+  JSD_LAUNCHED("k_plane_sums");
+  k_weighted_total<<<1, 32, 0, s>>>(g.ny, plan->yw, plan->partial, 0.25 * g.c_inv * g.c_inv, out);
+  JSD_LAUNCHED("k_weighted_total");
+  return 0;
+}
+
+int jsd_flow_rate(jsd_plan* plan, const void* u_field, double* out, void* stream) {
+  if (!plan || !u_field || !out) return fail(JSD_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Geo& g = plan->g;
+  k_plane_sums<<<g.ny, 256, 0, s>>>(g, static_cast<const double2*>(u_field), 1, 1, plan->partial);
+  JSD_LAUNCHED("k_plane_sums");
+  k_weighted_total<<<1, 32, 0, s>>>(g.ny, plan->yw, plan->partial, g.c_inv, out);
+  JSD_LAUNCHED("k_weighted_total");
+  return 0;
+}
+
+int jsd_nonlinear_terms(jsd_plan* plan, const void* state, int time_step, void* h_v, void* h_g, void* stream) {
+  if (!plan || !state || !h_v || !h_g) return fail(JSD_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Geo& g = plan->g;
+  const size_t fs = (size_t)g.ny * g.nk;
+  const double2* uhist = nullptr;
+  if (plan->desc.kind == JSD_KIND_DUAL && !plan->desc.linearise) {
+    if (!plan->history) return fail(JSD_ERR_STATE, "dual step needs jsd_set_history first");
+    const int idx = plan->n_history - 1 - time_step;
+    if (idx < 0) return fail(JSD_ERR_ARG, "time step beyond the registered forward history");
+    uhist = plan->history + (size_t)idx * 3 * fs;
+  }
+  int rc = nonlinear(plan, static_cast<const double2*>(state), uhist, 0, s);
+  if (rc) return rc;
+  GemmBatch b = gemm_batch(plan);
+  add_entry(b, plan->Dm, (const double*)plan->q, (double*)plan->tmp, g.ny, g.ny);
+  rc = launch_gemm(plan, b, g.ny, s);
+  if (rc) return rc;
+  k_assemble_hv<<<grid_for(fs, 256), 256, 0, s>>>(g, plan->tmp, plan->H1, static_cast<double2*>(h_v));
+  JSD_LAUNCHED("k_assemble_hv");
+  JSD_CUDA(cudaMemcpyAsync(h_g, plan->hg, fs * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,602 @@
+// Spectral-space kernels of the RK3/Crank-Nicolson velocity-vorticity step.
+//
+// Nonlinear terms (skew-symmetric form, reference navier_stokes.py:236-261 and
+// navier_stokes_perturbation.py:160-239) are evaluated pseudo-spectrally in
+// three fused passes over the y-planes:
+//   k_zinv : Hermitian part of the spectral inputs, zero-padded inverse FFT
+//            along z for every kx >= 0 (9 lines per (y, kx));
+//   k_xmid : inverse FFT along x of pairs of real fields packed as one complex
+//            line, the pointwise products, forward FFT along x (kx >= 0 kept);
+//   k_zfwd : forward FFT along z, truncation to |k| <= K with the reference's
+//            max-mode handling, and the spectral combinations the solve needs.
+// The linearised equations need no transform: their terms are y-local
+// multiples of spectral fields, handled by k_linear_terms.
+#pragma once
+
+#include "jsd_common.cuh"
+#include "jsd_fft.cuh"
+
+namespace jsd {
+
+enum EqKind { kNS = 0, kPerturbation = 1, kDual = 2 };
+
+__device__ __forceinline__ void load_twiddles(double2* dst, const double2* __restrict__ src, int n) {
+  for (int i = threadIdx.x; i < n - 1; i += blockDim.x) dst[i] = src[i];
+}
+
+// ---------------------------------------------------------------------------
+// inverse z pass: block (kx in [0, K], y). Inputs u, v, w and their y
+// derivatives du, dv, dw (spectral). Output lines (z positions 0..pz-1) of the
+// z-transformed Hermitian parts:
+//   0 u, 1 v, 2 w, 3 du/dy, 4 dv/dy, 5 dw/dy, 6 du/dz, 7 dv/dz, 8 dw/dz
+// stored at inter[((f * ny + y) * (K+1) + kx) * pz + z].
+// ---------------------------------------------------------------------------
+constexpr int kZinvLines = 9;
+
+__global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, const double2* __restrict__ u,
+                       const double2* __restrict__ v, const double2* __restrict__ w,
+                       const double2* __restrict__ du, const double2* __restrict__ dv,
+                       const double2* __restrict__ dw, double2* __restrict__ inter) {
+  extern __shared__ __align__(16) double2 zsm[];
+  const int pz = g.pz;
+  double2* twl = zsm;
+  double2* bufa = twl + pz;
+  double2* bufb = bufa + kZinvLines * pz;
+  const int kx = blockIdx.x;
+  const int y = blockIdx.y;
+  load_twiddles(twl, tw, pz);
+  for (int i = threadIdx.x; i < kZinvLines * pz; i += blockDim.x) bufa[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  const double2* src[6] = {u, v, w, du, dv, dw};
+  for (int i = threadIdx.x; i < 6 * g.mz; i += blockDim.x) {
+    const int f = i / g.mz;
+    const int iz = i - f * g.mz;
+    const int kz = signed_mode(iz, g.mz);
+    const double2 s = sym_at(g, src[f], y, kx, kz);
+    const int pos = kz >= 0 ? kz : pz + kz;
+    bufa[f * pz + pos] = s;
+    if (f < 3) bufa[(6 + f) * pz + pos] = cmul_ik(s, kz * g.az);
+  }
+  __syncthreads();
+  double2* res = fft_lines<true>(bufa, bufb, kZinvLines, fz, twl);
+  const int K1 = g.kx_max + 1;
+  for (int i = threadIdx.x; i < kZinvLines * pz; i += blockDim.x) {
+    const int f = i / pz;
+    const int z = i - f * pz;
+    inter[(((size_t)f * g.ny + y) * K1 + kx) * pz + z] = res[i];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x pass with the products: block (z block of ZB columns, y).
+// Pairs of real fields are packed as a + i b into one complex line of length
+// px whose spectrum is A[k] + i B[k] (k >= 0) and conj(A[k]) + i conj(B[k])
+// at px - k; the inverse FFT returns a in the real and b in the imaginary part.
+//
+// Skew-symmetric convective term (lam = 1 for the full equations, 0 when
+// linearised) plus the base-flow coupling of the perturbation equations with
+// U = U(y), U' = dU/dy:
+//   hel_i = -lam (u . grad) u_i + lam/2 (div u) u_i - U d_x u_i
+//           - delta_i0 (v U' - (div u) U / 2)
+// ---------------------------------------------------------------------------
+template <int ZB>
+struct XmidSmem {
+  static size_t bytes(const Geo& g) {
+    return sizeof(double2) * ((size_t)g.px + 2 * (size_t)ZB * g.px) + sizeof(double) * 7 * (size_t)ZB * g.px;
+  }
+};
+
+template <int ZB>
+__device__ __forceinline__ void xmid_build(const Geo& g, double2* line, const double2* __restrict__ inter, int y, int z0,
+                                           int fa, bool dxa, int fb, bool dxb) {
+  const int px = g.px, K1 = g.kx_max + 1;
+  for (int i = threadIdx.x; i < ZB * px; i += blockDim.x) line[i] = make_double2(0.0, 0.0);
+  __syncthreads();
+  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
+    const int kx = i / ZB;
+    const int zl = i - kx * ZB;
+    const int z = z0 + zl;
+    if (z >= g.pz) continue;
+    double2 A = inter[(((size_t)fa * g.ny + y) * K1 + kx) * g.pz + z];
+    double2 B = inter[(((size_t)fb * g.ny + y) * K1 + kx) * g.pz + z];
+    const double k = kx * g.ax;
+    if (dxa) A = cmul_ik(A, k);
+    if (dxb) B = cmul_ik(B, k);
+    double2* l = line + zl * px;
+    if (kx == 0) {
+      l[0] = make_double2(A.x, B.x);
+    } else {
+      l[kx] = make_double2(A.x - B.y, A.y + B.x);
+      l[px - kx] = make_double2(A.x + B.y, B.x - A.y);
+    }
+  }
+  __syncthreads();
+}
+
+template <int ZB>
+__global__ void k_xmid(Geo g, FftDesc fx, const double2* __restrict__ tw, const double2* __restrict__ inter,
+                       double2* __restrict__ out3, const double* __restrict__ ubase,
+                       const double* __restrict__ dubase, double lam) {
+  extern __shared__ __align__(16) double2 xsm[];
+  const int px = g.px;
+  double2* twl = xsm;
+  double2* la = twl + px;
+  double2* lb = la + ZB * px;
+  double* U = reinterpret_cast<double*>(lb + ZB * px);
+  double* V = U + ZB * px;
+  double* W = V + ZB * px;
+  double* DIV = W + ZB * px;
+  double* A0 = DIV + ZB * px;
+  double* A1 = A0 + ZB * px;
+  double* A2 = A1 + ZB * px;
+  const int z0 = blockIdx.x * ZB;
+  const int y = blockIdx.y;
+  const double ub = ubase ? ubase[y] : 0.0;
+  const double dub = dubase ? dubase[y] : 0.0;
+  const double c = g.c_inv;
+  const int npt = ZB * px;
+  load_twiddles(twl, tw, px);
+
+  // fields in the intermediate: 0 u, 1 v, 2 w, 3 du/dy, 4 dv/dy, 5 dw/dy, 6 du/dz, 7 dv/dz, 8 dw/dz
+  // pair 0: (u, v)
+  xmid_build<ZB>(g, la, inter, y, z0, 0, false, 1, false);
+  double2* r = fft_lines<true>(la, lb, ZB, fx, twl);
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    U[i] = r[i].x * c;
+    V[i] = r[i].y * c;
+  }
+  __syncthreads();
+  // pair 1: (w, du/dx)
+  xmid_build<ZB>(g, la, inter, y, z0, 2, false, 0, true);
+  r = fft_lines<true>(la, lb, ZB, fx, twl);
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double wv = r[i].x * c, dxu = r[i].y * c;
+    W[i] = wv;
+    DIV[i] = dxu;
+    A0[i] = lam * U[i] * dxu + ub * dxu;
+  }
+  __syncthreads();
+  // pair 2: (dv/dy, dw/dz)
+  xmid_build<ZB>(g, la, inter, y, z0, 4, false, 8, false);
+  r = fft_lines<true>(la, lb, ZB, fx, twl);
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double dyv = r[i].x * c, dzw = r[i].y * c;
+    DIV[i] += dyv + dzw;
+    A1[i] = lam * V[i] * dyv;
+    A2[i] = lam * W[i] * dzw;
+  }
+  __syncthreads();
+  // pair 3: (dv/dx, dw/dx)
+  xmid_build<ZB>(g, la, inter, y, z0, 1, true, 2, true);
+  r = fft_lines<true>(la, lb, ZB, fx, twl);
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double dxv = r[i].x * c, dxw = r[i].y * c;
+    A1[i] += lam * U[i] * dxv + ub * dxv;
+    A2[i] += lam * U[i] * dxw + ub * dxw;
+  }
+  __syncthreads();
+  // pair 4: (du/dy, dw/dy)
+  xmid_build<ZB>(g, la, inter, y, z0, 3, false, 5, false);
+  r = fft_lines<true>(la, lb, ZB, fx, twl);
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    A0[i] += lam * V[i] * (r[i].x * c);
+    A2[i] += lam * V[i] * (r[i].y * c);
+  }
+  __syncthreads();
+  // pair 5: (du/dz, dv/dz)
+  xmid_build<ZB>(g, la, inter, y, z0, 6, false, 7, false);
+  r = fft_lines<true>(la, lb, ZB, fx, twl);
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    A0[i] += lam * W[i] * (r[i].x * c);
+    A1[i] += lam * W[i] * (r[i].y * c);
+  }
+  __syncthreads();
+  // final products, packed (hel0 + i hel1) and (hel2 + 0 i) for the forward FFTs
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double d = DIV[i];
+    const double h0 = -A0[i] + 0.5 * lam * d * U[i] - V[i] * dub + 0.5 * d * ub;
+    const double h1 = -A1[i] + 0.5 * lam * d * V[i];
+    const double h2 = -A2[i] + 0.5 * lam * d * W[i];
+    la[i] = make_double2(h0, h1);
+    U[i] = h2;
+  }
+  __syncthreads();
+  r = fft_lines<false>(la, lb, ZB, fx, twl);
+  const int K1 = g.kx_max + 1;
+  // unpack H0, H1 for kx = 0..K
+  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
+    const int kx = i / ZB;
+    const int zl = i - kx * ZB;
+    const int z = z0 + zl;
+    if (z >= g.pz) continue;
+    const double2 a = r[zl * px + kx];
+    const double2 b = r[zl * px + (kx == 0 ? 0 : px - kx)];
+    // H0 = (Z[k] + conj Z[-k]) / 2, H1 = (Z[k] - conj Z[-k]) / (2 i)
+    const double2 h0 = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+    const double2 h1 = make_double2(0.5 * (a.y + b.y), -0.5 * (a.x - b.x));
+    out3[(((size_t)0 * g.ny + y) * K1 + kx) * g.pz + z] = h0;
+    out3[(((size_t)1 * g.ny + y) * K1 + kx) * g.pz + z] = h1;
+  }
+  __syncthreads();
+  double2* other = (r == la) ? lb : la;
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) other[i] = make_double2(U[i], 0.0);
+  __syncthreads();
+  double2* scratch = (other == la) ? lb : la;
+  r = fft_lines<false>(other, scratch, ZB, fx, twl);
+  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
+    const int kx = i / ZB;
+    const int zl = i - kx * ZB;
+    const int z = z0 + zl;
+    if (z >= g.pz) continue;
+    out3[(((size_t)2 * g.ny + y) * K1 + kx) * g.pz + z] = r[zl * px + kx];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Outputs shared by the transform path and the linear path. For a spectral
+// slot (y, ix, iz) with the three helicity components H (already truncated the
+// reference's way) compute
+//   q  = i kx H0 + i kz H2        (h_v = -d/dy q - k^2 H1)
+//   h1 = H1
+//   hg = i kz H0 - i kx H2        (h_g, navier_stokes.py:48-73)
+// and record conv00 = -H at (0, 0) for the mean-flow solve.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void write_terms(const Geo& g, int y, int ix, int iz, double2 h0, double2 h1, double2 h2,
+                                            double2* __restrict__ q, double2* __restrict__ H1,
+                                            double2* __restrict__ hg, double2* __restrict__ conv00) {
+  const double kx = kx_of(g, ix), kz = kz_of(g, iz);
+  const size_t o = sidx(g, y, ix, iz);
+  q[o] = cadd(cmul_ik(h0, kx), cmul_ik(h2, kz));
+  H1[o] = h1;
+  hg[o] = csub(cmul_ik(h0, kz), cmul_ik(h2, kx));
+  if (ix == 0 && iz == 0) {
+    conv00[y] = make_double2(-h0.x, -h0.y);
+    conv00[g.ny + y] = make_double2(-h2.x, -h2.y);
+  }
+}
+
+// forward z pass: block (kx in [0, K], y).
+__global__ void k_zfwd(Geo g, FftDesc fz, const double2* __restrict__ tw, const double2* __restrict__ out3,
+                       double2* __restrict__ q, double2* __restrict__ H1, double2* __restrict__ hg,
+                       double2* __restrict__ conv00) {
+  extern __shared__ __align__(16) double2 fsm[];
+  const int pz = g.pz;
+  double2* twl = fsm;
+  double2* bufa = twl + pz;
+  double2* bufb = bufa + 3 * pz;
+  const int kx = blockIdx.x;
+  const int y = blockIdx.y;
+  const int K1 = g.kx_max + 1;
+  load_twiddles(twl, tw, pz);
+  for (int i = threadIdx.x; i < 3 * pz; i += blockDim.x) {
+    const int f = i / pz;
+    const int z = i - f * pz;
+    bufa[i] = out3[(((size_t)f * g.ny + y) * K1 + kx) * pz + z];
+  }
+  __syncthreads();
+  double2* F = fft_lines<false>(bufa, bufb, 3, fz, twl);
+  const double cf = g.c_fwd;
+  auto getF = [&](int f, int kz) -> double2 {
+    return cscale(F[f * pz + (kz >= 0 ? kz : pz + kz)], cf);
+  };
+  const int K = g.kx_max;
+  // rows this block owns: kx itself; -kx for 1 <= kx < K; the -K slot when kx = K
+  int rows[2];
+  int nrows = 1;
+  rows[0] = kx;
+  if (kx >= 1 && kx < K) rows[nrows++] = g.mx - kx;
+  if (kx == K) rows[nrows++] = K + 1;
+  for (int i = threadIdx.x; i < nrows * g.mz; i += blockDim.x) {
+    const int rr = i / g.mz;
+    const int iz = i - rr * g.mz;
+    const int ix = rows[rr];
+    int sx, sz;
+    bool cj;
+    truncation_source(g, ix, iz, sx, sz, cj);
+    // true coefficient at (sx, sz): sx >= 0 here except for rows -kx
+    double2 h[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      double2 val = (sx >= 0) ? getF(f, sz) : cconj(getF(f, -sz));
+      h[f] = cj ? cconj(val) : val;
+    }
+    write_terms(g, y, ix, iz, h[0], h[1], h[2], q, H1, hg, conv00);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Linearised equations: every term is a y-dependent multiple of a spectral
+// field, so hat(no_hat(.) * U(y)) = U(y) * RT(.), where RT is the round trip
+// "Hermitian part, then the reference truncation". Thread per output slot.
+//   perturbation (navier_stokes_perturbation.py:160-239, lam = 0):
+//     P0 = -U i kx u - U' v + U div(u) / 2,  P1 = -U i kx v,  P2 = -U i kx w
+//   dual (navier_stokes_perturbation_dual.py:214-294, lam = 0, base (U, 0, 0)):
+//     P0 = -U i kx u + U div(u) / 4,  P1 = -U i kx v + U' u,  P2 = -U i kx w
+// ---------------------------------------------------------------------------
+template <int KIND>
+__device__ __forceinline__ void linear_pre(const Geo& g, const double2* __restrict__ u, const double2* __restrict__ v,
+                                           const double2* __restrict__ w, const double2* __restrict__ dv, int y,
+                                           int kx, int kz, double ub, double dub, double2* P) {
+  const size_t o = sidx(g, y, mode_pos(kx, g.mx), mode_pos(kz, g.mz));
+  const double2 uu = u[o], vv = v[o], ww = w[o], dvv = dv[o];
+  const double kxv = kx * g.ax, kzv = kz * g.az;
+  const double2 div = cadd(cadd(cmul_ik(uu, kxv), dvv), cmul_ik(ww, kzv));
+  if (KIND == kPerturbation) {
+    P[0] = cadd(csub(cscale(cmul_ik(uu, kxv), -ub), cscale(vv, dub)), cscale(div, 0.5 * ub));
+    P[1] = cscale(cmul_ik(vv, kxv), -ub);
+  } else {
+    P[0] = cadd(cscale(cmul_ik(uu, kxv), -ub), cscale(div, 0.25 * ub));
+    P[1] = cadd(cscale(cmul_ik(vv, kxv), -ub), cscale(uu, dub));
+  }
+  P[2] = cscale(cmul_ik(ww, kxv), -ub);
+}
+
+template <int KIND>
+__global__ void k_linear_terms(Geo g, const double2* __restrict__ u, const double2* __restrict__ v,
+                               const double2* __restrict__ w, const double2* __restrict__ dv,
+                               const double* __restrict__ ubase, const double* __restrict__ dubase,
+                               double2* __restrict__ q, double2* __restrict__ H1, double2* __restrict__ hg,
+                               double2* __restrict__ conv00) {
+  const size_t total = (size_t)g.ny * g.nk;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int y = (int)(t / g.nk);
+    const int r = (int)(t - (size_t)y * g.nk);
+    const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+    int sx, sz;
+    bool cj;
+    truncation_source(g, ix, iz, sx, sz, cj);
+    const double ub = ubase[y], dub = dubase[y];
+    double2 Pa[3], Pb[3];
+    linear_pre<KIND>(g, u, v, w, dv, y, sx, sz, ub, dub, Pa);
+    linear_pre<KIND>(g, u, v, w, dv, y, -sx, -sz, ub, dub, Pb);
+    double2 h[3];
+#pragma unroll
+    for (int f = 0; f < 3; ++f) {
+      const double2 s = make_double2(0.5 * (Pa[f].x + Pb[f].x), 0.5 * (Pa[f].y - Pb[f].y));
+      h[f] = cj ? cconj(s) : s;
+    }
+    write_terms(g, y, ix, iz, h[0], h[1], h[2], q, H1, hg, conv00);
+  }
+}
+
+// omega_y = i kz u - i kx w (the y component of curl u, domain.py:920-933)
+__global__ void k_omega(Geo g, const double2* __restrict__ u, const double2* __restrict__ w,
+                        double2* __restrict__ om) {
+  const size_t total = (size_t)g.ny * g.nk;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(t % g.nk);
+    const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+    om[t] = csub(cmul_ik(u[t], kz_of(g, iz)), cmul_ik(w[t], kx_of(g, ix)));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Per-column eigenbasis update of the Helmholtz / Poisson / influence-matrix
+// solve (navier_stokes.py:1291-1414). In the eigenbasis D2_int = V diag(lam) V^-1
+// every per-wavenumber operator is diagonal; L_j = lam_j - k^2:
+//   h_v~   = -X1 - k^2 H1~                        (h_v = -D q - k^2 H1)
+//   phi~   = L v~ + c0 v(+1) + cN v(-1)           (phi = lap v, interior)
+//   v_p~   = (R phi~ + dt_e (gamma h_v~ + xi h_v,old~)) / (H L)
+//   v_a~   = (beta dt / Re) c0 / (H L),  v_b~ = sgn v_a~   (v_b = flip v_a)
+//   [a b]  = M^-1 [-(w0 . v_p~), -(wN . v_p~)]  with M from w0, wN . v_a~, v_b~
+//   v~     = v_p~ + (a + b sgn) v_a~
+//   om~    = (R om~ + dt_e (gamma h_g~ + xi h_g,old~)) / H
+// with R = 1 + alpha dt/Re L, H = 1 - beta dt/Re L. One thread per real column.
+// ---------------------------------------------------------------------------
+struct EigTables {
+  const double* lam;
+  const double* c0;
+  const double* cN;
+  const double* sgn;
+  const double* w0;
+  const double* wN;
+};
+
+struct StageCoef {
+  double alpha, beta, gamma, xi;
+  double dt, dt_e, re;
+  int first;  // the previous-stage terms are zero
+};
+
+__global__ void k_eigen_update(Geo g, EigTables t, StageCoef sc, const double* __restrict__ X1,
+                               const double* __restrict__ H1t, const double* __restrict__ hgt,
+                               const double* __restrict__ vt, const double* __restrict__ omt,
+                               const double* __restrict__ vfield, double* __restrict__ hv_old,
+                               double* __restrict__ hg_old, double* __restrict__ vnt, double* __restrict__ omnt) {
+  const int N = 2 * g.nk;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= N) return;
+  const int kp = c >> 1;
+  const int ix = kp / g.mz, iz = kp - (kp / g.mz) * g.mz;
+  const double kx = kx_of(g, ix), kz = kz_of(g, iz);
+  const double k2 = kx * kx + kz * kz;
+  const int n = g.ny - 2;
+  const double v0 = vfield[c];
+  const double vN = vfield[(size_t)(g.ny - 1) * N + c];
+  const double ar = sc.alpha * sc.dt / sc.re;
+  const double br = sc.beta * sc.dt / sc.re;
+  double d0p = 0, dNp = 0, d0a = 0, dNa = 0, d0b = 0, dNb = 0;
+  for (int j = 0; j < n; ++j) {
+    const size_t o = (size_t)j * N + c;
+    const double L = t.lam[j] - k2;
+    const double R = 1.0 + ar * L;
+    const double H = 1.0 - br * L;
+    const double ih = 1.0 / H;
+    const double ihl = ih / L;
+    const double hv = -X1[o] - k2 * H1t[o];
+    const double hvo = sc.first ? 0.0 : hv_old[o];
+    const double phi = L * vt[o] + t.c0[j] * v0 + t.cN[j] * vN;
+    const double vp = (R * phi + sc.dt_e * (sc.gamma * hv + sc.xi * hvo)) * ihl;
+    const double va = br * t.c0[j] * ihl;
+    d0p += t.w0[j] * vp;
+    dNp += t.wN[j] * vp;
+    d0a += t.w0[j] * va;
+    dNa += t.wN[j] * va;
+    d0b += t.w0[j] * t.sgn[j] * va;
+    dNb += t.wN[j] * t.sgn[j] * va;
+    vnt[o] = vp;
+    hv_old[o] = hv;
+    const double hg = hgt[o];
+    const double hgo = sc.first ? 0.0 : hg_old[o];
+    omnt[o] = (R * omt[o] + sc.dt_e * (sc.gamma * hg + sc.xi * hgo)) * ih;
+    hg_old[o] = hg;
+  }
+  const double det = d0a * dNb - d0b * dNa;
+  const double ra = -d0p, rb = -dNp;
+  const double a = (dNb * ra - d0b * rb) / det;
+  const double b = (-dNa * ra + d0a * rb) / det;
+  for (int j = 0; j < n; ++j) {
+    const size_t o = (size_t)j * N + c;
+    const double L = t.lam[j] - k2;
+    const double H = 1.0 - br * L;
+    const double va = br * t.c0[j] / (H * L);
+    vnt[o] += (a + b * t.sgn[j]) * va;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// (0,0) mean flow: the reference's 2Ny x 2Ny system for (U00, W00)
+// (navier_stokes.py:1417-1504) with its own matrices:
+//   x_new = Linv_ns (R_ns x + dt_e gamma N + dt_e xi N_old),
+//   N = [-conv00_x - dpdx * scale, -conv00_z]
+// One block of 2 Ny threads (rows). conv_old == nullptr means zero.
+// ---------------------------------------------------------------------------
+__global__ void k_mean_flow(Geo g, const double* __restrict__ rhs_ns, const double* __restrict__ lhs_inv_ns,
+                            const double2* __restrict__ u, const double2* __restrict__ w,
+                            const double2* __restrict__ conv, const double2* __restrict__ conv_old,
+                            const double* __restrict__ dpdx, double dpdx_scale, double dt_gamma, double dt_xi,
+                            double2* __restrict__ uw00) {
+  extern __shared__ __align__(16) double2 msm[];
+  const int n = g.ny, n2 = 2 * g.ny;
+  double2* xv = msm;       // current (U00, W00)
+  double2* rv = xv + n2;   // right-hand side
+  const double dp = dpdx ? dpdx[0] * dpdx_scale : 0.0;
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+    xv[i] = (i < n) ? u[sidx(g, i, 0, 0)] : w[sidx(g, i - n, 0, 0)];
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    const double* row = rhs_ns + (size_t)i * n2;
+    for (int j = 0; j < n2; ++j) acc = cadd(acc, cscale(xv[j], row[j]));
+    const double src = (i < n) ? -dp : 0.0;
+    const double2 nn = make_double2(-conv[i].x + src, -conv[i].y);
+    const double2 no = conv_old ? make_double2(-conv_old[i].x + src, -conv_old[i].y) : make_double2(src, 0.0);
+    rv[i] = cadd(cadd(acc, cscale(nn, dt_gamma)), cscale(no, dt_xi));
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    const double* row = lhs_inv_ns + (size_t)i * n2;
+    for (int j = 0; j < n2; ++j) acc = cadd(acc, cscale(rv[j], row[j]));
+    uw00[i] = acc;
+  }
+}
+
+// u, w from continuity and omega_y (rk_not_00, navier_stokes.py:1506-1527);
+// the (0,0) mode from the mean-flow solve; walls zeroed (domain.py:630-647).
+__global__ void k_reconstruct(Geo g, const double2* __restrict__ dvn, const double2* __restrict__ omn,
+                              const double2* __restrict__ uw00, double2* __restrict__ u, double2* __restrict__ v,
+                              double2* __restrict__ w) {
+  const size_t total = (size_t)g.ny * g.nk;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int y = (int)(t / g.nk);
+    const int r = (int)(t - (size_t)y * g.nk);
+    const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+    if (y == 0 || y == g.ny - 1) {
+      u[t] = v[t] = w[t] = make_double2(0.0, 0.0);
+      continue;
+    }
+    if (ix == 0 && iz == 0) {
+      u[t] = uw00[y];
+      w[t] = uw00[g.ny + y];
+      continue;
+    }
+    const double kx = kx_of(g, ix), kz = kz_of(g, iz);
+    const double mk2 = -(kx * kx + kz * kz);
+    const double2 dv = dvn[t], om = omn[t];
+    const double2 uu = cadd(cmul_ik(dv, -kx), cmul_ik(om, kz));
+    const double2 ww = csub(cmul_ik(dv, -kz), cmul_ik(om, kx));
+    u[t] = make_double2(uu.x / mk2, uu.y / mk2);
+    w[t] = make_double2(ww.x / mk2, ww.y / mk2);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions. Both use a fixed order (per-plane partial sums, then one block
+// sums the planes) so results are reproducible run to run.
+// plane_sums: per y, sum over all modes of |Sym(f)|^2 over the three
+// components (mode = 0) or of Re f (mode = 1, one component).
+// ---------------------------------------------------------------------------
+__global__ void k_plane_sums(Geo g, const double2* __restrict__ f, int ncomp, int mode, double* __restrict__ out) {
+  const int y = blockIdx.x;
+  double acc = 0.0;
+  const size_t fs = (size_t)g.ny * g.nk;
+  for (int r = threadIdx.x; r < g.nk; r += blockDim.x) {
+    const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+    if (mode == 0) {
+      for (int c = 0; c < ncomp; ++c) {
+        const double2 s = sym_at(g, f + c * fs, y, signed_mode(ix, g.mx), signed_mode(iz, g.mz));
+        acc += s.x * s.x + s.y * s.y;
+      }
+    } else {
+      acc += f[sidx(g, y, ix, iz)].x;
+    }
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double a = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (threadIdx.x == 0) out[y] = a;
+  }
+}
+
+// out[0] = scale * sum_y weights[y] * partial[y]
+__global__ void k_weighted_total(int ny, const double* __restrict__ weights, const double* __restrict__ partial,
+                                 double scale, double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double acc = 0.0;
+    for (int y = 0; y < ny; ++y) acc += weights[y] * partial[y];
+    out[0] = scale * acc;
+  }
+}
+
+// Constant mass flux (navier_stokes.py:724-805, 1205-1214): with the flow rate
+// Q = c_inv * sum_y w_y sum_k Re u(y, k) (the y-integral of u at x = z = 0),
+//   dPdx += (Q - Q0) / dt_e,   u <- RT(u) + const
+// where the constant is -(Q - Q0) / 2 in physical units (walls included).
+__global__ void k_mass_flux_scalar(int ny, const double* __restrict__ weights, const double* __restrict__ partial,
+                                   double c_inv, double q0, double dt_e, double* __restrict__ dpdx,
+                                   double* __restrict__ qdiff) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double acc = 0.0;
+    for (int y = 0; y < ny; ++y) acc += weights[y] * partial[y];
+    const double q = c_inv * acc;
+    const double d = q - q0;
+    dpdx[0] = dpdx[0] + d / dt_e;
+    qdiff[0] = d;
+  }
+}
+
+__global__ void k_roundtrip_shift(Geo g, const double2* __restrict__ f, const double* __restrict__ qdiff,
+                                  double2* __restrict__ out) {
+  const size_t total = (size_t)g.ny * g.nk;
+  const double shift = -qdiff[0] * 0.5 / g.c_inv;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int y = (int)(t / g.nk);
+    const int r = (int)(t - (size_t)y * g.nk);
+    const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+    int sx, sz;
+    bool cj;
+    truncation_source(g, ix, iz, sx, sz, cj);
+    double2 s = sym_at(g, f, y, sx, sz);
+    if (cj) s = cconj(s);
+    if (ix == 0 && iz == 0) s.x += shift;
+    out[t] = s;
+  }
+}
+
+}  // namespace jsd

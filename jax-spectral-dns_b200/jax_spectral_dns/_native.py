@@ -1,0 +1,93 @@
+"""ctypes binding of the native step library (libjsd.so, C ABI in include/jsd.h).
+
+The library is built in-tree (``jax_spectral_dns/_build.py``) and loaded from
+this package directory. There is no fallback: if the library is missing or
+fails to load, every time-stepping call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libjsd.so")
+
+JSD_KIND_NS = 0
+JSD_KIND_PERTURBATION = 1
+JSD_KIND_DUAL = 2
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+class JsdDesc(ctypes.Structure):
+    """Mirror of ``jsd_desc`` (include/jsd.h)."""
+
+    _fields_ = [
+        ("mx", ctypes.c_int), ("ny", ctypes.c_int), ("mz", ctypes.c_int),
+        ("px_ref", ctypes.c_int), ("pz_ref", ctypes.c_int),
+        ("px_fft", ctypes.c_int), ("pz_fft", ctypes.c_int),
+        ("lx", ctypes.c_double), ("lz", ctypes.c_double),
+        ("kind", ctypes.c_int), ("linearise", ctypes.c_int), ("constant_mass_flux", ctypes.c_int),
+        ("re_tau", ctypes.c_double), ("dt", ctypes.c_double), ("dt_explicit", ctypes.c_double),
+        ("flow_rate_target", ctypes.c_double),
+        ("base_u", _dp), ("base_du", _dp),
+        ("D", _dp), ("V", _dp), ("Vinv", _dp), ("lam", _dp), ("sgn", _dp),
+        ("c0", _dp), ("cN", _dp), ("w0", _dp), ("wN", _dp), ("y_weights", _dp),
+        ("rhs_ns", _dp), ("lhs_inv_ns", _dp),
+    ]
+
+
+EXPORTED = (
+    "jsd_plan_create", "jsd_plan_destroy", "jsd_step", "jsd_set_history",
+    "jsd_correct_mass_flux", "jsd_energy", "jsd_flow_rate", "jsd_nonlinear_terms",
+    "jsd_workspace_bytes", "jsd_launches_per_step", "jsd_last_error", "jsd_abi_version",
+    "jsd_profile_enable", "jsd_profile_read",
+)
+
+PROF_CLASSES = {"gemm": 0, "zinv": 1, "xmid": 2, "zfwd": 3, "eigen": 4, "linear": 5}
+
+_lib = None
+
+
+class NativeError(RuntimeError):
+    pass
+
+
+def load(path: str = LIB_PATH):
+    """Load libjsd.so and declare its signatures (raises if it is absent)."""
+    global _lib
+    if _lib is not None and path == LIB_PATH:
+        return _lib
+    if not os.path.exists(path):
+        raise NativeError(
+            f"native library not found at {path}; build it with "
+            "`python -c 'import __graft_entry__ as g; g.build()'` (requires nvcc)")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    lib.jsd_plan_create.argtypes = [ctypes.POINTER(JsdDesc), ctypes.POINTER(vp)]
+    lib.jsd_plan_destroy.argtypes = [vp]
+    lib.jsd_step.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
+    lib.jsd_set_history.argtypes = [vp, vp, ctypes.c_int]
+    lib.jsd_correct_mass_flux.argtypes = [vp, vp, vp, vp]
+    lib.jsd_energy.argtypes = [vp, vp, vp, vp]
+    lib.jsd_flow_rate.argtypes = [vp, vp, vp, vp]
+    lib.jsd_nonlinear_terms.argtypes = [vp, vp, ctypes.c_int, vp, vp, vp]
+    lib.jsd_workspace_bytes.argtypes = [vp]
+    lib.jsd_workspace_bytes.restype = ctypes.c_size_t
+    lib.jsd_launches_per_step.argtypes = [vp]
+    lib.jsd_last_error.restype = ctypes.c_char_p
+    lib.jsd_profile_enable.argtypes = [vp, ctypes.c_int]
+    lib.jsd_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                     ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
+    for name in EXPORTED:
+        if name not in ("jsd_workspace_bytes", "jsd_last_error"):
+            getattr(lib, name).restype = ctypes.c_int
+    if path == LIB_PATH:
+        _lib = lib
+    return lib
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        msg = load().jsd_last_error().decode(errors="replace")
+        raise NativeError(f"{what} failed ({rc}): {msg}")

@@ -1,0 +1,161 @@
+"""Device step plan: owns a native jsd_plan and the device buffers around it.
+
+Spectral states handed to the native library use the plane-major layout
+(3, Ny, Mx, Mz) complex128; the reference layout (3, Mx, Ny, Mz) is converted
+at this boundary (``to_device_layout`` / ``to_reference_layout``).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _native
+from ._ops import fourier_scale, mean_flow_matrices, operator_tables, smooth_fft_size
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def to_device_layout(x, device="cuda") -> torch.Tensor:
+    """(3, Mx, Ny, Mz) or (Mx, Ny, Mz) complex -> contiguous (.., Ny, Mx, Mz) on device."""
+    t = torch.as_tensor(x)
+    if not t.is_complex():
+        t = t.to(torch.complex128)
+    t = t.to(device=device, dtype=torch.complex128)
+    return t.transpose(-3, -2).contiguous()
+
+
+def to_reference_layout(x: torch.Tensor) -> torch.Tensor:
+    return x.transpose(-3, -2).contiguous()
+
+
+def _stream_ptr() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class StepPlan:
+    """One native plan for a box, an equation kind and (Re, dt)."""
+
+    def __init__(self, modes, phys_ref, lx, lz, kind, re_tau, dt, dt_explicit=None, linearise=False,
+                 constant_mass_flux=False, flow_rate_target=0.0, base_u: Optional[np.ndarray] = None,
+                 fft_sizes=None, device="cuda"):
+        if not torch.cuda.is_available():
+            raise _native.NativeError("the velocity-vorticity step needs a CUDA device")
+        self.lib = _native.load()
+        mx, ny, mz = (int(m) for m in modes)
+        self.modes = (mx, ny, mz)
+        self.device = torch.device(device)
+        t = operator_tables(ny)
+        rhs_ns, lhs_inv_ns = mean_flow_matrices(ny, re_tau, dt)
+        self._keep = []
+
+        def arr(a):
+            a = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+            self._keep.append(a)
+            return _ptr(a)
+
+        d = _native.JsdDesc()
+        d.mx, d.ny, d.mz = mx, ny, mz
+        d.px_ref, d.pz_ref = int(phys_ref[0]), int(phys_ref[-1])
+        px, pz = fft_sizes if fft_sizes is not None else (smooth_fft_size(mx), smooth_fft_size(mz))
+        d.px_fft, d.pz_fft = int(px), int(pz)
+        self.fft_sizes = (int(px), int(pz))
+        d.lx, d.lz = float(lx), float(lz)
+        d.kind = int(kind)
+        d.linearise = int(bool(linearise))
+        d.constant_mass_flux = int(bool(constant_mass_flux))
+        d.re_tau = float(re_tau)
+        d.dt = float(dt)
+        d.dt_explicit = float(dt if dt_explicit is None else dt_explicit)
+        d.flow_rate_target = float(flow_rate_target)
+        if base_u is not None:
+            bu = np.asarray(base_u, dtype=np.float64)
+            d.base_u = arr(bu)
+            d.base_du = arr(t.D @ bu)
+        d.D, d.V, d.Vinv = arr(t.D), arr(t.V), arr(t.Vinv)
+        d.lam, d.sgn, d.c0, d.cN = arr(t.lam), arr(t.sgn), arr(t.c0), arr(t.cN)
+        d.w0, d.wN, d.y_weights = arr(t.w0), arr(t.wN), arr(t.y_weights)
+        d.rhs_ns, d.lhs_inv_ns = arr(rhs_ns), arr(lhs_inv_ns)
+        self.desc = d
+        h = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _native.check(self.lib.jsd_plan_create(ctypes.byref(d), ctypes.byref(h)), "jsd_plan_create")
+        self.handle = h
+        self.scale = fourier_scale(lx, lz)
+        self._scalar = torch.zeros(4, dtype=torch.float64, device=self.device)
+        self._history = None
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                self.lib.jsd_plan_destroy(h)
+            except Exception:
+                pass
+            self.handle = None
+
+    # --- calls ------------------------------------------------------------
+    def workspace_bytes(self) -> int:
+        return int(self.lib.jsd_workspace_bytes(self.handle))
+
+    def launches_per_step(self) -> int:
+        return int(self.lib.jsd_launches_per_step(self.handle))
+
+    def step(self, state: torch.Tensor, dpdx: torch.Tensor, first_step: int, n_steps: int):
+        """Advance a device-layout state in place; dpdx is a 1-element float64 device tensor."""
+        assert state.is_contiguous() and state.dtype == torch.complex128 and state.device.type == "cuda"
+        assert dpdx.dtype == torch.float64 and dpdx.device.type == "cuda"
+        _native.check(self.lib.jsd_step(self.handle, ctypes.c_void_p(state.data_ptr()),
+                                        ctypes.c_void_p(dpdx.data_ptr()), int(first_step), int(n_steps),
+                                        _stream_ptr()), "jsd_step")
+
+    def set_history(self, states: Optional[torch.Tensor]):
+        """Forward trajectory (n, 3, Ny, Mx, Mz) for the dual equations."""
+        self._history = states
+        if states is None:
+            _native.check(self.lib.jsd_set_history(self.handle, None, 0), "jsd_set_history")
+        else:
+            assert states.is_contiguous() and states.dtype == torch.complex128
+            _native.check(self.lib.jsd_set_history(self.handle, ctypes.c_void_p(states.data_ptr()),
+                                                   int(states.shape[0])), "jsd_set_history")
+
+    def energy(self, state: torch.Tensor) -> torch.Tensor:
+        out = torch.empty(1, dtype=torch.float64, device=state.device)
+        _native.check(self.lib.jsd_energy(self.handle, ctypes.c_void_p(state.data_ptr()),
+                                          ctypes.c_void_p(out.data_ptr()), _stream_ptr()), "jsd_energy")
+        return out
+
+    def flow_rate(self, u_field: torch.Tensor) -> torch.Tensor:
+        out = torch.empty(1, dtype=torch.float64, device=u_field.device)
+        _native.check(self.lib.jsd_flow_rate(self.handle, ctypes.c_void_p(u_field.data_ptr()),
+                                             ctypes.c_void_p(out.data_ptr()), _stream_ptr()), "jsd_flow_rate")
+        return out
+
+    def correct_mass_flux(self, state: torch.Tensor, dpdx: Optional[torch.Tensor] = None):
+        _native.check(self.lib.jsd_correct_mass_flux(
+            self.handle, ctypes.c_void_p(state.data_ptr()),
+            ctypes.c_void_p(dpdx.data_ptr()) if dpdx is not None else None, _stream_ptr()),
+            "jsd_correct_mass_flux")
+
+    def profile(self, enable: bool) -> None:
+        _native.check(self.lib.jsd_profile_enable(self.handle, int(bool(enable))), "jsd_profile_enable")
+
+    def profile_read(self, name: str):
+        """(total ms, launches, algorithmic work) of one kernel class since the last read."""
+        ms, n, w = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_double()
+        _native.check(self.lib.jsd_profile_read(self.handle, _native.PROF_CLASSES[name], ctypes.byref(ms),
+                                                ctypes.byref(n), ctypes.byref(w)), "jsd_profile_read")
+        return ms.value, n.value, w.value
+
+    def nonlinear_terms(self, state: torch.Tensor, time_step: int = 0):
+        mx, ny, mz = self.modes
+        hv = torch.empty((ny, mx, mz), dtype=torch.complex128, device=state.device)
+        hg = torch.empty_like(hv)
+        _native.check(self.lib.jsd_nonlinear_terms(self.handle, ctypes.c_void_p(state.data_ptr()), int(time_step),
+                                                   ctypes.c_void_p(hv.data_ptr()), ctypes.c_void_p(hg.data_ptr()),
+                                                   _stream_ptr()), "jsd_nonlinear_terms")
+        return hv, hg

@@ -1,0 +1,181 @@
+"""Dual (adjoint) perturbation equations on the B200 step kernels.
+
+Drop-in for ``NavierStokesVelVortPerturbationDual`` of
+dakling/jax-spectral-dns (navier_stokes_perturbation_dual.py:376-1201): the
+dual is the same RK3/CN stepper run backward -- Re and dt negated, the
+implicit operators taken from the forward equation, the nonlinear term replaced
+by the adjoint convection with the forward state u(T - t) frozen over each step
+-- started from -u(T). The gradient of the gain G = E(T)/E(0) is
+(u0 - v0) / E0.
+"""
+from __future__ import annotations
+
+from typing import Any, Optional, Tuple
+
+import torch
+
+from . import _native
+from ._plan import to_device_layout, to_reference_layout
+from .equation import print_verb
+from .field import FourierField, VectorField
+from .navier_stokes_perturbation import NavierStokesVelVortPerturbation
+
+
+class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
+    name = ("Dual Navier Stokes equation (velocity-vorticity formulation) for perturbations on top of a "
+            "base flow.")
+    _kind = _native.JSD_KIND_DUAL
+
+    def __init__(self, velocity_field: Optional[VectorField], forward_equation: NavierStokesVelVortPerturbation,
+                 **params: Any):
+        self.epsilon = params.get("epsilon", 1e-5)
+        mode = params.get("optimisation_mode", "gain")
+        if mode != "gain":
+            raise NotImplementedError(f"optimisation_mode={mode!r}: only 'gain' is supported")
+        self.optimisation_mode = mode
+        if params.get("constant_mass_flux", False):
+            raise NotImplementedError("the dual with constant mass flux is not supported")
+        if velocity_field is None:
+            velocity_field = forward_equation.get_latest_field("velocity_hat") * 0.0
+        self.forward_equation = forward_equation
+        super().__init__(velocity_field, **params)
+        self.velocity_u_hat_0 = forward_equation.get_initial_field("velocity_hat")
+        self.velocity_field_u_history = None
+        self.dPdx_history = None
+        self.checkpointing = bool(params.get("checkpointing", False))
+        self.gain = None
+        self._forward_done = False
+        self._backward_done = False
+
+    def get_fixed_params(self):
+        return self.forward_equation
+
+    @classmethod
+    def FromNavierStokesVelVortPerturbation(cls, nse: NavierStokesVelVortPerturbation, **params: Any):
+        """Dual of a forward perturbation problem (..._dual.py:542-589)."""
+        nse.write_entire_output = True
+        nse.write_intermediate_output = False
+        stripped = {k: v for k, v in params.items() if k not in (
+            "Re_tau", "Re", "dt", "end_time", "velocity_base_hat", "constant_mass_flux", "linearise",
+            "linearise_switch", "coupling_term", "coupling_term_switch")}
+        dual = cls(None, nse, Re_tau=-nse.get_Re_tau(), dt=-nse.get_dt(), end_time=-nse.end_time,
+                   velocity_base_hat=nse.get_latest_field("velocity_base_hat"),
+                   constant_mass_flux=nse.constant_mass_flux, linearise=nse.linearise(0),
+                   coupling_term=True, **stripped)
+        return dual
+
+    def _plan_spec(self) -> dict:
+        """The dual steps with the forward equation's implicit operators
+        (positive Re and dt) and -dt on the explicit terms."""
+        spec = super()._plan_spec()
+        spec["re_tau"] = self.forward_equation.get_Re_tau()
+        spec["dt"] = self.forward_equation.get_dt()
+        spec["dt_explicit"] = self.get_dt()
+        spec["constant_mass_flux"] = False
+        return spec
+
+    def _prepare_plan_history(self, plan) -> None:
+        if self.linearise(0):
+            return
+        traj = getattr(self.forward_equation, "_trajectory_device", None)
+        if traj is None:
+            raise RuntimeError("run the forward calculation before the nonlinear dual step")
+        if plan._history is not traj:
+            plan.set_history(traj)
+
+    def is_forward_calculation_done(self) -> bool:
+        return self._forward_done
+
+    def is_backward_calculation_done(self) -> bool:
+        return self._backward_done
+
+    def run_forward_calculation(self) -> None:
+        """Forward run keeping the trajectory; dual initial field -u(T)
+        (..._dual.py:850-939)."""
+        nse = self.forward_equation
+        self.velocity_u_hat_0 = nse.get_initial_field("velocity_hat")
+        if not self._forward_done:
+            nse.write_entire_output = True
+            nse.end_time = -1.0 * self.end_time
+            traj, dps, _ = nse.solve_scan()
+            self.velocity_field_u_history = traj
+            self.dPdx_history = dps
+            self._forward_done = True
+        self.set_initial_field("velocity_hat", -1 * nse.get_latest_field("velocity_hat"))
+
+    def run_backward_calculation(self) -> None:
+        if not self._backward_done:
+            self.run_forward_calculation()
+            self.write_entire_output = False
+            self.write_intermediate_output = False
+            self.dPdx = 0.0
+            print_verb("performing backward (adjoint) calculation...", verbosity_level=2)
+            self.solve_scan()
+            self._backward_done = True
+
+    def get_gain(self) -> float:
+        self.run_forward_calculation()
+        nse = self.forward_equation
+        e0 = nse.energy_of(nse.get_initial_field("velocity_hat").get_data())
+        eT = nse.energy_of(nse.get_latest_field("velocity_hat").get_data())
+        self.gain = eT / e0
+        return self.gain
+
+    def get_objective_fun(self) -> float:
+        return self.get_gain()
+
+    def get_objective_fun_name(self) -> str:
+        return self.optimisation_mode
+
+    def get_grad(self, u_hat_0: Optional[VectorField] = None, v_hat_0: Optional[VectorField] = None):
+        """(u0 - v0) / E0 (..._dual.py:1106-1120)."""
+        if u_hat_0 is None and v_hat_0 is None:
+            self.run_backward_calculation()
+        if u_hat_0 is None:
+            u_hat_0 = self.forward_equation.get_initial_field("velocity_hat")
+        if v_hat_0 is None:
+            v_hat_0 = self.get_latest_field("velocity_hat")
+        self.get_gain()
+        e0 = self.forward_equation.energy_of(u_hat_0.get_data())
+        return (u_hat_0.get_data() - v_hat_0.get_data()) / e0
+
+    def _projection(self, step_size, u_hat_0, v_data, step_size_factor):
+        """Step along the gradient projected on the constant-energy sphere
+        (..._dual.py:1122-1150)."""
+        if step_size_factor is None:
+            step_size_factor = 0.9
+        assert 0 < step_size_factor < 1, "invalid choice of initial step size factor."
+        nse = self.forward_equation
+        u_data = u_hat_0.get_data()
+        e0 = nse.energy_of(u_data)
+        e0_adj = nse.energy_of(v_data)
+        # 2 <v, u> = E(u + v) - E(u) - E(v) (energy is a quadratic form)
+        c0 = nse.energy_of(u_data + v_data) - e0 - e0_adj
+        max_step = step_size_factor * (e0_adj / e0 - c0 ** 2 / (4 * e0 ** 2)) ** (-1 / 2)
+        step_size = min(step_size, max_step)
+        A = (step_size * c0 - 2 * e0) / (2 * step_size * e0)
+        lam = A + (A ** 2 - (step_size * e0_adj - c0) / (step_size * e0)) ** 0.5
+        return lam, step_size
+
+    def get_projected_grad(self, step_size: float, u_hat_0=None, v_hat_0=None, step_size_factor=None
+                           ) -> Tuple[torch.Tensor, bool]:
+        if u_hat_0 is None and v_hat_0 is None:
+            self.run_backward_calculation()
+        if u_hat_0 is None:
+            u_hat_0 = self.velocity_u_hat_0
+        if v_hat_0 is None:
+            v_hat_0 = self.get_latest_field("velocity_hat")
+        lam, _ = self._projection(step_size, u_hat_0, v_hat_0.get_data(), step_size_factor)
+        return lam * u_hat_0.get_data() - v_hat_0.get_data(), True
+
+    def get_projected_cg_grad(self, step_size: float, beta: float, old_grad, u_hat_0=None, v_hat_0=None,
+                              step_size_factor=None) -> Tuple[torch.Tensor, bool]:
+        if u_hat_0 is None and v_hat_0 is None:
+            self.run_backward_calculation()
+        if u_hat_0 is None:
+            u_hat_0 = self.velocity_u_hat_0
+        if v_hat_0 is None:
+            v_hat_0 = self.get_latest_field("velocity_hat")
+        v_data = v_hat_0.get_data() - beta * old_grad
+        lam, _ = self._projection(step_size, u_hat_0, v_data, step_size_factor)
+        return lam * u_hat_0.get_data() + (-1.0 * v_hat_0.get_data() + beta * old_grad), True

@@ -5,7 +5,10 @@ benchmark configurations: for every admissible wavenumber pair (kx, kz) draw
 complex Chebyshev coefficients c_n, d_n ~ N(0,1) + i N(0,1) damped by
 exp(-n/8); evaluate on the Gauss-Lobatto points; multiply by (1-y^2)^2 for the
 wall-normal velocity v and by (1-y^2) for the wall-normal vorticity omega_y so
-that no-slip holds exactly; impose Hermitian symmetry F(-k) = conj F(k); then
+that no-slip holds exactly; the series stop at n < Ny-4 (v) and n < Ny-2
+(omega_y) so both products are polynomials of degree <= Ny-1, which the
+collocation grid represents exactly (dv/dy then vanishes at the walls to
+round-off and the field is divergence-free at every point); impose Hermitian symmetry F(-k) = conj F(k); then
 recover (u, w) from continuity and the definition of omega_y exactly as the
 reference does in ``NavierStokesVelVort.vort_yvel_to_vel``
 (navier_stokes.py:1100-1123):
@@ -27,8 +30,9 @@ import numpy as np
 
 
 def cheb_points(ny: int) -> np.ndarray:
-    """Gauss-Lobatto points y_i = cos(pi i / (Ny-1)) (domain.py:130-140)."""
-    return np.cos(np.pi * np.arange(ny) / (ny - 1))
+    """Gauss-Lobatto points y_i = cos(pi / (Ny-1) * i), evaluated point by
+    point in the same operation order as get_cheb_grid (domain.py:130-140)."""
+    return np.array([np.cos(np.pi / (ny - 1) * i) for i in np.arange(ny)])
 
 
 def cheb_diff_matrix(y: np.ndarray) -> np.ndarray:
@@ -163,6 +167,8 @@ def seeded_velocity_hat(
                 continue
             c = (rng.standard_normal(ny) + 1j * rng.standard_normal(ny)) * damp
             dd = (rng.standard_normal(ny) + 1j * rng.standard_normal(ny)) * damp
+            c[ny - 4:] = 0.0
+            dd[ny - 2:] = 0.0
             vy = (1.0 - y ** 2) ** 2 * (tmat @ c)
             oy = (1.0 - y ** 2) * (tmat @ dd)
             a, b = idx(ix, mx), idx(iz, mz)

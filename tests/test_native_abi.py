@@ -1,0 +1,60 @@
+"""The C-ABI library loads and exports every symbol include/jsd.h declares
+(no compute calls: runs without a GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import REPO
+
+HEADER = os.path.join(REPO, "include", "jsd.h")
+
+
+def _declared():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(jsd_[a-z_0-9]+)\s*\(", src)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from jax_spectral_dns import _build, _native
+
+    if not os.path.exists(_native.LIB_PATH):
+        _build.build()
+    return _native.load()
+
+
+def test_header_declares_entry_points():
+    names = _declared()
+    for n in ("jsd_plan_create", "jsd_step", "jsd_energy", "jsd_set_history"):
+        assert n in names
+
+
+def test_every_declared_symbol_is_exported(lib):
+    for name in _declared():
+        assert hasattr(lib, name), name
+
+
+def test_binding_covers_header(lib):
+    from jax_spectral_dns import _native
+
+    assert set(_declared()) <= set(_native.EXPORTED) | {"jsd_abi_version", "jsd_last_error"}
+
+
+def test_abi_version_and_error_strings(lib):
+    assert lib.jsd_abi_version() == 1
+    assert isinstance(lib.jsd_last_error(), bytes)
+
+
+def test_plan_create_rejects_bad_descriptor_without_gpu(lib):
+    """Argument validation happens before any CUDA call."""
+    from jax_spectral_dns import _native
+
+    d = _native.JsdDesc()
+    d.mx, d.ny, d.mz = 4, 33, 9  # even mode count
+    h = ctypes.c_void_p()
+    rc = lib.jsd_plan_create(ctypes.byref(d), ctypes.byref(h))
+    assert rc == -1
+    assert b"odd" in lib.jsd_last_error()

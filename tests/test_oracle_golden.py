@@ -1,0 +1,68 @@
+"""The CPU oracle against outputs of the unmodified reference (golden fixtures).
+
+These pin the oracle: each fixture was produced by the reference package
+itself (tests/golden/make_golden.py), so agreement to ~1e-12 here means the
+oracle restates the reference's arithmetic, quirks included.
+"""
+import numpy as np
+import pytest
+
+import jsd_oracle as O
+from conftest import golden, rel
+
+
+def _pert(d, linearise):
+    return O.make_stepper("perturbation", tuple(d["shape"]), *d["lengths"], float(d["re"]), float(d["dt"]),
+                          linearise=linearise)
+
+
+def test_linearised_perturbation_pseudo2d():
+    d = golden("lin_pert_9x65x5")
+    st = _pert(d, True)
+    u = d["u0"]
+    for t in range(10):
+        u, _ = st.rk_step(u, 0.0, t)
+        if t == 0:
+            assert rel(u, d["u1"]) < 1e-12
+    assert rel(u, d["u10"]) < 1e-12
+    assert abs(st.g.energy(u) / d["energy"][10] - 1) < 1e-12
+
+
+@pytest.mark.parametrize("name,steps", [("nonlin_pert_9x33x9", 20), ("nonlin_pert_5x24x13", 5)])
+def test_nonlinear_perturbation(name, steps):
+    d = golden(name)
+    st = _pert(d, False)
+    u, _, _ = O.run(st, d["u0"], steps)
+    assert rel(u, d["u%d" % steps]) < 1e-12
+
+
+@pytest.mark.parametrize("name,cmf", [("ns_cmf_9x33x9", True), ("ns_cpg_9x33x9", False)])
+def test_navier_stokes(name, cmf):
+    d = golden(name)
+    g = O.Grid(tuple(d["shape"]), *d["lengths"])
+    q0 = g.flow_rate(d["u0"][0])
+    if cmf:
+        assert abs(q0 / float(d["flow_rate"]) - 1) < 1e-13
+    st = O.Stepper(g, float(d["re_tau"]), float(d["dt"]), kind="ns", constant_mass_flux=cmf, flow_rate_target=q0)
+    u, dp, _ = O.run(st, d["u0"], 10, dpdx=float(d["dpdx"][0]))
+    assert rel(u, d["u10"]) < 1e-12
+    assert abs(dp - d["dpdx"][-1]) < 1e-9 * max(1.0, abs(dp))
+
+
+@pytest.mark.parametrize("name,lin", [("dual_lin_5x33x5", True), ("dual_nonlin_9x33x9", False)])
+def test_dual_gradient(name, lin):
+    d = golden(name)
+    grad, gain, _, uT = O.dual_gradient(tuple(d["shape"]), *d["lengths"], float(d["re"]), float(d["dt"]),
+                                        int(d["n_steps"]), d["u0"], lin)
+    assert rel(grad, d["grad"]) < 1e-12
+    assert rel(uT, d["uT"]) < 1e-12
+    assert abs(gain / float(d["gain"]) - 1) < 1e-13
+
+
+def test_transient_growth_energy_history():
+    """E(t) over the first 100 steps of the pseudo-2D linear case."""
+    d = golden("lin_pert_9x65x5")
+    e = d["energy"]
+    assert e.shape == (101,)
+    assert np.all(np.isfinite(e)) and e[0] > 0
+    assert abs(e[0] / 1e-6 - 1) < 1e-10  # seeded at E0 = 1e-6
