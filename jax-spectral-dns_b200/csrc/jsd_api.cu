@@ -267,10 +267,8 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
   const int ny = g.ny;
   double2* conv = p->conv + (size_t)stage * 2 * ny;
   const bool linear = p->desc.linearise && p->desc.kind != JSD_KIND_NS;
-  if (p->desc.kind == JSD_KIND_DUAL && !linear) {
-    (void)uhist;
-    return fail(JSD_ERR_ARG, "the nonlinear dual step is not available in this build");
-  }
+  if (p->desc.kind == JSD_KIND_DUAL && !linear && !uhist)
+    return fail(JSD_ERR_STATE, "dual step needs the forward state (jsd_set_history)");
   if (linear) {
     GemmBatch b = gemm_batch(p);
     add_entry(b, p->Dm, (const double*)v, (double*)(p->Dfld + fs), ny, ny);
@@ -287,20 +285,41 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
     JSD_LAUNCHED("k_linear_terms");
     return 0;
   }
+  const bool dual = p->desc.kind == JSD_KIND_DUAL;
+  const int nsets = dual ? 2 : 1;
   GemmBatch b = gemm_batch(p);
   for (int c = 0; c < 3; ++c) add_entry(b, p->Dm, (const double*)(state + c * fs), (double*)(p->Dfld + c * fs), ny, ny);
+  if (dual)
+    for (int c = 0; c < 3; ++c)
+      add_entry(b, p->Dm, (const double*)(uhist + c * fs), (double*)(p->Dfld + (3 + c) * fs), ny, ny);
   int rc = launch_gemm(p, b, ny, s);
   if (rc) return rc;
   const int K1 = g.kx_max + 1;
   {
-    const size_t sm = sizeof(double2) * ((size_t)g.pz + 2 * kZinvLines * (size_t)g.pz);
-    const double bytes = sizeof(double2) * (6.0 * fs + (double)kZinvLines * ny * K1 * g.pz);
+    ZinvSrc src;
+    src.nsets = nsets;
+    for (int c = 0; c < 3; ++c) {
+      src.f[c] = state + c * fs;
+      src.f[3 + c] = p->Dfld + c * fs;
+      if (dual) {
+        src.f[6 + c] = uhist + c * fs;
+        src.f[9 + c] = p->Dfld + (3 + c) * fs;
+      }
+    }
+    const int nl = kZinvLines * nsets;
+    const size_t sm = sizeof(double2) * ((size_t)g.pz + 2 * (size_t)nl * g.pz);
+    const double bytes = sizeof(double2) * (6.0 * nsets * fs + (double)nl * ny * K1 * g.pz);
     ProfScope ps(p, JSD_PROF_ZINV, bytes, s);
-    k_zinv<<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, p->twz, u, v, w, p->Dfld, p->Dfld + fs, p->Dfld + 2 * fs,
-                                         p->inter);
+    k_zinv<<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, p->twz, src, p->inter);
     JSD_LAUNCHED("k_zinv");
   }
-  {
+  if (dual) {
+    const size_t sm = XmidDualSmem<kXmidZB>::bytes(g);
+    ProfScope ps(p, JSD_PROF_XMID, sizeof(double2) * (double)(2 * kZinvLines + 3) * ny * K1 * g.pz, s);
+    k_xmid_dual<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), 256, sm, s>>>(
+        g, p->fx, p->twx, p->inter, p->out3, p->ub, p->dub);
+    JSD_LAUNCHED("k_xmid_dual");
+  } else {
     const size_t sm = XmidSmem<kXmidZB>::bytes(g);
     ProfScope ps(p, JSD_PROF_XMID, sizeof(double2) * (double)(kZinvLines + 3) * ny * K1 * g.pz, s);
     const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
@@ -406,6 +425,7 @@ int set_smem_limits() {
   const int big = 200 * 1024;
   JSD_CUDA(cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_xmid<kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_xmid_dual<kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_dgemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<48>::BYTES));
   JSD_CUDA(cudaFuncSetAttribute(k_dgemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<64>::BYTES));
@@ -571,9 +591,10 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
 
   const bool linear = d->linearise && d->kind != JSD_KIND_NS;
   const size_t K1 = g.kx_max + 1;
-  JSD_TRY(dev_alloc(p, (void**)&p->Dfld, 3 * fs * sizeof(double2)));
+  const int nsets = (d->kind == JSD_KIND_DUAL) ? 2 : 1;
+  JSD_TRY(dev_alloc(p, (void**)&p->Dfld, 3 * (size_t)nsets * fs * sizeof(double2)));
   if (!linear) {
-    JSD_TRY(dev_alloc(p, (void**)&p->inter, kZinvLines * (size_t)ny * K1 * g.pz * sizeof(double2)));
+    JSD_TRY(dev_alloc(p, (void**)&p->inter, (size_t)kZinvLines * nsets * ny * K1 * g.pz * sizeof(double2)));
     JSD_TRY(dev_alloc(p, (void**)&p->out3, 3 * (size_t)ny * K1 * g.pz * sizeof(double2)));
   }
   for (double2** f : {&p->q, &p->H1, &p->hg, &p->om, &p->dvn, &p->tmp})

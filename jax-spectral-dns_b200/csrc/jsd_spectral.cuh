@@ -33,34 +33,41 @@ __device__ __forceinline__ void load_twiddles(double2* dst, const double2* __res
 // ---------------------------------------------------------------------------
 constexpr int kZinvLines = 9;
 
-__global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, const double2* __restrict__ u,
-                       const double2* __restrict__ v, const double2* __restrict__ w,
-                       const double2* __restrict__ du, const double2* __restrict__ dv,
-                       const double2* __restrict__ dw, double2* __restrict__ inter) {
+// Up to two sets of spectral inputs (u, v, w, du/dy, dv/dy, dw/dy): the state
+// being stepped and, for the dual equations, the frozen forward state.
+struct ZinvSrc {
+  const double2* f[12];
+  int nsets;
+};
+
+__global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, ZinvSrc src,
+                       double2* __restrict__ inter) {
   extern __shared__ __align__(16) double2 zsm[];
   const int pz = g.pz;
+  const int nl = kZinvLines * src.nsets;
   double2* twl = zsm;
   double2* bufa = twl + pz;
-  double2* bufb = bufa + kZinvLines * pz;
+  double2* bufb = bufa + nl * pz;
   const int kx = blockIdx.x;
   const int y = blockIdx.y;
   load_twiddles(twl, tw, pz);
-  for (int i = threadIdx.x; i < kZinvLines * pz; i += blockDim.x) bufa[i] = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < nl * pz; i += blockDim.x) bufa[i] = make_double2(0.0, 0.0);
   __syncthreads();
-  const double2* src[6] = {u, v, w, du, dv, dw};
-  for (int i = threadIdx.x; i < 6 * g.mz; i += blockDim.x) {
-    const int f = i / g.mz;
+  for (int i = threadIdx.x; i < 6 * src.nsets * g.mz; i += blockDim.x) {
+    const int f = i / g.mz;        // input index 0 .. 6 nsets - 1
     const int iz = i - f * g.mz;
+    const int set = f / 6, fi = f - set * 6;
     const int kz = signed_mode(iz, g.mz);
-    const double2 s = sym_at(g, src[f], y, kx, kz);
+    const double2 sv = sym_at(g, src.f[f], y, kx, kz);
     const int pos = kz >= 0 ? kz : pz + kz;
-    bufa[f * pz + pos] = s;
-    if (f < 3) bufa[(6 + f) * pz + pos] = cmul_ik(s, kz * g.az);
+    double2* lines = bufa + (size_t)set * kZinvLines * pz;
+    lines[fi * pz + pos] = sv;
+    if (fi < 3) lines[(6 + fi) * pz + pos] = cmul_ik(sv, kz * g.az);
   }
   __syncthreads();
-  double2* res = fft_lines<true>(bufa, bufb, kZinvLines, fz, twl);
+  double2* res = fft_lines<true>(bufa, bufb, nl, fz, twl);
   const int K1 = g.kx_max + 1;
-  for (int i = threadIdx.x; i < kZinvLines * pz; i += blockDim.x) {
+  for (int i = threadIdx.x; i < nl * pz; i += blockDim.x) {
     const int f = i / pz;
     const int z = i - f * pz;
     inter[(((size_t)f * g.ny + y) * K1 + kx) * pz + z] = res[i];
@@ -220,6 +227,162 @@ __global__ void k_xmid(Geo g, FftDesc fx, const double2* __restrict__ tw, const 
   __syncthreads();
   double2* other = (r == la) ? lb : la;
   for (int i = threadIdx.x; i < npt; i += blockDim.x) other[i] = make_double2(U[i], 0.0);
+  __syncthreads();
+  double2* scratch = (other == la) ? lb : la;
+  r = fft_lines<false>(other, scratch, ZB, fx, twl);
+  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
+    const int kx = i / ZB;
+    const int zl = i - kx * ZB;
+    const int z = z0 + zl;
+    if (z >= g.pz) continue;
+    out3[(((size_t)2 * g.ny + y) * K1 + kx) * g.pz + z] = r[zl * px + kx];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x pass with the adjoint products (navier_stokes_perturbation_dual.py:214-294,
+// lam = 1): dual state v, frozen forward state u, base U(y) e_x, Ut = U + u:
+//   hel_i = -(Ut . grad) v_i + sum_j v_j d_i Ut_j + [(div u) v_i + (div v) Ut_i] / 4
+// Intermediate lines 0..8 hold v (v, dv/dy, dv/dz), 9..17 the same for u.
+// ---------------------------------------------------------------------------
+template <int ZB>
+struct XmidDualSmem {
+  static size_t bytes(const Geo& g) {
+    return sizeof(double2) * ((size_t)g.px + 2 * (size_t)ZB * g.px) + sizeof(double) * 11 * (size_t)ZB * g.px;
+  }
+};
+
+template <int ZB>
+__global__ void k_xmid_dual(Geo g, FftDesc fx, const double2* __restrict__ tw, const double2* __restrict__ inter,
+                            double2* __restrict__ out3, const double* __restrict__ ubase,
+                            const double* __restrict__ dubase) {
+  extern __shared__ __align__(16) double2 xsm[];
+  const int px = g.px;
+  double2* twl = xsm;
+  double2* la = twl + px;
+  double2* lb = la + ZB * px;
+  double* V0 = reinterpret_cast<double*>(lb + ZB * px);
+  double* V1 = V0 + ZB * px;
+  double* V2 = V1 + ZB * px;
+  double* U0 = V2 + ZB * px;
+  double* U1 = U0 + ZB * px;
+  double* U2 = U1 + ZB * px;
+  double* A0 = U2 + ZB * px;
+  double* A1 = A0 + ZB * px;
+  double* A2 = A1 + ZB * px;
+  double* DV = A2 + ZB * px;
+  double* DU = DV + ZB * px;
+  const int z0 = blockIdx.x * ZB;
+  const int y = blockIdx.y;
+  const double ub = ubase[y];
+  const double dub = dubase[y];
+  const double c = g.c_inv;
+  const int npt = ZB * px;
+  load_twiddles(twl, tw, px);
+  double2* r;
+#define JSD_PAIR(fa, dxa, fb, dxb)                                  \
+  xmid_build<ZB>(g, la, inter, y, z0, fa, dxa, fb, dxb);            \
+  r = fft_lines<true>(la, lb, ZB, fx, twl);
+  // v, u components
+  JSD_PAIR(0, false, 1, false)
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) { V0[i] = r[i].x * c; V1[i] = r[i].y * c; }
+  __syncthreads();
+  JSD_PAIR(2, false, 9, false)
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) { V2[i] = r[i].x * c; U0[i] = r[i].y * c; }
+  __syncthreads();
+  JSD_PAIR(10, false, 11, false)
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) { U1[i] = r[i].x * c; U2[i] = r[i].y * c; }
+  __syncthreads();
+  // -(Ut . grad) v_i
+  JSD_PAIR(0, true, 1, true)  // dv0/dx, dv1/dx
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double ut = ub + U0[i];
+    const double a = r[i].x * c, b = r[i].y * c;
+    A0[i] = -ut * a;
+    A1[i] = -ut * b;
+    DV[i] = a;
+  }
+  __syncthreads();
+  JSD_PAIR(2, true, 3, false)  // dv2/dx, dv0/dy
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    A2[i] = -(ub + U0[i]) * (r[i].x * c);
+    A0[i] -= U1[i] * (r[i].y * c);
+  }
+  __syncthreads();
+  JSD_PAIR(4, false, 5, false)  // dv1/dy, dv2/dy
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double a = r[i].x * c, b = r[i].y * c;
+    A1[i] -= U1[i] * a;
+    A2[i] -= U1[i] * b;
+    DV[i] += a;
+  }
+  __syncthreads();
+  JSD_PAIR(6, false, 7, false)  // dv0/dz, dv1/dz
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    A0[i] -= U2[i] * (r[i].x * c);
+    A1[i] -= U2[i] * (r[i].y * c);
+  }
+  __syncthreads();
+  // + sum_j v_j d_i u_j
+  JSD_PAIR(8, false, 9, true)  // dv2/dz, du0/dx
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double a = r[i].x * c, b = r[i].y * c;
+    A2[i] -= U2[i] * a;
+    DV[i] += a;
+    A0[i] += V0[i] * b;
+    DU[i] = b;
+  }
+  __syncthreads();
+  JSD_PAIR(10, true, 11, true)  // du1/dx, du2/dx
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    A0[i] += V1[i] * (r[i].x * c) + V2[i] * (r[i].y * c);
+  }
+  __syncthreads();
+  JSD_PAIR(12, false, 13, false)  // du0/dy, du1/dy
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double a = r[i].x * c, b = r[i].y * c;
+    A1[i] += V0[i] * a + V1[i] * b;
+    DU[i] += b;
+  }
+  __syncthreads();
+  JSD_PAIR(14, false, 15, false)  // du2/dy, du0/dz
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    A1[i] += V2[i] * (r[i].x * c);
+    A2[i] += V0[i] * (r[i].y * c);
+  }
+  __syncthreads();
+  JSD_PAIR(16, false, 17, false)  // du1/dz, du2/dz
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double a = r[i].x * c, b = r[i].y * c;
+    A2[i] += V1[i] * a + V2[i] * b;
+    DU[i] += b;
+  }
+  __syncthreads();
+#undef JSD_PAIR
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
+    const double du = DU[i], dv = DV[i];
+    const double h0 = A0[i] + 0.25 * du * V0[i] + 0.25 * dv * (ub + U0[i]);
+    const double h1 = A1[i] + dub * V0[i] + 0.25 * du * V1[i] + 0.25 * dv * U1[i];
+    const double h2 = A2[i] + 0.25 * du * V2[i] + 0.25 * dv * U2[i];
+    la[i] = make_double2(h0, h1);
+    V0[i] = h2;
+  }
+  __syncthreads();
+  r = fft_lines<false>(la, lb, ZB, fx, twl);
+  const int K1 = g.kx_max + 1;
+  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
+    const int kx = i / ZB;
+    const int zl = i - kx * ZB;
+    const int z = z0 + zl;
+    if (z >= g.pz) continue;
+    const double2 a = r[zl * px + kx];
+    const double2 b = r[zl * px + (kx == 0 ? 0 : px - kx)];
+    out3[(((size_t)0 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+    out3[(((size_t)1 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.y + b.y), -0.5 * (a.x - b.x));
+  }
+  __syncthreads();
+  double2* other = (r == la) ? lb : la;
+  for (int i = threadIdx.x; i < npt; i += blockDim.x) other[i] = make_double2(V0[i], 0.0);
   __syncthreads();
   double2* scratch = (other == la) ? lb : la;
   r = fft_lines<false>(other, scratch, ZB, fx, twl);

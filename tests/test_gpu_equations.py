@@ -67,3 +67,13 @@ def test_dual_class_gradient(cuda):
     assert abs(dual.gain / float(d["gain"]) - 1) < TOL
     pg, ok = dual.get_projected_grad(1e-2)
     assert ok and bool(torch.isfinite(torch.view_as_real(pg)).all())
+
+
+def test_dual_class_nonlinear_gradient(cuda):
+    d = golden("dual_nonlin_9x33x9")
+    n, dt = int(d["n_steps"]), float(d["dt"])
+    nse = NavierStokesVelVortPerturbation(_vf(d), Re=float(d["re"]), dt=dt, end_time=n * dt, linearise=False)
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse)
+    grad = dual.get_grad()
+    assert rel(grad.cpu().numpy(), d["grad"]) < TOL
+    assert abs(dual.gain / float(d["gain"]) - 1) < TOL

@@ -153,3 +153,26 @@ def test_deterministic_and_finite_full_size(cuda):
     b, _, _ = _run(p, u0, 3, -1.0)
     assert torch.equal(a, b)
     assert bool(torch.isfinite(torch.view_as_real(a)).all())
+
+
+def test_dual_nonlinear_gradient(cuda):
+    """Nonlinear adjoint: the forward trajectory is registered with the plan
+    (jsd_set_history) and dual step t uses u(T - t) for all three stages."""
+    d = golden("dual_nonlin_9x33x9")
+    n, dt = int(d["n_steps"]), float(d["dt"])
+    fwd = _pert_plan(d["shape"], d["lengths"], d["re"], dt, False)
+    st = to_device_layout(d["u0"])
+    dp = torch.zeros(1, dtype=torch.float64, device="cuda")
+    traj = torch.empty((n + 1,) + tuple(st.shape), dtype=st.dtype, device=st.device)
+    traj[0].copy_(st)
+    for t in range(n):
+        fwd.step(st, dp, t, 1)
+        traj[t + 1].copy_(st)
+    e0 = fwd.energy(traj[0]).item()
+    dual = _pert_plan(d["shape"], d["lengths"], d["re"], dt, False, kind=2, dt_explicit=-dt)
+    dual.set_history(traj)
+    v = (-st).contiguous()
+    dual.step(v, dp, 0, n)
+    grad = (d["u0"] - to_reference_layout(v).cpu().numpy()) / e0
+    assert rel(grad, d["grad"]) < TOL
+    assert rel(to_reference_layout(st).cpu().numpy(), d["uT"]) < TOL
