@@ -111,6 +111,25 @@ int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* strea
  * 1468-1474). */
 int jsd_energy(jsd_plan* plan, const void* state, double* out, void* stream);
 
+/* Kinetic energy of a state without a plan and without allocating anything.
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory: code that runs under a host framework which has already reserved
+ * the GPU's memory for its own pool, or in-situ monitoring hooks inside a
+ * time loop that must not allocate or free (cudaMalloc/cudaFree can
+ * synchronise the device and fragment a long-running job's memory).
+ * The caller passes the state (layout as above), the grid, the reference
+ * physical grid sizes, the box lengths, the Ny Chebyshev integration weights
+ * (device array, field.py:2618-2650) and a device double for the result.
+ * Limit: ny <= 4096. The per-plane scratch is a fixed 32 KiB device array
+ * inside the library, held by every GPU that loads it until the process exits.
+ * The first call on a device looks up that array's address (with that device
+ * current); make that first call before any stream capture. All calls share
+ * the array, so calls that overlap on the GPU (e.g. on two streams) race;
+ * each call overwrites the entries it reads, so sequential calls need no
+ * clearing. Calls no cudaMalloc/cudaFree. */
+int jsd_energy_noalloc(const void* state, int mx, int ny, int mz, int px_ref, int pz_ref, double lx, double lz,
+                       const double* y_weights, double* out, void* stream);
+
 /* Flow rate Q = int u(x=0, y, z=0) dy of the streamwise component, written to
  * the device double `out`. Replaces NavierStokesVelVort.get_flow_rate
  * (navier_stokes.py:709-722). */

@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -445,9 +446,70 @@ void destroy(jsd_plan* p) {
   delete p;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free energy reduction. Its only scratch (one partial sum per
+// y-plane) is this file-scope device array: every GPU that loads the library
+// holds it until the process exits. In host code `g_static_partial` is a
+// host-side stand-in, not a device address; the device address is looked up
+// with cudaGetSymbolAddress once per device (with that device current) and
+// cached.
+// ---------------------------------------------------------------------------
+constexpr int kStaticMaxNy = 4096;
+static __device__ __align__(256) double g_static_partial[kStaticMaxNy];
+
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_static_mutex;
+double* g_static_partial_addr[kStaticMaxDevices] = {nullptr};
+
+int static_partial_address(double** out) {
+  int dev = -1;
+  JSD_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kStaticMaxDevices) return fail(JSD_ERR_ARG, "device ordinal out of range");
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (!g_static_partial_addr[dev]) {
+    void* ptr = nullptr;
+    JSD_CUDA(cudaGetSymbolAddress(&ptr, g_static_partial));
+    g_static_partial_addr[dev] = static_cast<double*>(ptr);
+  }
+  *out = g_static_partial_addr[dev];
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
+
+int jsd_energy_noalloc(const void* state, int mx, int ny, int mz, int px_ref, int pz_ref, double lx, double lz,
+                       const double* y_weights, double* out, void* stream) {
+  if (!state || !y_weights || !out) return fail(JSD_ERR_ARG, "null argument");
+  if (mx < 1 || mz < 1 || (mx % 2) == 0 || (mz % 2) == 0 || ny < 2 || px_ref < 1 || pz_ref < 1 || lx <= 0 ||
+      lz <= 0)
+    return fail(JSD_ERR_ARG, "invalid grid");
+  if (ny > kStaticMaxNy)
+    return fail(JSD_ERR_ARG, "jsd_energy_noalloc supports at most " + std::to_string(kStaticMaxNy) +
+                                 " Chebyshev points (got " + std::to_string(ny) + ")");
+  double* partial = nullptr;
+  int rc = static_partial_address(&partial);
+  if (rc) return rc;
+  Geo g{};
+  g.mx = mx;
+  g.ny = ny;
+  g.mz = mz;
+  g.kx_max = mx / 2;
+  g.kz_max = mz / 2;
+  g.nk = mx * mz;
+  const double two_pi = 2.0 * M_PI;
+  const double s = (lx / two_pi) * (lz / two_pi);
+  g.c_inv = s / std::sqrt((double)px_ref * (double)pz_ref);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  // k_plane_sums overwrites partial[0 .. ny) before k_weighted_total reads it,
+  // so nothing left by an earlier call is used
+  k_plane_sums<<<ny, 256, 0, st>>>(g, static_cast<const double2*>(state), 3, 0, partial);
+  JSD_LAUNCHED("k_plane_sums");
+  k_weighted_total<<<1, 32, 0, st>>>(ny, y_weights, partial, 0.25 * g.c_inv * g.c_inv, out);
+  JSD_LAUNCHED("k_weighted_total");
+  return 0;
+}
 
 int jsd_abi_version(void) { return JSD_ABI_VERSION; }
 

@@ -41,7 +41,7 @@ EXPORTED = (
     "jsd_plan_create", "jsd_plan_destroy", "jsd_step", "jsd_set_history",
     "jsd_correct_mass_flux", "jsd_energy", "jsd_flow_rate", "jsd_nonlinear_terms",
     "jsd_workspace_bytes", "jsd_launches_per_step", "jsd_last_error", "jsd_abi_version",
-    "jsd_profile_enable", "jsd_profile_read",
+    "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc",
 )
 
 PROF_CLASSES = {"gemm": 0, "zinv": 1, "xmid": 2, "zfwd": 3, "eigen": 4, "linear": 5}
@@ -76,6 +76,8 @@ def load(path: str = LIB_PATH):
     lib.jsd_workspace_bytes.restype = ctypes.c_size_t
     lib.jsd_launches_per_step.argtypes = [vp]
     lib.jsd_last_error.restype = ctypes.c_char_p
+    lib.jsd_energy_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_double, ctypes.c_double, vp, vp, vp]
     lib.jsd_profile_enable.argtypes = [vp, ctypes.c_int]
     lib.jsd_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
