@@ -308,16 +308,16 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
       }
     }
     const int nl = kZinvLines * nsets;
-    const size_t sm = sizeof(double2) * ((size_t)g.pz + 2 * (size_t)nl * g.pz);
+    const size_t sm = sizeof(double2) * ((size_t)g.pz + 2 * (size_t)nl * fline(g.pz));
     const double bytes = sizeof(double2) * (6.0 * nsets * fs + (double)nl * ny * K1 * g.pz);
     ProfScope ps(p, JSD_PROF_ZINV, bytes, s);
     k_zinv<<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, p->twz, src, p->inter);
     JSD_LAUNCHED("k_zinv");
   }
   if (dual) {
-    const size_t sm = XmidDualSmem<kXmidZB>::bytes(g);
+    const size_t sm = XmidSmem<kXmidZB>::bytes(g);
     ProfScope ps(p, JSD_PROF_XMID, sizeof(double2) * (double)(2 * kZinvLines + 3) * ny * K1 * g.pz, s);
-    k_xmid_dual<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), 256, sm, s>>>(
+    k_xmid_dual<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
         g, p->fx, p->twx, p->inter, p->out3, p->ub, p->dub);
     JSD_LAUNCHED("k_xmid_dual");
   } else {
@@ -325,12 +325,12 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
     ProfScope ps(p, JSD_PROF_XMID, sizeof(double2) * (double)(kZinvLines + 3) * ny * K1 * g.pz, s);
     const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
     const bool pert = p->desc.kind == JSD_KIND_PERTURBATION;
-    k_xmid<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), 256, sm, s>>>(
+    k_xmid<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
         g, p->fx, p->twx, p->inter, p->out3, pert ? p->ub : nullptr, pert ? p->dub : nullptr, lam);
     JSD_LAUNCHED("k_xmid");
   }
   {
-    const size_t sm = sizeof(double2) * 7 * (size_t)g.pz;
+    const size_t sm = sizeof(double2) * ((size_t)g.pz + 6 * (size_t)fline(g.pz));
     ProfScope ps(p, JSD_PROF_ZFWD, sizeof(double2) * (3.0 * ny * K1 * g.pz + 3.0 * fs), s);
     k_zfwd<<<dim3(K1, ny), 128, sm, s>>>(g, p->fz, p->twz, p->out3, p->q, p->H1, p->hg, conv);
     JSD_LAUNCHED("k_zfwd");
@@ -378,7 +378,7 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     const size_t E = p->edoubles;
     // reads X1, 4 transformed fields, 2 old terms; writes 2 old terms, v~ twice, om~
     ProfScope ps(p, JSD_PROF_EIGEN, sizeof(double) * 13.0 * (double)E, s);
-    k_eigen_update<<<(N + 127) / 128, 128, 0, s>>>(g, t, sc, p->X1, p->T, p->T + E, p->T + 2 * E, p->T + 3 * E,
+    k_eigen_update<<<(N + kEigCols - 1) / kEigCols, kEigCols * kEigParts, 0, s>>>(g, t, sc, p->X1, p->T, p->T + E, p->T + 2 * E, p->T + 3 * E,
                                                    (const double*)v, p->hv_old, p->hg_old, p->vnt, p->omnt);
     JSD_LAUNCHED("k_eigen_update");
   }
@@ -389,7 +389,7 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     const double2* conv = p->conv + (size_t)st * 2 * ny;
     const double2* conv_old = st == 0 ? nullptr : p->conv + (size_t)(st - 1) * 2 * ny;
     const double dte = p->desc.dt_explicit;
-    k_mean_flow<<<1, 256, sizeof(double2) * 2 * n2, s>>>(g, rns, lns, u, w, conv, conv_old, dpdx, p->dpdx_scale,
+    k_mean_flow<<<1, kMeanFlowThreads, sizeof(double2) * 2 * n2, s>>>(g, rns, lns, u, w, conv, conv_old, dpdx, p->dpdx_scale,
                                                         dte * kGamma[st], dte * kXi[st], p->uw00);
     JSD_LAUNCHED("k_mean_flow");
   }
@@ -591,6 +591,11 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   g.c_fwd = std::sqrt((double)d->px_ref * (double)d->pz_ref) / (s * (double)g.px * (double)g.pz);
   p->dpdx_scale = std::sqrt(((double)d->px_ref * (two_pi / d->lx) * (two_pi / d->lx)) *
                             ((double)d->pz_ref * (two_pi / d->lz) * (two_pi / d->lz)));
+  if ((size_t)kXmidZB * g.px > (size_t)kXmidEPT * kXmidThreads) {
+    destroy(p);
+    return fail(JSD_ERR_ARG, "x FFT length too large for the x-pass kernel (max " +
+                                 std::to_string(kXmidEPT * kXmidThreads / kXmidZB) + ")");
+  }
   if (g.px < 3 * g.kx_max + 1 || g.pz < 3 * g.kz_max + 1) {
     destroy(p);
     return fail(JSD_ERR_ARG, "FFT length below 3K+1 would alias the quadratic products");

@@ -24,6 +24,11 @@ struct FftDesc {
   int twoff[kMaxFftPasses];
 };
 
+// Lines are stored with one padding slot after every 32 complex elements so
+// the strided Stockham writes spread over all shared-memory banks.
+__host__ __device__ __forceinline__ int fpad(int i) { return i + (i >> 5); }
+__host__ __device__ __forceinline__ int fline(int n) { return n + (n >> 5) + 1; }
+
 // cos(2 pi m / R) and sin(2 pi m / R) for R = 3, 5, 7 (m = 0..R-1)
 __device__ __forceinline__ void root_table(int r, int m, double& c, double& s) {
   if (r == 3) {
@@ -45,22 +50,40 @@ __device__ __forceinline__ void root_table(int r, int m, double& c, double& s) {
   }
 }
 
-// generic odd-radix DFT: y[q] = sum_t x[t] exp(-+2 pi i q t / R)
+// Odd-radix DFT in conjugate-pair form: with a_t = x_t + x_{R-t} and
+// b_t = x_t - x_{R-t} (t = 1..h, h = (R-1)/2),
+//   y[q]   = x_0 + sum_t a_t cos(2 pi q t / R) -+ i sum_t b_t sin(2 pi q t / R)
+//   y[R-q] = x_0 + sum_t a_t cos(2 pi q t / R) +- i sum_t b_t sin(2 pi q t / R)
+// (upper signs forward), h^2 complex-by-real products per half instead of R^2.
 template <int R, bool INV>
 __device__ __forceinline__ void dft_odd(double2* x) {
+  constexpr int H = (R - 1) / 2;
+  double2 a[H], b[H];
+  double2 y0 = x[0];
+#pragma unroll
+  for (int t = 1; t <= H; ++t) {
+    a[t - 1] = cadd(x[t], x[R - t]);
+    b[t - 1] = csub(x[t], x[R - t]);
+    y0 = cadd(y0, a[t - 1]);
+  }
   double2 y[R];
+  y[0] = y0;
 #pragma unroll
-  for (int q = 0; q < R; ++q) {
-    double2 acc = x[0];
+  for (int q = 1; q <= H; ++q) {
+    double2 re = x[0], im = make_double2(0.0, 0.0);
 #pragma unroll
-    for (int t = 1; t < R; ++t) {
-      double c, s;
-      root_table(R, (q * t) % R, c, s);
-      const double si = INV ? s : -s;
-      acc.x += x[t].x * c - x[t].y * si;
-      acc.y += x[t].x * si + x[t].y * c;
+    for (int t = 1; t <= H; ++t) {
+      double c, sn;
+      root_table(R, (q * t) % R, c, sn);
+      re.x += a[t - 1].x * c;
+      re.y += a[t - 1].y * c;
+      im.x += b[t - 1].x * sn;
+      im.y += b[t - 1].y * sn;
     }
-    y[q] = acc;
+    // i * im = (-im.y, im.x)
+    const double2 iim = make_double2(-im.y, im.x);
+    y[q] = INV ? cadd(re, iim) : csub(re, iim);
+    y[R - q] = INV ? csub(re, iim) : cadd(re, iim);
   }
 #pragma unroll
   for (int q = 0; q < R; ++q) x[q] = y[q];
@@ -117,14 +140,15 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ src, double
                                          int n, int ls, const double2* __restrict__ tw) {
   const int m = n / R;
   const int total = nlines * m;
+  const int stride = fline(n);
   for (int task = threadIdx.x; task < total; task += blockDim.x) {
     const int l = task / m;
     const int j = task - l * m;
     const int k = j % ls;
-    const double2* s = src + (size_t)l * n;
+    const double2* s = src + (size_t)l * stride;
     double2 x[R];
 #pragma unroll
-    for (int t = 0; t < R; ++t) x[t] = s[j + t * m];
+    for (int t = 0; t < R; ++t) x[t] = s[fpad(j + t * m)];
     if (ls > 1) {
 #pragma unroll
       for (int t = 1; t < R; ++t) {
@@ -137,14 +161,15 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ src, double
     else if constexpr (R == 4) dft4<INV>(x);
     else if constexpr (R == 8) dft8<INV>(x);
     else dft_odd<R, INV>(x);
-    double2* o = dst + (size_t)l * n + (j / ls) * ls * R + k;
+    double2* o = dst + (size_t)l * stride;
+    const int base = (j / ls) * ls * R + k;
 #pragma unroll
-    for (int t = 0; t < R; ++t) o[t * ls] = x[t];
+    for (int t = 0; t < R; ++t) o[fpad(base + t * ls)] = x[t];
   }
 }
 
-// Transform nlines contiguous lines of length d.n starting at a; b is scratch
-// of the same size. Returns the buffer that holds the result. Must be called
+// Transform nlines lines of length d.n (line l at a + l * fline(n), element i
+// at fpad(i)) starting at a; b is scratch of the same size. Returns the buffer that holds the result. Must be called
 // by all threads of the block; ends with a barrier.
 template <bool INV>
 __device__ double2* fft_lines(double2* a, double2* b, int nlines, const FftDesc& d, const double2* __restrict__ tw) {

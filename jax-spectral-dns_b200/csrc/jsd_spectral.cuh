@@ -44,25 +44,26 @@ __global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, ZinvSr
                        double2* __restrict__ inter) {
   extern __shared__ __align__(16) double2 zsm[];
   const int pz = g.pz;
+  const int L = fline(pz);
   const int nl = kZinvLines * src.nsets;
   double2* twl = zsm;
   double2* bufa = twl + pz;
-  double2* bufb = bufa + nl * pz;
+  double2* bufb = bufa + nl * L;
   const int kx = blockIdx.x;
   const int y = blockIdx.y;
   load_twiddles(twl, tw, pz);
-  for (int i = threadIdx.x; i < nl * pz; i += blockDim.x) bufa[i] = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < nl * L; i += blockDim.x) bufa[i] = make_double2(0.0, 0.0);
   __syncthreads();
   for (int i = threadIdx.x; i < 6 * src.nsets * g.mz; i += blockDim.x) {
-    const int f = i / g.mz;        // input index 0 .. 6 nsets - 1
+    const int f = i / g.mz;  // input index 0 .. 6 nsets - 1
     const int iz = i - f * g.mz;
     const int set = f / 6, fi = f - set * 6;
     const int kz = signed_mode(iz, g.mz);
     const double2 sv = sym_at(g, src.f[f], y, kx, kz);
-    const int pos = kz >= 0 ? kz : pz + kz;
-    double2* lines = bufa + (size_t)set * kZinvLines * pz;
-    lines[fi * pz + pos] = sv;
-    if (fi < 3) lines[(6 + fi) * pz + pos] = cmul_ik(sv, kz * g.az);
+    const int pos = fpad(kz >= 0 ? kz : pz + kz);
+    double2* lines = bufa + (size_t)set * kZinvLines * L;
+    lines[fi * L + pos] = sv;
+    if (fi < 3) lines[(6 + fi) * L + pos] = cmul_ik(sv, kz * g.az);
   }
   __syncthreads();
   double2* res = fft_lines<true>(bufa, bufb, nl, fz, twl);
@@ -70,7 +71,7 @@ __global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, ZinvSr
   for (int i = threadIdx.x; i < nl * pz; i += blockDim.x) {
     const int f = i / pz;
     const int z = i - f * pz;
-    inter[(((size_t)f * g.ny + y) * K1 + kx) * pz + z] = res[i];
+    inter[(((size_t)f * g.ny + y) * K1 + kx) * pz + z] = res[f * L + fpad(z)];
   }
 }
 
@@ -79,6 +80,9 @@ __global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, ZinvSr
 // Pairs of real fields are packed as a + i b into one complex line of length
 // px whose spectrum is A[k] + i B[k] (k >= 0) and conj(A[k]) + i conj(B[k])
 // at px - k; the inverse FFT returns a in the real and b in the imaginary part.
+// Two pairs (2 ZB lines) go through each FFT batch. Every thread owns the same
+// physical points in every batch (point i = threadIdx.x + e * blockDim.x), so
+// the per-point fields and product accumulators stay in registers.
 //
 // Skew-symmetric convective term (lam = 1 for the full equations, 0 when
 // linearised) plus the base-flow coupling of the perturbation equations with
@@ -86,56 +90,95 @@ __global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, ZinvSr
 //   hel_i = -lam (u . grad) u_i + lam/2 (div u) u_i - U d_x u_i
 //           - delta_i0 (v U' - (div u) U / 2)
 // ---------------------------------------------------------------------------
+constexpr int kXmidThreads = 256;
+constexpr int kXmidEPT = 4;  // points per thread: ZB * px <= kXmidEPT * kXmidThreads
+
 template <int ZB>
 struct XmidSmem {
   static size_t bytes(const Geo& g) {
-    return sizeof(double2) * ((size_t)g.px + 2 * (size_t)ZB * g.px) + sizeof(double) * 7 * (size_t)ZB * g.px;
+    return sizeof(double2) * ((size_t)g.px + 2 * 2 * (size_t)ZB * fline(g.px));
   }
 };
 
+__device__ __forceinline__ void zero_lines(double2* line, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) line[i] = make_double2(0.0, 0.0);
+}
+
+// Write ZB complete packed lines (zeros included) for fields (fa, fb) of the ZB
+// columns starting at `line` (no barrier). Threads run x-major over (x, zl) so
+// neighbouring threads read neighbouring z of one kx row of the intermediate.
 template <int ZB>
-__device__ __forceinline__ void xmid_build(const Geo& g, double2* line, const double2* __restrict__ inter, int y, int z0,
-                                           int fa, bool dxa, int fb, bool dxb) {
-  const int px = g.px, K1 = g.kx_max + 1;
-  for (int i = threadIdx.x; i < ZB * px; i += blockDim.x) line[i] = make_double2(0.0, 0.0);
-  __syncthreads();
+__device__ __forceinline__ void fill_pair(const Geo& g, double2* line, const double2* __restrict__ inter, int y, int z0,
+                                          int fa, bool dxa, int fb, bool dxb) {
+  const int px = g.px, K = g.kx_max, K1 = K + 1, L = fline(px);
+  for (int i = threadIdx.x; i < ZB * px; i += blockDim.x) {
+    const int x = i / ZB;
+    const int zl = i - x * ZB;
+    const int z = z0 + zl;
+    double2 out = make_double2(0.0, 0.0);
+    const bool lo = x <= K, hi = x >= px - K;
+    if ((lo || hi) && z < g.pz) {
+      const int kx = lo ? x : px - x;
+      double2 A = inter[(((size_t)fa * g.ny + y) * K1 + kx) * g.pz + z];
+      double2 B = inter[(((size_t)fb * g.ny + y) * K1 + kx) * g.pz + z];
+      const double k = kx * g.ax;
+      if (dxa) A = cmul_ik(A, k);
+      if (dxb) B = cmul_ik(B, k);
+      if (x == 0) out = make_double2(A.x, B.x);
+      else if (lo) out = make_double2(A.x - B.y, A.y + B.x);
+      else out = make_double2(A.x + B.y, B.x - A.y);
+    }
+    line[zl * L + fpad(x)] = out;
+  }
+}
+
+// fill a batch of two pairs (2 ZB lines); no barrier
+template <int ZB>
+__device__ __forceinline__ void fill_two_pairs(const Geo& g, double2* la, const double2* __restrict__ inter, int y,
+                                               int z0, int fa1, bool dxa1, int fb1, bool dxb1, int fa2, bool dxa2,
+                                               int fb2, bool dxb2) {
+  fill_pair<ZB>(g, la, inter, y, z0, fa1, dxa1, fb1, dxb1);
+  fill_pair<ZB>(g, la + ZB * fline(g.px), inter, y, z0, fa2, dxa2, fb2, dxb2);
+}
+
+// value of point i (line zl = i / px, position x) of pair set `set` in r
+__device__ __forceinline__ double2 pair_value(const double2* r, int set, int zb, int px, int i) {
+  const int L = fline(px);
+  const int zl = i / px;
+  const int x = i - zl * px;
+  return r[(set * zb + zl) * L + fpad(x)];
+}
+
+// forward FFT of (h0 + i h1) and (h2 + 0 i) lines and the kx >= 0 outputs
+template <int ZB>
+__device__ __forceinline__ void forward_and_store(const Geo& g, const FftDesc& fx, const double2* twl, double2* la,
+                                                  double2* lb, double2* __restrict__ out3, int y, int z0) {
+  const int px = g.px, L = fline(px), K1 = g.kx_max + 1;
+  double2* r = fft_lines<false>(la, lb, 2 * ZB, fx, twl);
   for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
     const int kx = i / ZB;
     const int zl = i - kx * ZB;
     const int z = z0 + zl;
     if (z >= g.pz) continue;
-    double2 A = inter[(((size_t)fa * g.ny + y) * K1 + kx) * g.pz + z];
-    double2 B = inter[(((size_t)fb * g.ny + y) * K1 + kx) * g.pz + z];
-    const double k = kx * g.ax;
-    if (dxa) A = cmul_ik(A, k);
-    if (dxb) B = cmul_ik(B, k);
-    double2* l = line + zl * px;
-    if (kx == 0) {
-      l[0] = make_double2(A.x, B.x);
-    } else {
-      l[kx] = make_double2(A.x - B.y, A.y + B.x);
-      l[px - kx] = make_double2(A.x + B.y, B.x - A.y);
-    }
+    const double2 a = r[zl * L + fpad(kx)];
+    const double2 b = r[zl * L + fpad(kx == 0 ? 0 : px - kx)];
+    // H0 = (Z[k] + conj Z[-k]) / 2, H1 = (Z[k] - conj Z[-k]) / (2 i)
+    out3[(((size_t)0 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
+    out3[(((size_t)1 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.y + b.y), -0.5 * (a.x - b.x));
+    out3[(((size_t)2 * g.ny + y) * K1 + kx) * g.pz + z] = r[(ZB + zl) * L + fpad(kx)];
   }
-  __syncthreads();
 }
 
 template <int ZB>
-__global__ void k_xmid(Geo g, FftDesc fx, const double2* __restrict__ tw, const double2* __restrict__ inter,
-                       double2* __restrict__ out3, const double* __restrict__ ubase,
-                       const double* __restrict__ dubase, double lam) {
+__global__ void __launch_bounds__(kXmidThreads) k_xmid(Geo g, FftDesc fx, const double2* __restrict__ tw,
+                                                       const double2* __restrict__ inter, double2* __restrict__ out3,
+                                                       const double* __restrict__ ubase,
+                                                       const double* __restrict__ dubase, double lam) {
   extern __shared__ __align__(16) double2 xsm[];
-  const int px = g.px;
+  const int px = g.px, L = fline(px);
   double2* twl = xsm;
   double2* la = twl + px;
-  double2* lb = la + ZB * px;
-  double* U = reinterpret_cast<double*>(lb + ZB * px);
-  double* V = U + ZB * px;
-  double* W = V + ZB * px;
-  double* DIV = W + ZB * px;
-  double* A0 = DIV + ZB * px;
-  double* A1 = A0 + ZB * px;
-  double* A2 = A1 + ZB * px;
+  double2* lb = la + 2 * ZB * L;
   const int z0 = blockIdx.x * ZB;
   const int y = blockIdx.y;
   const double ub = ubase ? ubase[y] : 0.0;
@@ -143,100 +186,70 @@ __global__ void k_xmid(Geo g, FftDesc fx, const double2* __restrict__ tw, const 
   const double c = g.c_inv;
   const int npt = ZB * px;
   load_twiddles(twl, tw, px);
+  double U[kXmidEPT], V[kXmidEPT], W[kXmidEPT], DIV[kXmidEPT], A0[kXmidEPT], A1[kXmidEPT], A2[kXmidEPT];
 
-  // fields in the intermediate: 0 u, 1 v, 2 w, 3 du/dy, 4 dv/dy, 5 dw/dy, 6 du/dz, 7 dv/dz, 8 dw/dz
-  // pair 0: (u, v)
-  xmid_build<ZB>(g, la, inter, y, z0, 0, false, 1, false);
-  double2* r = fft_lines<true>(la, lb, ZB, fx, twl);
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    U[i] = r[i].x * c;
-    V[i] = r[i].y * c;
+  // intermediate: 0 u, 1 v, 2 w, 3 du/dy, 4 dv/dy, 5 dw/dy, 6 du/dz, 7 dv/dz, 8 dw/dz
+  // Batches of two pairs; consuming batch b overlaps filling batch b + 1 when
+  // the FFT result sits in lb (odd number of passes).
+  fill_two_pairs<ZB>(g, la, inter, y, z0, 0, false, 1, false, 2, false, 0, true);
+  __syncthreads();
+  double2* r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
+#pragma unroll
+  for (int e = 0; e < kXmidEPT; ++e) {
+    const int i = threadIdx.x + e * blockDim.x;
+    if (i >= npt) break;
+    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
+    U[e] = p.x * c;
+    V[e] = p.y * c;
+    W[e] = q.x * c;
+    const double dxu = q.y * c;
+    DIV[e] = dxu;
+    A0[e] = lam * U[e] * dxu + ub * dxu;
+  }
+  if (r == la) __syncthreads();
+  fill_two_pairs<ZB>(g, la, inter, y, z0, 4, false, 8, false, 1, true, 2, true);
+  __syncthreads();
+  r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
+#pragma unroll
+  for (int e = 0; e < kXmidEPT; ++e) {
+    const int i = threadIdx.x + e * blockDim.x;
+    if (i >= npt) break;
+    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
+    const double dyv = p.x * c, dzw = p.y * c, dxv = q.x * c, dxw = q.y * c;
+    DIV[e] += dyv + dzw;
+    A1[e] = lam * V[e] * dyv + lam * U[e] * dxv + ub * dxv;
+    A2[e] = lam * W[e] * dzw + lam * U[e] * dxw + ub * dxw;
+  }
+  if (r == la) __syncthreads();
+  fill_two_pairs<ZB>(g, la, inter, y, z0, 3, false, 5, false, 6, false, 7, false);
+  __syncthreads();
+  r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
+#pragma unroll
+  for (int e = 0; e < kXmidEPT; ++e) {
+    const int i = threadIdx.x + e * blockDim.x;
+    if (i >= npt) break;
+    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
+    const double dyu = p.x * c, dyw = p.y * c, dzu = q.x * c, dzv = q.y * c;
+    A0[e] += lam * V[e] * dyu + lam * W[e] * dzu;
+    A2[e] += lam * V[e] * dyw;
+    A1[e] += lam * W[e] * dzv;
+  }
+  if (r == la) __syncthreads();
+  // products packed as (hel0 + i hel1) and (hel2 + 0 i)
+#pragma unroll
+  for (int e = 0; e < kXmidEPT; ++e) {
+    const int i = threadIdx.x + e * blockDim.x;
+    if (i >= npt) break;
+    const double d = DIV[e];
+    const double h0 = -A0[e] + 0.5 * lam * d * U[e] - V[e] * dub + 0.5 * d * ub;
+    const double h1 = -A1[e] + 0.5 * lam * d * V[e];
+    const double h2 = -A2[e] + 0.5 * lam * d * W[e];
+    const int zl = i / px, x = i - zl * px;
+    la[zl * L + fpad(x)] = make_double2(h0, h1);
+    la[(ZB + zl) * L + fpad(x)] = make_double2(h2, 0.0);
   }
   __syncthreads();
-  // pair 1: (w, du/dx)
-  xmid_build<ZB>(g, la, inter, y, z0, 2, false, 0, true);
-  r = fft_lines<true>(la, lb, ZB, fx, twl);
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double wv = r[i].x * c, dxu = r[i].y * c;
-    W[i] = wv;
-    DIV[i] = dxu;
-    A0[i] = lam * U[i] * dxu + ub * dxu;
-  }
-  __syncthreads();
-  // pair 2: (dv/dy, dw/dz)
-  xmid_build<ZB>(g, la, inter, y, z0, 4, false, 8, false);
-  r = fft_lines<true>(la, lb, ZB, fx, twl);
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double dyv = r[i].x * c, dzw = r[i].y * c;
-    DIV[i] += dyv + dzw;
-    A1[i] = lam * V[i] * dyv;
-    A2[i] = lam * W[i] * dzw;
-  }
-  __syncthreads();
-  // pair 3: (dv/dx, dw/dx)
-  xmid_build<ZB>(g, la, inter, y, z0, 1, true, 2, true);
-  r = fft_lines<true>(la, lb, ZB, fx, twl);
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double dxv = r[i].x * c, dxw = r[i].y * c;
-    A1[i] += lam * U[i] * dxv + ub * dxv;
-    A2[i] += lam * U[i] * dxw + ub * dxw;
-  }
-  __syncthreads();
-  // pair 4: (du/dy, dw/dy)
-  xmid_build<ZB>(g, la, inter, y, z0, 3, false, 5, false);
-  r = fft_lines<true>(la, lb, ZB, fx, twl);
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    A0[i] += lam * V[i] * (r[i].x * c);
-    A2[i] += lam * V[i] * (r[i].y * c);
-  }
-  __syncthreads();
-  // pair 5: (du/dz, dv/dz)
-  xmid_build<ZB>(g, la, inter, y, z0, 6, false, 7, false);
-  r = fft_lines<true>(la, lb, ZB, fx, twl);
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    A0[i] += lam * W[i] * (r[i].x * c);
-    A1[i] += lam * W[i] * (r[i].y * c);
-  }
-  __syncthreads();
-  // final products, packed (hel0 + i hel1) and (hel2 + 0 i) for the forward FFTs
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double d = DIV[i];
-    const double h0 = -A0[i] + 0.5 * lam * d * U[i] - V[i] * dub + 0.5 * d * ub;
-    const double h1 = -A1[i] + 0.5 * lam * d * V[i];
-    const double h2 = -A2[i] + 0.5 * lam * d * W[i];
-    la[i] = make_double2(h0, h1);
-    U[i] = h2;
-  }
-  __syncthreads();
-  r = fft_lines<false>(la, lb, ZB, fx, twl);
-  const int K1 = g.kx_max + 1;
-  // unpack H0, H1 for kx = 0..K
-  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
-    const int kx = i / ZB;
-    const int zl = i - kx * ZB;
-    const int z = z0 + zl;
-    if (z >= g.pz) continue;
-    const double2 a = r[zl * px + kx];
-    const double2 b = r[zl * px + (kx == 0 ? 0 : px - kx)];
-    // H0 = (Z[k] + conj Z[-k]) / 2, H1 = (Z[k] - conj Z[-k]) / (2 i)
-    const double2 h0 = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
-    const double2 h1 = make_double2(0.5 * (a.y + b.y), -0.5 * (a.x - b.x));
-    out3[(((size_t)0 * g.ny + y) * K1 + kx) * g.pz + z] = h0;
-    out3[(((size_t)1 * g.ny + y) * K1 + kx) * g.pz + z] = h1;
-  }
-  __syncthreads();
-  double2* other = (r == la) ? lb : la;
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) other[i] = make_double2(U[i], 0.0);
-  __syncthreads();
-  double2* scratch = (other == la) ? lb : la;
-  r = fft_lines<false>(other, scratch, ZB, fx, twl);
-  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
-    const int kx = i / ZB;
-    const int zl = i - kx * ZB;
-    const int z = z0 + zl;
-    if (z >= g.pz) continue;
-    out3[(((size_t)2 * g.ny + y) * K1 + kx) * g.pz + z] = r[zl * px + kx];
-  }
+  forward_and_store<ZB>(g, fx, twl, la, lb, out3, y, z0);
 }
 
 // ---------------------------------------------------------------------------
@@ -246,32 +259,16 @@ __global__ void k_xmid(Geo g, FftDesc fx, const double2* __restrict__ tw, const 
 // Intermediate lines 0..8 hold v (v, dv/dy, dv/dz), 9..17 the same for u.
 // ---------------------------------------------------------------------------
 template <int ZB>
-struct XmidDualSmem {
-  static size_t bytes(const Geo& g) {
-    return sizeof(double2) * ((size_t)g.px + 2 * (size_t)ZB * g.px) + sizeof(double) * 11 * (size_t)ZB * g.px;
-  }
-};
-
-template <int ZB>
-__global__ void k_xmid_dual(Geo g, FftDesc fx, const double2* __restrict__ tw, const double2* __restrict__ inter,
-                            double2* __restrict__ out3, const double* __restrict__ ubase,
-                            const double* __restrict__ dubase) {
+__global__ void __launch_bounds__(kXmidThreads) k_xmid_dual(Geo g, FftDesc fx, const double2* __restrict__ tw,
+                                                            const double2* __restrict__ inter,
+                                                            double2* __restrict__ out3,
+                                                            const double* __restrict__ ubase,
+                                                            const double* __restrict__ dubase) {
   extern __shared__ __align__(16) double2 xsm[];
-  const int px = g.px;
+  const int px = g.px, L = fline(px);
   double2* twl = xsm;
   double2* la = twl + px;
-  double2* lb = la + ZB * px;
-  double* V0 = reinterpret_cast<double*>(lb + ZB * px);
-  double* V1 = V0 + ZB * px;
-  double* V2 = V1 + ZB * px;
-  double* U0 = V2 + ZB * px;
-  double* U1 = U0 + ZB * px;
-  double* U2 = U1 + ZB * px;
-  double* A0 = U2 + ZB * px;
-  double* A1 = A0 + ZB * px;
-  double* A2 = A1 + ZB * px;
-  double* DV = A2 + ZB * px;
-  double* DU = DV + ZB * px;
+  double2* lb = la + 2 * ZB * L;
   const int z0 = blockIdx.x * ZB;
   const int y = blockIdx.y;
   const double ub = ubase[y];
@@ -279,120 +276,58 @@ __global__ void k_xmid_dual(Geo g, FftDesc fx, const double2* __restrict__ tw, c
   const double c = g.c_inv;
   const int npt = ZB * px;
   load_twiddles(twl, tw, px);
-  double2* r;
-#define JSD_PAIR(fa, dxa, fb, dxb)                                  \
-  xmid_build<ZB>(g, la, inter, y, z0, fa, dxa, fb, dxb);            \
-  r = fft_lines<true>(la, lb, ZB, fx, twl);
-  // v, u components
-  JSD_PAIR(0, false, 1, false)
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) { V0[i] = r[i].x * c; V1[i] = r[i].y * c; }
-  __syncthreads();
-  JSD_PAIR(2, false, 9, false)
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) { V2[i] = r[i].x * c; U0[i] = r[i].y * c; }
-  __syncthreads();
-  JSD_PAIR(10, false, 11, false)
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) { U1[i] = r[i].x * c; U2[i] = r[i].y * c; }
-  __syncthreads();
-  // -(Ut . grad) v_i
-  JSD_PAIR(0, true, 1, true)  // dv0/dx, dv1/dx
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double ut = ub + U0[i];
-    const double a = r[i].x * c, b = r[i].y * c;
-    A0[i] = -ut * a;
-    A1[i] = -ut * b;
-    DV[i] = a;
+  double V0[kXmidEPT], V1[kXmidEPT], V2[kXmidEPT], U0[kXmidEPT], U1[kXmidEPT], U2[kXmidEPT];
+  double A0[kXmidEPT], A1[kXmidEPT], A2[kXmidEPT], DV[kXmidEPT], DU[kXmidEPT];
+#define JSD_EACH(body)                                                        \
+  _Pragma("unroll") for (int e = 0; e < kXmidEPT; ++e) {                      \
+    const int i = threadIdx.x + e * blockDim.x;                               \
+    if (i >= npt) break;                                                      \
+    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i); \
+    const double pa = p.x * c, pb = p.y * c, qa = q.x * c, qb = q.y * c;      \
+    body                                                                      \
+  }                                                                           \
+  if (r == la) __syncthreads();
+#define JSD_BATCH(fa1, dxa1, fb1, dxb1, fa2, dxa2, fb2, dxb2)                   \
+  fill_two_pairs<ZB>(g, la, inter, y, z0, fa1, dxa1, fb1, dxb1, fa2, dxa2, fb2, dxb2); \
+  __syncthreads();                                                            \
+  r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
+  // (v0, v1) + (v2, u0)
+  double2* r = la;
+  JSD_BATCH(0, false, 1, false, 2, false, 9, false)
+  JSD_EACH(V0[e] = pa; V1[e] = pb; V2[e] = qa; U0[e] = qb;)
+  // (u1, u2) + (dv0/dx, dv1/dx)
+  JSD_BATCH(10, false, 11, false, 0, true, 1, true)
+  JSD_EACH(U1[e] = pa; U2[e] = pb; const double ut = ub + U0[e]; A0[e] = -ut * qa; A1[e] = -ut * qb; DV[e] = qa;)
+  // (dv2/dx, dv0/dy) + (dv1/dy, dv2/dy)
+  JSD_BATCH(2, true, 3, false, 4, false, 5, false)
+  JSD_EACH(A2[e] = -(ub + U0[e]) * pa; A0[e] -= U1[e] * pb; A1[e] -= U1[e] * qa; A2[e] -= U1[e] * qb;
+           DV[e] += qa;)
+  // (dv0/dz, dv1/dz) + (dv2/dz, du0/dx)
+  JSD_BATCH(6, false, 7, false, 8, false, 9, true)
+  JSD_EACH(A0[e] -= U2[e] * pa; A1[e] -= U2[e] * pb; A2[e] -= U2[e] * qa; DV[e] += qa; A0[e] += V0[e] * qb;
+           DU[e] = qb;)
+  // (du1/dx, du2/dx) + (du0/dy, du1/dy)
+  JSD_BATCH(10, true, 11, true, 12, false, 13, false)
+  JSD_EACH(A0[e] += V1[e] * pa + V2[e] * pb; A1[e] += V0[e] * qa + V1[e] * qb; DU[e] += qb;)
+  // (du2/dy, du0/dz) + (du1/dz, du2/dz)
+  JSD_BATCH(14, false, 15, false, 16, false, 17, false)
+  JSD_EACH(A1[e] += V2[e] * pa; A2[e] += V0[e] * pb + V1[e] * qa + V2[e] * qb; DU[e] += qb;)
+#undef JSD_EACH
+#undef JSD_BATCH
+#pragma unroll
+  for (int e = 0; e < kXmidEPT; ++e) {
+    const int i = threadIdx.x + e * blockDim.x;
+    if (i >= npt) break;
+    const double du = DU[e], dv = DV[e];
+    const double h0 = A0[e] + 0.25 * du * V0[e] + 0.25 * dv * (ub + U0[e]);
+    const double h1 = A1[e] + dub * V0[e] + 0.25 * du * V1[e] + 0.25 * dv * U1[e];
+    const double h2 = A2[e] + 0.25 * du * V2[e] + 0.25 * dv * U2[e];
+    const int zl = i / px, x = i - zl * px;
+    la[zl * L + fpad(x)] = make_double2(h0, h1);
+    la[(ZB + zl) * L + fpad(x)] = make_double2(h2, 0.0);
   }
   __syncthreads();
-  JSD_PAIR(2, true, 3, false)  // dv2/dx, dv0/dy
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    A2[i] = -(ub + U0[i]) * (r[i].x * c);
-    A0[i] -= U1[i] * (r[i].y * c);
-  }
-  __syncthreads();
-  JSD_PAIR(4, false, 5, false)  // dv1/dy, dv2/dy
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double a = r[i].x * c, b = r[i].y * c;
-    A1[i] -= U1[i] * a;
-    A2[i] -= U1[i] * b;
-    DV[i] += a;
-  }
-  __syncthreads();
-  JSD_PAIR(6, false, 7, false)  // dv0/dz, dv1/dz
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    A0[i] -= U2[i] * (r[i].x * c);
-    A1[i] -= U2[i] * (r[i].y * c);
-  }
-  __syncthreads();
-  // + sum_j v_j d_i u_j
-  JSD_PAIR(8, false, 9, true)  // dv2/dz, du0/dx
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double a = r[i].x * c, b = r[i].y * c;
-    A2[i] -= U2[i] * a;
-    DV[i] += a;
-    A0[i] += V0[i] * b;
-    DU[i] = b;
-  }
-  __syncthreads();
-  JSD_PAIR(10, true, 11, true)  // du1/dx, du2/dx
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    A0[i] += V1[i] * (r[i].x * c) + V2[i] * (r[i].y * c);
-  }
-  __syncthreads();
-  JSD_PAIR(12, false, 13, false)  // du0/dy, du1/dy
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double a = r[i].x * c, b = r[i].y * c;
-    A1[i] += V0[i] * a + V1[i] * b;
-    DU[i] += b;
-  }
-  __syncthreads();
-  JSD_PAIR(14, false, 15, false)  // du2/dy, du0/dz
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    A1[i] += V2[i] * (r[i].x * c);
-    A2[i] += V0[i] * (r[i].y * c);
-  }
-  __syncthreads();
-  JSD_PAIR(16, false, 17, false)  // du1/dz, du2/dz
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double a = r[i].x * c, b = r[i].y * c;
-    A2[i] += V1[i] * a + V2[i] * b;
-    DU[i] += b;
-  }
-  __syncthreads();
-#undef JSD_PAIR
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) {
-    const double du = DU[i], dv = DV[i];
-    const double h0 = A0[i] + 0.25 * du * V0[i] + 0.25 * dv * (ub + U0[i]);
-    const double h1 = A1[i] + dub * V0[i] + 0.25 * du * V1[i] + 0.25 * dv * U1[i];
-    const double h2 = A2[i] + 0.25 * du * V2[i] + 0.25 * dv * U2[i];
-    la[i] = make_double2(h0, h1);
-    V0[i] = h2;
-  }
-  __syncthreads();
-  r = fft_lines<false>(la, lb, ZB, fx, twl);
-  const int K1 = g.kx_max + 1;
-  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
-    const int kx = i / ZB;
-    const int zl = i - kx * ZB;
-    const int z = z0 + zl;
-    if (z >= g.pz) continue;
-    const double2 a = r[zl * px + kx];
-    const double2 b = r[zl * px + (kx == 0 ? 0 : px - kx)];
-    out3[(((size_t)0 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
-    out3[(((size_t)1 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.y + b.y), -0.5 * (a.x - b.x));
-  }
-  __syncthreads();
-  double2* other = (r == la) ? lb : la;
-  for (int i = threadIdx.x; i < npt; i += blockDim.x) other[i] = make_double2(V0[i], 0.0);
-  __syncthreads();
-  double2* scratch = (other == la) ? lb : la;
-  r = fft_lines<false>(other, scratch, ZB, fx, twl);
-  for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
-    const int kx = i / ZB;
-    const int zl = i - kx * ZB;
-    const int z = z0 + zl;
-    if (z >= g.pz) continue;
-    out3[(((size_t)2 * g.ny + y) * K1 + kx) * g.pz + z] = r[zl * px + kx];
-  }
+  forward_and_store<ZB>(g, fx, twl, la, lb, out3, y, z0);
 }
 
 // ---------------------------------------------------------------------------
@@ -424,9 +359,10 @@ __global__ void k_zfwd(Geo g, FftDesc fz, const double2* __restrict__ tw, const 
                        double2* __restrict__ conv00) {
   extern __shared__ __align__(16) double2 fsm[];
   const int pz = g.pz;
+  const int L = fline(pz);
   double2* twl = fsm;
   double2* bufa = twl + pz;
-  double2* bufb = bufa + 3 * pz;
+  double2* bufb = bufa + 3 * L;
   const int kx = blockIdx.x;
   const int y = blockIdx.y;
   const int K1 = g.kx_max + 1;
@@ -434,13 +370,13 @@ __global__ void k_zfwd(Geo g, FftDesc fz, const double2* __restrict__ tw, const 
   for (int i = threadIdx.x; i < 3 * pz; i += blockDim.x) {
     const int f = i / pz;
     const int z = i - f * pz;
-    bufa[i] = out3[(((size_t)f * g.ny + y) * K1 + kx) * pz + z];
+    bufa[f * L + fpad(z)] = out3[(((size_t)f * g.ny + y) * K1 + kx) * pz + z];
   }
   __syncthreads();
   double2* F = fft_lines<false>(bufa, bufb, 3, fz, twl);
   const double cf = g.c_fwd;
   auto getF = [&](int f, int kz) -> double2 {
-    return cscale(F[f * pz + (kz >= 0 ? kz : pz + kz)], cf);
+    return cscale(F[f * L + fpad(kz >= 0 ? kz : pz + kz)], cf);
   };
   const int K = g.kx_max;
   // rows this block owns: kx itself; -kx for 1 <= kx < K; the -K slot when kx = K
@@ -561,54 +497,84 @@ struct StageCoef {
   int first;  // the previous-stage terms are zero
 };
 
-__global__ void k_eigen_update(Geo g, EigTables t, StageCoef sc, const double* __restrict__ X1,
-                               const double* __restrict__ H1t, const double* __restrict__ hgt,
-                               const double* __restrict__ vt, const double* __restrict__ omt,
-                               const double* __restrict__ vfield, double* __restrict__ hv_old,
-                               double* __restrict__ hg_old, double* __restrict__ vnt, double* __restrict__ omnt) {
+constexpr int kEigCols = 32;    // columns per block (one warp-wide row segment)
+constexpr int kEigParts = 4;    // warps per block, each walking a quarter of the eigen rows
+
+__global__ void __launch_bounds__(kEigCols * kEigParts) k_eigen_update(
+    Geo g, EigTables t, StageCoef sc, const double* __restrict__ X1, const double* __restrict__ H1t,
+    const double* __restrict__ hgt, const double* __restrict__ vt, const double* __restrict__ omt,
+    const double* __restrict__ vfield, double* __restrict__ hv_old, double* __restrict__ hg_old,
+    double* __restrict__ vnt, double* __restrict__ omnt) {
+  __shared__ double red[kEigParts][6][kEigCols];
   const int N = 2 * g.nk;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= N) return;
-  const int kp = c >> 1;
-  const int ix = kp / g.mz, iz = kp - (kp / g.mz) * g.mz;
-  const double kx = kx_of(g, ix), kz = kz_of(g, iz);
-  const double k2 = kx * kx + kz * kz;
+  const int lane = threadIdx.x % kEigCols;
+  const int part = threadIdx.x / kEigCols;
+  const int c = blockIdx.x * kEigCols + lane;
+  const bool active = c < N;
   const int n = g.ny - 2;
-  const double v0 = vfield[c];
-  const double vN = vfield[(size_t)(g.ny - 1) * N + c];
+  const int j0 = (n * part) / kEigParts, j1 = (n * (part + 1)) / kEigParts;
+  double k2 = 0.0, v0 = 0.0, vN = 0.0;
+  if (active) {
+    const int kp = c >> 1;
+    const int ix = kp / g.mz, iz = kp - (kp / g.mz) * g.mz;
+    const double kx = kx_of(g, ix), kz = kz_of(g, iz);
+    k2 = kx * kx + kz * kz;
+    v0 = vfield[c];
+    vN = vfield[(size_t)(g.ny - 1) * N + c];
+  }
   const double ar = sc.alpha * sc.dt / sc.re;
   const double br = sc.beta * sc.dt / sc.re;
   double d0p = 0, dNp = 0, d0a = 0, dNa = 0, d0b = 0, dNb = 0;
-  for (int j = 0; j < n; ++j) {
-    const size_t o = (size_t)j * N + c;
-    const double L = t.lam[j] - k2;
-    const double R = 1.0 + ar * L;
-    const double H = 1.0 - br * L;
-    const double ih = 1.0 / H;
-    const double ihl = ih / L;
-    const double hv = -X1[o] - k2 * H1t[o];
-    const double hvo = sc.first ? 0.0 : hv_old[o];
-    const double phi = L * vt[o] + t.c0[j] * v0 + t.cN[j] * vN;
-    const double vp = (R * phi + sc.dt_e * (sc.gamma * hv + sc.xi * hvo)) * ihl;
-    const double va = br * t.c0[j] * ihl;
-    d0p += t.w0[j] * vp;
-    dNp += t.wN[j] * vp;
-    d0a += t.w0[j] * va;
-    dNa += t.wN[j] * va;
-    d0b += t.w0[j] * t.sgn[j] * va;
-    dNb += t.wN[j] * t.sgn[j] * va;
-    vnt[o] = vp;
-    hv_old[o] = hv;
-    const double hg = hgt[o];
-    const double hgo = sc.first ? 0.0 : hg_old[o];
-    omnt[o] = (R * omt[o] + sc.dt_e * (sc.gamma * hg + sc.xi * hgo)) * ih;
-    hg_old[o] = hg;
+  if (active) {
+#pragma unroll 4
+    for (int j = j0; j < j1; ++j) {
+      const size_t o = (size_t)j * N + c;
+      const double L = t.lam[j] - k2;
+      const double R = 1.0 + ar * L;
+      const double H = 1.0 - br * L;
+      const double ih = 1.0 / H;
+      const double ihl = ih / L;
+      const double hv = -X1[o] - k2 * H1t[o];
+      const double hvo = sc.first ? 0.0 : hv_old[o];
+      const double phi = L * vt[o] + t.c0[j] * v0 + t.cN[j] * vN;
+      const double vp = (R * phi + sc.dt_e * (sc.gamma * hv + sc.xi * hvo)) * ihl;
+      const double va = br * t.c0[j] * ihl;
+      const double w0 = t.w0[j], wN = t.wN[j], sg = t.sgn[j];
+      d0p += w0 * vp;
+      dNp += wN * vp;
+      d0a += w0 * va;
+      dNa += wN * va;
+      d0b += w0 * sg * va;
+      dNb += wN * sg * va;
+      vnt[o] = vp;
+      hv_old[o] = hv;
+      const double hg = hgt[o];
+      const double hgo = sc.first ? 0.0 : hg_old[o];
+      omnt[o] = (R * omt[o] + sc.dt_e * (sc.gamma * hg + sc.xi * hgo)) * ih;
+      hg_old[o] = hg;
+    }
   }
-  const double det = d0a * dNb - d0b * dNa;
-  const double ra = -d0p, rb = -dNp;
-  const double a = (dNb * ra - d0b * rb) / det;
-  const double b = (-dNa * ra + d0a * rb) / det;
-  for (int j = 0; j < n; ++j) {
+  red[part][0][lane] = d0p;
+  red[part][1][lane] = dNp;
+  red[part][2][lane] = d0a;
+  red[part][3][lane] = dNa;
+  red[part][4][lane] = d0b;
+  red[part][5][lane] = dNb;
+  __syncthreads();
+  if (!active) return;
+  double sum[6];
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    double acc = 0.0;
+#pragma unroll
+    for (int pp = 0; pp < kEigParts; ++pp) acc += red[pp][q][lane];
+    sum[q] = acc;
+  }
+  const double det = sum[2] * sum[5] - sum[4] * sum[3];
+  const double ra = -sum[0], rb = -sum[1];
+  const double a = (sum[5] * ra - sum[4] * rb) / det;
+  const double b = (-sum[3] * ra + sum[2] * rb) / det;
+  for (int j = j0; j < j1; ++j) {
     const size_t o = (size_t)j * N + c;
     const double L = t.lam[j] - k2;
     const double H = 1.0 - br * L;
@@ -624,35 +590,54 @@ __global__ void k_eigen_update(Geo g, EigTables t, StageCoef sc, const double* _
 //   N = [-conv00_x - dpdx * scale, -conv00_z]
 // One block of 2 Ny threads (rows). conv_old == nullptr means zero.
 // ---------------------------------------------------------------------------
-__global__ void k_mean_flow(Geo g, const double* __restrict__ rhs_ns, const double* __restrict__ lhs_inv_ns,
-                            const double2* __restrict__ u, const double2* __restrict__ w,
-                            const double2* __restrict__ conv, const double2* __restrict__ conv_old,
-                            const double* __restrict__ dpdx, double dpdx_scale, double dt_gamma, double dt_xi,
-                            double2* __restrict__ uw00) {
+constexpr int kMeanFlowThreads = 1024;
+
+__global__ void __launch_bounds__(kMeanFlowThreads) k_mean_flow(
+    Geo g, const double* __restrict__ rhs_ns, const double* __restrict__ lhs_inv_ns, const double2* __restrict__ u,
+    const double2* __restrict__ w, const double2* __restrict__ conv, const double2* __restrict__ conv_old,
+    const double* __restrict__ dpdx, double dpdx_scale, double dt_gamma, double dt_xi, double2* __restrict__ uw00) {
   extern __shared__ __align__(16) double2 msm[];
   const int n = g.ny, n2 = 2 * g.ny;
   double2* xv = msm;       // current (U00, W00)
   double2* rv = xv + n2;   // right-hand side
   const double dp = dpdx ? dpdx[0] * dpdx_scale : 0.0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int i = threadIdx.x; i < n2; i += blockDim.x) {
     xv[i] = (i < n) ? u[sidx(g, i, 0, 0)] : w[sidx(g, i - n, 0, 0)];
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-    double2 acc = make_double2(0.0, 0.0);
+  // one warp per row, lanes along the row (coalesced)
+  for (int i = warp; i < n2; i += nwarps) {
     const double* row = rhs_ns + (size_t)i * n2;
-    for (int j = 0; j < n2; ++j) acc = cadd(acc, cscale(xv[j], row[j]));
-    const double src = (i < n) ? -dp : 0.0;
-    const double2 nn = make_double2(-conv[i].x + src, -conv[i].y);
-    const double2 no = conv_old ? make_double2(-conv_old[i].x + src, -conv_old[i].y) : make_double2(src, 0.0);
-    rv[i] = cadd(cadd(acc, cscale(nn, dt_gamma)), cscale(no, dt_xi));
+    double ax = 0.0, ay = 0.0;
+    for (int j = lane; j < n2; j += 32) {
+      ax += xv[j].x * row[j];
+      ay += xv[j].y * row[j];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      ax += __shfl_down_sync(0xffffffffu, ax, o);
+      ay += __shfl_down_sync(0xffffffffu, ay, o);
+    }
+    if (lane == 0) {
+      const double src = (i < n) ? -dp : 0.0;
+      const double2 nn = make_double2(-conv[i].x + src, -conv[i].y);
+      const double2 no = conv_old ? make_double2(-conv_old[i].x + src, -conv_old[i].y) : make_double2(src, 0.0);
+      rv[i] = cadd(cadd(make_double2(ax, ay), cscale(nn, dt_gamma)), cscale(no, dt_xi));
+    }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-    double2 acc = make_double2(0.0, 0.0);
+  for (int i = warp; i < n2; i += nwarps) {
     const double* row = lhs_inv_ns + (size_t)i * n2;
-    for (int j = 0; j < n2; ++j) acc = cadd(acc, cscale(rv[j], row[j]));
-    uw00[i] = acc;
+    double ax = 0.0, ay = 0.0;
+    for (int j = lane; j < n2; j += 32) {
+      ax += rv[j].x * row[j];
+      ay += rv[j].y * row[j];
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      ax += __shfl_down_sync(0xffffffffu, ax, o);
+      ay += __shfl_down_sync(0xffffffffu, ay, o);
+    }
+    if (lane == 0) uw00[i] = make_double2(ax, ay);
   }
 }
 

@@ -211,23 +211,36 @@ def turbulent_channel_hat(
     kmax: tuple[int, int],
     seed: int,
     aliasing: float = 1.5,
-    rms_fraction: float = 0.1,
+    peak_fraction: float = 0.1,
 ) -> np.ndarray:
     """Reichardt mean profile in the (0,0) streamwise mode plus a seeded
-    solenoidal perturbation whose rms velocity is `rms_fraction` of the
-    centreline velocity."""
+    solenoidal perturbation whose largest velocity component value on the
+    reference physical grid is `peak_fraction` of the centreline velocity."""
     (mx, ny, mz), (px, _, pz) = mode_counts(shape, aliasing)
     lx, lz = lengths
     y = cheb_points(ny)
     u_mean = reichardt_profile(y, re_tau)
     u_cl = float(u_mean.max())
-    # rms over the three components: E = 1/2 <|u|^2> = 1/2 (rms_fraction u_cl)^2
-    e_pert = 0.5 * (rms_fraction * u_cl) ** 2
-    vel = seeded_velocity_hat(shape, lengths, kmax, e_pert, seed, aliasing)
+    vel = seeded_velocity_hat(shape, lengths, kmax, 1.0, seed, aliasing)
     s = lx * lz / (4.0 * np.pi ** 2)
+    peak = max(float(np.abs(_physical(vel[c], px, pz, s)).max()) for c in range(3))
+    if peak > 0.0:
+        vel *= peak_fraction * u_cl / peak
     # a constant-in-(x,z) physical field c maps to c * sqrt(Px Pz) / s at (0,0)
     vel[0, 0, :, 0] += u_mean * math.sqrt(px * pz) / s
     return vel
+
+
+def _physical(f_hat: np.ndarray, px: int, pz: int, s: float) -> np.ndarray:
+    """Physical values of one spectral field on the reference grid (zero
+    padding, ortho inverse FFT, real part, times s: domain.py:1167-1242)."""
+    mx, ny, mz = f_hat.shape
+    kx, kz = mx // 2, mz // 2
+    full = np.zeros((px, ny, pz), dtype=np.complex128)
+    ix = np.concatenate([np.arange(kx + 1), np.arange(px - kx, px)])
+    iz = np.concatenate([np.arange(kz + 1), np.arange(pz - kz, pz)])
+    full[np.ix_(ix, np.arange(ny), iz)] = f_hat
+    return np.fft.ifftn(full, axes=(0, 2), norm="ortho").real * s
 
 
 def laminar_base_hat(shape, lengths, u_max: float = 1.0, aliasing: float = 1.5) -> np.ndarray:
