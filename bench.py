@@ -168,22 +168,30 @@ def run_ours(args):
 
     modes, phys = mode_counts(SHAPE)
     u0 = _seed_state()
+    u0_dev = to_device_layout(u0, device=dev)
     probe = StepPlan(modes, phys, LX, LZ, 0, RE_TAU, DT, device=dev)
-    q0 = probe.flow_rate(to_device_layout(u0, device=dev)[0]).item()
+    q0 = probe.flow_rate(u0_dev[0]).item()
     del probe
-    plan = StepPlan(modes, phys, LX, LZ, 0, RE_TAU, DT, constant_mass_flux=True, flow_rate_target=q0, device=dev)
-    state = to_device_layout(u0, device=dev)
-    dpdx = torch.tensor([-q0 * 3 / 2 / RE_TAU], dtype=torch.float64, device=dev)
+    dpdx0 = -q0 * 3 / 2 / RE_TAU
     stream = torch.cuda.current_stream()
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        time.sleep(0.3)  # let the sampler start before the GPU is loaded
-        plan.step(state, dpdx, 0, args.warmup)  # warm-up
+    def max_over_ranks(x: float) -> float:
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(plan, sampler=None):
+        """W warm-up steps, then K steps timed with CUDA events on the
+        launching stream, barrier + synchronize on both sides."""
+        state = u0_dev.clone()
+        dpdx = torch.tensor([dpdx0], dtype=torch.float64, device=dev)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        plan.step(state, dpdx, 0, args.warmup)
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
@@ -191,22 +199,39 @@ def run_ours(args):
         plan.step(state, dpdx, args.warmup, args.steps)
         ev1.record(stream)
         torch.cuda.synchronize()
-    barrier()
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    t_max = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_max = float(t_max.item())
+        barrier()
+        torch.cuda.synchronize()
+        return max_over_ranks(ev0.elapsed_time(ev1)), state, dpdx
+
+    forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    plans, results = {}, {}
+    with ClockSampler(local) as clocks:
+        time.sleep(0.3)  # let the sampler start before the GPU is loaded
+        for pr in forms:
+            plans[pr] = StepPlan(modes, phys, LX, LZ, 0, RE_TAU, DT, constant_mass_flux=True, flow_rate_target=q0,
+                                 device=dev, precision=pr)
+            ms, state, dpdx = timed(plans[pr])
+            results[pr] = {"ms": ms, "state": state, "dpdx": dpdx, "energy": plans[pr].energy(state).item()}
+    finite = all(bool(torch.isfinite(torch.view_as_real(r["state"])).all()) for r in results.values())
+    mixed_err = None
+    if "mixed" in results and "fp64" in results:
+        mixed_err = abs(results["mixed"]["energy"] / results["fp64"]["energy"] - 1)
+    # headline form: mixed when its energy error against FP64 meets the 1e-6 bar
+    if args.precision == "both":
+        head = "mixed" if (mixed_err is not None and mixed_err <= 1e-6) else "fp64"
+    else:
+        head = forms[0]
+    plan = plans[head]
+    ms_max = results[head]["ms"]
     value = world * args.steps / (ms_max / 1e3)
-    finite = bool(torch.isfinite(torch.view_as_real(state)).all())
+    state, dpdx = results[head]["state"], results[head]["dpdx"]
 
     # per-kernel-class timing with CUDA events on the launching stream (same workload)
     plan.profile(True)
     plan.step(state, dpdx, args.warmup + args.steps, args.steps)
     torch.cuda.synchronize()
     kernels = {}
-    for name in ("gemm", "zinv", "xmid", "zfwd", "eigen"):
+    for name in ("gemm", "sgemm", "zinv", "xmid", "zfwd", "eigen"):
         tms, n, work = plan.profile_read(name)
         if n:
             kernels[name] = {"ms": tms, "launches": n, "work": work}
@@ -228,15 +253,12 @@ def run_ours(args):
         host_out.copy_(st.transpose(-3, -2), non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = torch.tensor([e0.elapsed_time(e1) / n_e2e], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
-    e2e_value = world / (float(e2e_ms.item()) / 1e3)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / n_e2e)
+    e2e_value = world / (e2e_ms / 1e3)
     state_bytes = host_in.numel() * host_in.element_size()
 
     if rank == 0:
         peaks, peak_src = _peaks()
-        # dominant kernel class by device time
         dom = max(kernels, key=lambda k: kernels[k]["ms"]) if kernels else None
         total_k = sum(v["ms"] for v in kernels.values())
         roofline = None
@@ -253,13 +275,14 @@ def run_ours(args):
                             "traffic": None, "share_of_kernel_time": k["ms"] / total_k}
             else:
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e9
-                roofline = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peak_src,
+                roofline = {"kernel": "k_" + dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                            "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
                             "traffic": None, "share_of_kernel_time": k["ms"] / total_k}
         per_kernel = {k: {"avg_us": 1e3 * v["ms"] / v["launches"], "launches": v["launches"],
                           "share": v["ms"] / total_k} for k, v in kernels.items()}
         for k, v in kernels.items():
-            if k == "gemm":
+            if k in ("gemm", "sgemm"):
                 per_kernel[k]["tflops"] = v["work"] / (v["ms"] / 1e3) / 1e12
             else:
                 per_kernel[k]["gbs"] = v["work"] / (v["ms"] / 1e3) / 1e9
@@ -267,15 +290,23 @@ def run_ours(args):
         if world == 1 and not args.no_cpu_baseline:
             rate, sec, sample, threads = cpu_reference_leg(1, 0)
             cpu = {"value": rate, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample}
+        forms_out = {pr: {"steps_per_s": world * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
+                          "energy_after": r["energy"]} for pr, r in results.items()}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if head == "fp64" else "mixed: f32 transforms/products, 3xtf32 y-derivatives, f64 solves",
             "data": "synthetic (seeded Reichardt mean + solenoidal perturbation)",
             "config": {"workload": WORKLOAD, "modes": list(modes), "fft_sizes": list(plan.fft_sizes),
                        "reference_physical_grid": list(phys), "parallelism": f"replicas x{world}",
                        "l2": "working set per step ~1 GB > 126 MB L2 (no flush needed)",
-                       "precision": "fp64"},
+                       "precision": head},
+            "forms": forms_out,
+            "mixed_over_fp64": (forms_out["mixed"]["steps_per_s"] / forms_out["fp64"]["steps_per_s"]
+                                if len(forms_out) == 2 else None),
+            "mixed_energy_rel_err_vs_fp64": mixed_err,
+            "mixed_error_steps": args.warmup + args.steps,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "api": "StepPlan.step on host (pinned) state"},
             "gpu_launches": plan.launches_per_step() * args.steps,
@@ -315,6 +346,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
+                    help="headline form; 'both' times FP64 and mixed and reports mixed beside FP64")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

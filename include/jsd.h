@@ -74,7 +74,11 @@ typedef struct jsd_desc {
   const double* y_weights; /* [ny] Chebyshev integration weights (field.py:2618-2650) */
   const double* rhs_ns;    /* [3*(2ny)^2] (0,0) explicit matrices per RK stage (navier_stokes.py:1000-1022) */
   const double* lhs_inv_ns;/* [3*(2ny)^2] (0,0) implicit inverses per RK stage */
+  int precision;           /* JSD_PRECISION_FP64, or JSD_PRECISION_MIXED: FP32 transforms and products,
+                              split-TF32 tensor-core y-derivatives; solves stay FP64 */
 } jsd_desc;
+
+enum jsd_precision { JSD_PRECISION_FP64 = 0, JSD_PRECISION_MIXED = 1 };
 
 typedef struct jsd_plan jsd_plan;
 
@@ -156,7 +160,8 @@ enum jsd_prof_class {
   JSD_PROF_XMID = 2,    /* x transforms + products */
   JSD_PROF_ZFWD = 3,    /* forward z transforms + truncation */
   JSD_PROF_EIGEN = 4,   /* eigenbasis update + influence correction */
-  JSD_PROF_LINEAR = 5   /* linearised terms */
+  JSD_PROF_LINEAR = 5,  /* linearised terms */
+  JSD_PROF_SGEMM = 6    /* split-TF32 y-derivatives (mixed precision) */
 };
 int jsd_profile_enable(jsd_plan* plan, int enable);
 int jsd_profile_read(jsd_plan* plan, int kernel_class, double* total_ms, long long* launches, double* work);

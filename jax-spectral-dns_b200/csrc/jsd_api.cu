@@ -71,6 +71,18 @@ int choose_fft_size(int m) {
   return n;
 }
 
+// Round an FP32 value to the nearest TF32 value (10 explicit mantissa bits,
+// ties away from zero as cvt.rna does).
+float tf32_round(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return x;  // inf / nan unchanged
+  u = (u + 0x1000u) & 0xffffe000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
 // Factor n into supported radices and build the forward twiddle table.
 bool build_fft(int n, FftDesc& d, std::vector<double2>& tw) {
   std::vector<int> rs;
@@ -115,13 +127,16 @@ struct jsd_plan {
   double dpdx_scale;
   // device operator tables
   double2 *twx = nullptr, *twz = nullptr;
+  float2 *twx32 = nullptr, *twz32 = nullptr;
+  float *Dhi = nullptr, *Dlo = nullptr;  // TF32 split of D (mixed precision)
+  bool mixed = false;
   double *Dm = nullptr, *VinvD = nullptr, *Vinv = nullptr, *Vfull = nullptr, *DVfull = nullptr;
   double *lam = nullptr, *sgn = nullptr, *c0 = nullptr, *cN = nullptr, *w0 = nullptr, *wN = nullptr;
   double *yw = nullptr, *rhs_ns = nullptr, *lhs_inv_ns = nullptr, *ub = nullptr, *dub = nullptr;
   // workspace
   double2 *Dfld = nullptr;     // 3 fields: D u, D v, D w
-  double2 *inter = nullptr;    // 9 z-transformed lines per (y, kx >= 0)
-  double2 *out3 = nullptr;     // 3 x-transformed products per (y, kx >= 0)
+  void *inter = nullptr;       // 9 (18 for the dual) z-transformed lines per (y, kx >= 0)
+  void *out3 = nullptr;        // 3 x-transformed products per (y, kx >= 0)
   double2 *q = nullptr, *H1 = nullptr, *hg = nullptr, *om = nullptr, *dvn = nullptr, *tmp = nullptr;
   double2 *conv = nullptr;     // 3 stages x 2 ny
   double2 *uw00 = nullptr;     // 2 ny
@@ -219,6 +234,40 @@ int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, cudaStream_t s
   return 0;
 }
 
+GemmBatch gemm_batch(const jsd_plan* p);
+void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M, int K, double alpha = 1.0);
+
+// y-derivatives D * f of up to kGemmMaxBatch fields: FP64 DMMA, or 3xTF32 in
+// the mixed-precision mode
+int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
+  const int ny = p->g.ny;
+  if (!p->mixed) {
+    GemmBatch b = gemm_batch(p);
+    for (int i = 0; i < count; ++i) add_entry(b, p->Dm, src[i], dst[i], ny, ny, 1.0);
+    return launch_gemm(p, b, ny, s);
+  }
+  SplitGemmBatch b;
+  memset(&b, 0, sizeof(b));
+  b.N = 2 * p->g.nk;
+  b.lda = p->lda;
+  b.ldb = b.N;
+  b.ldc = b.N;
+  for (int i = 0; i < count; ++i) {
+    SplitGemmEntry& e = b.e[b.count++];
+    e.Ahi = p->Dhi;
+    e.Alo = p->Dlo;
+    e.B = src[i];
+    e.C = dst[i];
+    e.M = ny;
+    e.K = ny;
+  }
+  ProfScope ps(p, JSD_PROF_SGEMM, 2.0 * ny * (double)ny * b.N * count, s);
+  const dim3 grid((b.N + Sgemm3Smem::BN - 1) / Sgemm3Smem::BN, 1, b.count);
+  k_sgemm3<<<grid, Sgemm3Smem::THREADS, Sgemm3Smem::BYTES, s>>>(b);
+  JSD_LAUNCHED("k_sgemm3");
+  return 0;
+}
+
 GemmBatch gemm_batch(const jsd_plan* p) {
   GemmBatch b;
   memset(&b, 0, sizeof(b));
@@ -229,7 +278,7 @@ GemmBatch gemm_batch(const jsd_plan* p) {
   return b;
 }
 
-void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M, int K, double alpha = 1.0) {
+void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M, int K, double alpha) {
   GemmEntry& e = b.e[b.count++];
   e.A = A;
   e.B = B;
@@ -258,6 +307,9 @@ __global__ void k_assemble_hv(Geo g, const double2* __restrict__ dq, const doubl
   }
 }
 
+template <typename C>
+int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2* conv, cudaStream_t s);
+
 // nonlinear terms of `state` into p->q, p->H1, p->hg and conv00 slot `stage`
 int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage, cudaStream_t s) {
   const Geo& g = p->g;
@@ -271,9 +323,9 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
   if (p->desc.kind == JSD_KIND_DUAL && !linear && !uhist)
     return fail(JSD_ERR_STATE, "dual step needs the forward state (jsd_set_history)");
   if (linear) {
-    GemmBatch b = gemm_batch(p);
-    add_entry(b, p->Dm, (const double*)v, (double*)(p->Dfld + fs), ny, ny);
-    int rc = launch_gemm(p, b, ny, s);
+    const double* src[1] = {(const double*)v};
+    double* dst[1] = {(double*)(p->Dfld + fs)};
+    int rc = launch_dfield(p, src, dst, 1, s);
     if (rc) return rc;
     const int blk = 256;
     ProfScope ps(p, JSD_PROF_LINEAR, sizeof(double2) * 7.0 * fs, s);
@@ -288,14 +340,35 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
   }
   const bool dual = p->desc.kind == JSD_KIND_DUAL;
   const int nsets = dual ? 2 : 1;
-  GemmBatch b = gemm_batch(p);
-  for (int c = 0; c < 3; ++c) add_entry(b, p->Dm, (const double*)(state + c * fs), (double*)(p->Dfld + c * fs), ny, ny);
-  if (dual)
-    for (int c = 0; c < 3; ++c)
-      add_entry(b, p->Dm, (const double*)(uhist + c * fs), (double*)(p->Dfld + (3 + c) * fs), ny, ny);
-  int rc = launch_gemm(p, b, ny, s);
-  if (rc) return rc;
+  {
+    const double* src[6];
+    double* dst[6];
+    for (int c = 0; c < 3; ++c) {
+      src[c] = (const double*)(state + c * fs);
+      dst[c] = (double*)(p->Dfld + c * fs);
+      if (dual) {
+        src[3 + c] = (const double*)(uhist + c * fs);
+        dst[3 + c] = (double*)(p->Dfld + (3 + c) * fs);
+      }
+    }
+    int rc = launch_dfield(p, src, dst, 3 * nsets, s);
+    if (rc) return rc;
+  }
+  return p->mixed ? transforms<float2>(p, state, uhist, conv, s) : transforms<double2>(p, state, uhist, conv, s);
+}
+
+template <typename C>
+int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2* conv, cudaStream_t s) {
+  const Geo& g = p->g;
+  const size_t fs = (size_t)g.ny * g.nk;
+  const int ny = g.ny;
+  const bool dual = p->desc.kind == JSD_KIND_DUAL;
+  const int nsets = dual ? 2 : 1;
   const int K1 = g.kx_max + 1;
+  const C* twx = p->mixed ? (const C*)p->twx32 : (const C*)p->twx;
+  const C* twz = p->mixed ? (const C*)p->twz32 : (const C*)p->twz;
+  C* inter = static_cast<C*>(p->inter);
+  C* out3 = static_cast<C*>(p->out3);
   {
     ZinvSrc src;
     src.nsets = nsets;
@@ -308,31 +381,31 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
       }
     }
     const int nl = kZinvLines * nsets;
-    const size_t sm = sizeof(double2) * ((size_t)g.pz + 2 * (size_t)nl * fline(g.pz));
-    const double bytes = sizeof(double2) * (6.0 * nsets * fs + (double)nl * ny * K1 * g.pz);
+    const size_t sm = sizeof(C) * ((size_t)g.pz + 2 * (size_t)nl * fline(g.pz));
+    const double bytes = sizeof(double2) * 6.0 * nsets * fs + sizeof(C) * (double)nl * ny * K1 * g.pz;
     ProfScope ps(p, JSD_PROF_ZINV, bytes, s);
-    k_zinv<<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, p->twz, src, p->inter);
+    k_zinv<C><<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, twz, src, inter);
     JSD_LAUNCHED("k_zinv");
   }
   if (dual) {
-    const size_t sm = XmidSmem<kXmidZB>::bytes(g);
-    ProfScope ps(p, JSD_PROF_XMID, sizeof(double2) * (double)(2 * kZinvLines + 3) * ny * K1 * g.pz, s);
-    k_xmid_dual<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
-        g, p->fx, p->twx, p->inter, p->out3, p->ub, p->dub);
+    const size_t sm = XmidSmem<C, kXmidZB>::bytes(g);
+    ProfScope ps(p, JSD_PROF_XMID, sizeof(C) * (double)(2 * kZinvLines + 3) * ny * K1 * g.pz, s);
+    k_xmid_dual<C, kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
+        g, p->fx, twx, inter, out3, p->ub, p->dub);
     JSD_LAUNCHED("k_xmid_dual");
   } else {
-    const size_t sm = XmidSmem<kXmidZB>::bytes(g);
-    ProfScope ps(p, JSD_PROF_XMID, sizeof(double2) * (double)(kZinvLines + 3) * ny * K1 * g.pz, s);
+    const size_t sm = XmidSmem<C, kXmidZB>::bytes(g);
+    ProfScope ps(p, JSD_PROF_XMID, sizeof(C) * (double)(kZinvLines + 3) * ny * K1 * g.pz, s);
     const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
     const bool pert = p->desc.kind == JSD_KIND_PERTURBATION;
-    k_xmid<kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
-        g, p->fx, p->twx, p->inter, p->out3, pert ? p->ub : nullptr, pert ? p->dub : nullptr, lam);
+    k_xmid<C, kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
+        g, p->fx, twx, inter, out3, pert ? p->ub : nullptr, pert ? p->dub : nullptr, lam);
     JSD_LAUNCHED("k_xmid");
   }
   {
-    const size_t sm = sizeof(double2) * ((size_t)g.pz + 6 * (size_t)fline(g.pz));
-    ProfScope ps(p, JSD_PROF_ZFWD, sizeof(double2) * (3.0 * ny * K1 * g.pz + 3.0 * fs), s);
-    k_zfwd<<<dim3(K1, ny), 128, sm, s>>>(g, p->fz, p->twz, p->out3, p->q, p->H1, p->hg, conv);
+    const size_t sm = sizeof(C) * ((size_t)g.pz + 6 * (size_t)fline(g.pz));
+    ProfScope ps(p, JSD_PROF_ZFWD, sizeof(C) * 3.0 * ny * K1 * g.pz + sizeof(double2) * 3.0 * fs, s);
+    k_zfwd<C><<<dim3(K1, ny), 128, sm, s>>>(g, p->fz, twz, out3, p->q, p->H1, p->hg, conv);
     JSD_LAUNCHED("k_zfwd");
   }
   return 0;
@@ -424,10 +497,15 @@ int set_smem_limits() {
   static bool done = false;
   if (done) return 0;
   const int big = 200 * 1024;
-  JSD_CUDA(cudaFuncSetAttribute(k_zinv, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  JSD_CUDA(cudaFuncSetAttribute(k_xmid<kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  JSD_CUDA(cudaFuncSetAttribute(k_xmid_dual<kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  JSD_CUDA(cudaFuncSetAttribute(k_zfwd, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_zinv<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_zinv<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_xmid<double2, kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_xmid<float2, kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_xmid_dual<double2, kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_xmid_dual<float2, kXmidZB>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_zfwd<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_zfwd<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_sgemm3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sgemm3Smem::BYTES));
   JSD_CUDA(cudaFuncSetAttribute(k_dgemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<48>::BYTES));
   JSD_CUDA(cudaFuncSetAttribute(k_dgemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<64>::BYTES));
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -574,6 +652,7 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
 
   jsd_plan* p = new jsd_plan();
   p->desc = *d;
+  p->mixed = d->precision == JSD_PRECISION_MIXED;
   Geo& g = p->g;
   g.mx = d->mx;
   g.ny = d->ny;
@@ -639,6 +718,24 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
 
   JSD_TRY(upload(p, &p->twx, twx.data(), twx.size()));
   JSD_TRY(upload(p, &p->twz, twz.data(), twz.size()));
+  if (p->mixed) {
+    std::vector<float2> tx(twx.size()), tz(twz.size());
+    for (size_t i = 0; i < twx.size(); ++i) tx[i] = make_float2((float)twx[i].x, (float)twx[i].y);
+    for (size_t i = 0; i < twz.size(); ++i) tz[i] = make_float2((float)twz[i].x, (float)twz[i].y);
+    JSD_TRY(upload(p, &p->twx32, tx.data(), tx.size()));
+    JSD_TRY(upload(p, &p->twz32, tz.data(), tz.size()));
+    // D = D_hi + D_lo with both parts representable in TF32 (round to nearest)
+    std::vector<float> hi((size_t)ny * p->lda, 0.f), lo((size_t)ny * p->lda, 0.f);
+    for (int r = 0; r < ny; ++r)
+      for (int c = 0; c < ny; ++c) {
+        const double x = d->D[(size_t)r * ny + c];
+        const float h = tf32_round((float)x);
+        hi[(size_t)r * p->lda + c] = h;
+        lo[(size_t)r * p->lda + c] = tf32_round((float)(x - (double)h));
+      }
+    JSD_TRY(upload(p, &p->Dhi, hi.data(), hi.size()));
+    JSD_TRY(upload(p, &p->Dlo, lo.data(), lo.size()));
+  }
   JSD_TRY(upload_padded(p, &p->Dm, d->D, ny, ny, p->lda));
   JSD_TRY(upload_padded(p, &p->VinvD, VinvD.data(), ni, ny, p->lda));
   JSD_TRY(upload_padded(p, &p->Vinv, d->Vinv, ni, ni, p->lda));
@@ -661,8 +758,9 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   const int nsets = (d->kind == JSD_KIND_DUAL) ? 2 : 1;
   JSD_TRY(dev_alloc(p, (void**)&p->Dfld, 3 * (size_t)nsets * fs * sizeof(double2)));
   if (!linear) {
-    JSD_TRY(dev_alloc(p, (void**)&p->inter, (size_t)kZinvLines * nsets * ny * K1 * g.pz * sizeof(double2)));
-    JSD_TRY(dev_alloc(p, (void**)&p->out3, 3 * (size_t)ny * K1 * g.pz * sizeof(double2)));
+    const size_t csz = p->mixed ? sizeof(float2) : sizeof(double2);
+    JSD_TRY(dev_alloc(p, (void**)&p->inter, (size_t)kZinvLines * nsets * ny * K1 * g.pz * csz));
+    JSD_TRY(dev_alloc(p, (void**)&p->out3, 3 * (size_t)ny * K1 * g.pz * csz));
   }
   for (double2** f : {&p->q, &p->H1, &p->hg, &p->om, &p->dvn, &p->tmp})
     JSD_TRY(dev_alloc(p, (void**)f, fs * sizeof(double2)));

@@ -21,6 +21,29 @@ struct Geo {
   double c_fwd;      // sqrt(Px_ref Pz_ref) / (s px pz): unnormalised DFT -> coefficient
 };
 
+// complex helpers for double2 (FP64 path) and float2 (FP32 transforms of the
+// mixed-precision path)
+template <typename T> struct real_of;
+template <> struct real_of<double2> { using type = double; };
+template <> struct real_of<float2> { using type = float; };
+
+__device__ __forceinline__ double2 mkc(double x, double y, double2*) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mkc(float x, float y, float2*) { return make_float2(x, y); }
+template <typename C>
+__device__ __forceinline__ C cmake(typename real_of<C>::type x, typename real_of<C>::type y) {
+  return mkc(x, y, (C*)nullptr);
+}
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cmul_ik(float2 a, float k) { return make_float2(-k * a.y, k * a.x); }
+template <typename C> __device__ __forceinline__ C to_c(double2 a) { return cmake<C>(a.x, a.y); }
+template <typename C> __device__ __forceinline__ C to_c(float2 a) { return cmake<C>(a.x, a.y); }
+
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }

@@ -55,33 +55,35 @@ __device__ __forceinline__ void root_table(int r, int m, double& c, double& s) {
 //   y[q]   = x_0 + sum_t a_t cos(2 pi q t / R) -+ i sum_t b_t sin(2 pi q t / R)
 //   y[R-q] = x_0 + sum_t a_t cos(2 pi q t / R) +- i sum_t b_t sin(2 pi q t / R)
 // (upper signs forward), h^2 complex-by-real products per half instead of R^2.
-template <int R, bool INV>
-__device__ __forceinline__ void dft_odd(double2* x) {
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void dft_odd(C* x) {
+  using Rl = typename real_of<C>::type;
   constexpr int H = (R - 1) / 2;
-  double2 a[H], b[H];
-  double2 y0 = x[0];
+  C a[H], b[H];
+  C y0 = x[0];
 #pragma unroll
   for (int t = 1; t <= H; ++t) {
     a[t - 1] = cadd(x[t], x[R - t]);
     b[t - 1] = csub(x[t], x[R - t]);
     y0 = cadd(y0, a[t - 1]);
   }
-  double2 y[R];
+  C y[R];
   y[0] = y0;
 #pragma unroll
   for (int q = 1; q <= H; ++q) {
-    double2 re = x[0], im = make_double2(0.0, 0.0);
+    C re = x[0], im = cmake<C>(0, 0);
 #pragma unroll
     for (int t = 1; t <= H; ++t) {
-      double c, sn;
-      root_table(R, (q * t) % R, c, sn);
+      double cd, sd;
+      root_table(R, (q * t) % R, cd, sd);
+      const Rl c = (Rl)cd, sn = (Rl)sd;
       re.x += a[t - 1].x * c;
       re.y += a[t - 1].y * c;
       im.x += b[t - 1].x * sn;
       im.y += b[t - 1].y * sn;
     }
     // i * im = (-im.y, im.x)
-    const double2 iim = make_double2(-im.y, im.x);
+    const C iim = cmake<C>(-im.y, im.x);
     y[q] = INV ? cadd(re, iim) : csub(re, iim);
     y[R - q] = INV ? csub(re, iim) : cadd(re, iim);
   }
@@ -89,42 +91,43 @@ __device__ __forceinline__ void dft_odd(double2* x) {
   for (int q = 0; q < R; ++q) x[q] = y[q];
 }
 
-template <bool INV>
-__device__ __forceinline__ void dft2(double2* x) {
-  const double2 a = x[0], b = x[1];
+template <bool INV, typename C>
+__device__ __forceinline__ void dft2(C* x) {
+  const C a = x[0], b = x[1];
   x[0] = cadd(a, b);
   x[1] = csub(a, b);
 }
 
 // multiply by -i (forward) or +i (inverse)
-template <bool INV>
-__device__ __forceinline__ double2 rot90(double2 a) {
-  return INV ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <bool INV, typename C>
+__device__ __forceinline__ C rot90(C a) {
+  return INV ? cmake<C>(-a.y, a.x) : cmake<C>(a.y, -a.x);
 }
 
-template <bool INV>
-__device__ __forceinline__ void dft4(double2* x) {
-  const double2 s02 = cadd(x[0], x[2]), d02 = csub(x[0], x[2]);
-  const double2 s13 = cadd(x[1], x[3]), d13 = rot90<INV>(csub(x[1], x[3]));
+template <bool INV, typename C>
+__device__ __forceinline__ void dft4(C* x) {
+  const C s02 = cadd(x[0], x[2]), d02 = csub(x[0], x[2]);
+  const C s13 = cadd(x[1], x[3]), d13 = rot90<INV>(csub(x[1], x[3]));
   x[0] = cadd(s02, s13);
   x[2] = csub(s02, s13);
   x[1] = cadd(d02, d13);
   x[3] = csub(d02, d13);
 }
 
-template <bool INV>
-__device__ __forceinline__ void dft8(double2* x) {
-  const double h = 0.70710678118654752440;
-  double2 e[4] = {x[0], x[2], x[4], x[6]};
-  double2 o[4] = {x[1], x[3], x[5], x[7]};
+template <bool INV, typename C>
+__device__ __forceinline__ void dft8(C* x) {
+  using Rl = typename real_of<C>::type;
+  const Rl h = (Rl)0.70710678118654752440;
+  C e[4] = {x[0], x[2], x[4], x[6]};
+  C o[4] = {x[1], x[3], x[5], x[7]};
   dft4<INV>(e);
   dft4<INV>(o);
   // twiddles exp(-+2 pi i m / 8), m = 0..3
-  const double2 o1 = INV ? make_double2(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
-                         : make_double2(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
-  const double2 o2 = rot90<INV>(o[2]);
-  const double2 o3 = INV ? make_double2(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
-                         : make_double2(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
+  const C o1 = INV ? cmake<C>(h * (o[1].x - o[1].y), h * (o[1].x + o[1].y))
+                   : cmake<C>(h * (o[1].x + o[1].y), h * (o[1].y - o[1].x));
+  const C o2 = rot90<INV>(o[2]);
+  const C o3 = INV ? cmake<C>(-h * (o[3].x + o[3].y), h * (o[3].x - o[3].y))
+                   : cmake<C>(h * (o[3].y - o[3].x), -h * (o[3].x + o[3].y));
   x[0] = cadd(e[0], o[0]);
   x[4] = csub(e[0], o[0]);
   x[1] = cadd(e[1], o1);
@@ -135,9 +138,9 @@ __device__ __forceinline__ void dft8(double2* x) {
   x[7] = csub(e[3], o3);
 }
 
-template <int R, bool INV>
-__device__ __forceinline__ void fft_pass(const double2* __restrict__ src, double2* __restrict__ dst, int nlines,
-                                         int n, int ls, const double2* __restrict__ tw) {
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void fft_pass(const C* __restrict__ src, C* __restrict__ dst, int nlines, int n, int ls,
+                                         const C* __restrict__ tw) {
   const int m = n / R;
   const int total = nlines * m;
   const int stride = fline(n);
@@ -145,14 +148,14 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ src, double
     const int l = task / m;
     const int j = task - l * m;
     const int k = j % ls;
-    const double2* s = src + (size_t)l * stride;
-    double2 x[R];
+    const C* s = src + (size_t)l * stride;
+    C x[R];
 #pragma unroll
     for (int t = 0; t < R; ++t) x[t] = s[fpad(j + t * m)];
     if (ls > 1) {
 #pragma unroll
       for (int t = 1; t < R; ++t) {
-        double2 w = tw[k * (R - 1) + (t - 1)];
+        C w = tw[k * (R - 1) + (t - 1)];
         if (INV) w.y = -w.y;
         x[t] = cmul(x[t], w);
       }
@@ -161,7 +164,7 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ src, double
     else if constexpr (R == 4) dft4<INV>(x);
     else if constexpr (R == 8) dft8<INV>(x);
     else dft_odd<R, INV>(x);
-    double2* o = dst + (size_t)l * stride;
+    C* o = dst + (size_t)l * stride;
     const int base = (j / ls) * ls * R + k;
 #pragma unroll
     for (int t = 0; t < R; ++t) o[fpad(base + t * ls)] = x[t];
@@ -171,12 +174,12 @@ __device__ __forceinline__ void fft_pass(const double2* __restrict__ src, double
 // Transform nlines lines of length d.n (line l at a + l * fline(n), element i
 // at fpad(i)) starting at a; b is scratch of the same size. Returns the buffer that holds the result. Must be called
 // by all threads of the block; ends with a barrier.
-template <bool INV>
-__device__ double2* fft_lines(double2* a, double2* b, int nlines, const FftDesc& d, const double2* __restrict__ tw) {
-  double2* src = a;
-  double2* dst = b;
+template <bool INV, typename C>
+__device__ C* fft_lines(C* a, C* b, int nlines, const FftDesc& d, const C* __restrict__ tw) {
+  C* src = a;
+  C* dst = b;
   for (int p = 0; p < d.passes; ++p) {
-    const double2* twp = tw + d.twoff[p];
+    const C* twp = tw + d.twoff[p];
     switch (d.radix[p]) {
       case 2: fft_pass<2, INV>(src, dst, nlines, d.n, d.ls[p], twp); break;
       case 3: fft_pass<3, INV>(src, dst, nlines, d.n, d.ls[p], twp); break;
@@ -186,7 +189,7 @@ __device__ double2* fft_lines(double2* a, double2* b, int nlines, const FftDesc&
       default: fft_pass<8, INV>(src, dst, nlines, d.n, d.ls[p], twp); break;
     }
     __syncthreads();
-    double2* t = src;
+    C* t = src;
     src = dst;
     dst = t;
   }

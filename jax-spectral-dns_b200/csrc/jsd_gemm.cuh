@@ -149,4 +149,165 @@ __global__ void __launch_bounds__(128) k_dgemm(GemmBatch batch) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Split-precision variant for the mixed-precision step: C = A * B with A given
+// as two TF32 parts (A = A_hi + A_lo, split on the host from FP64), B read in
+// FP64 and split on the fly (b_hi = tf32(b), b_lo = tf32(b - b_hi)), three
+// tensor-core products per tile (hi*hi + hi*lo + lo*hi) accumulated in FP32
+// (3xTF32), result written in FP64. CTA tile 144 x 64 (one tile covers every
+// row of an Ny <= 144 operator), K chunk 16, 6 warps of 48 x 32.
+// mma.sync m16n8k8 TF32 fragments (g = lane / 4, t = lane % 4):
+//   A a0 (g, t) a1 (g+8, t) a2 (g, t+4) a3 (g+8, t+4); B b0 (t, g) b1 (t+4, g)
+//   C c0 (g, 2t) c1 (g, 2t+1) c2 (g+8, 2t) c3 (g+8, 2t+1)
+// ---------------------------------------------------------------------------
+struct Sgemm3Smem {
+  static constexpr int BM = 144, BN = 64, BK = 16;
+  static constexpr int AS = BK + 4;  // floats
+  static constexpr int BS = BN + 8;  // doubles
+  static constexpr int A_BYTES = 2 * BM * AS * 4;
+  static constexpr int B_BYTES = BK * BS * 8;
+  static constexpr int STAGE_BYTES = A_BYTES + B_BYTES;
+  static constexpr size_t BYTES = 2 * (size_t)STAGE_BYTES;
+  static constexpr int THREADS = 192;
+};
+
+struct SplitGemmEntry {
+  const float* Ahi;  // M x lda (zero-padded beyond K)
+  const float* Alo;
+  const double* B;   // K x ldb
+  double* C;         // M x ldc
+  int M, K;
+};
+
+struct SplitGemmBatch {
+  SplitGemmEntry e[kGemmMaxBatch];
+  int count;
+  int N, lda, ldb, ldc;
+};
+
+__device__ __forceinline__ unsigned tf32_bits(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ void mma_tf32(float* d, const unsigned* a, const unsigned* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(Sgemm3Smem::THREADS) k_sgemm3(SplitGemmBatch batch) {
+  using S = Sgemm3Smem;
+  constexpr int BN = S::BN, BK = S::BK, BM = S::BM;
+  constexpr int TM = 3, TN = 4;
+  extern __shared__ __align__(16) unsigned char ssm[];
+
+  const SplitGemmEntry& e = batch.e[blockIdx.z];
+  const int n0 = blockIdx.x * BN;
+  const int N = batch.N;
+  const int lda = batch.lda, ldb = batch.ldb, ldc = batch.ldc;
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5, lane = tid & 31;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp >> 1) * 48;
+  const int wn = (warp & 1) * 32;
+
+  auto load_chunk = [&](int stage, int k0) {
+    float* Ah = reinterpret_cast<float*>(ssm + stage * S::STAGE_BYTES);
+    float* Al = Ah + BM * S::AS;
+    double* Bs = reinterpret_cast<double*>(ssm + stage * S::STAGE_BYTES + S::A_BYTES);
+    // A parts: BM rows x 16 floats = 4 copies of 16 bytes per row and part
+    for (int c = tid; c < 2 * BM * (BK / 4); c += S::THREADS) {
+      const int part = c / (BM * (BK / 4));
+      const int cc_ = c - part * BM * (BK / 4);
+      const int r = cc_ / (BK / 4), cc = (cc_ % (BK / 4)) * 4;
+      const bool ok = r < e.M;
+      const float* base = part ? e.Alo : e.Ahi;
+      const float* src = base + (size_t)(ok ? r : 0) * lda + k0 + cc;
+      cp_async16((part ? Al : Ah) + r * S::AS + cc, src, ok ? 16 : 0);
+    }
+    for (int c = tid; c < BK * (BN / 2); c += S::THREADS) {
+      const int r = c / (BN / 2), cc = (c % (BN / 2)) * 2;
+      const int gk = k0 + r, gn = n0 + cc;
+      const bool ok = (gk < e.K) && (gn < N);
+      const double* src = e.B + (ok ? ((size_t)gk * ldb + gn) : 0);
+      cp_async16(Bs + r * S::BS + cc, src, ok ? 16 : 0);
+    }
+    cp_async_commit();
+  };
+
+  float acc[TM][TN][4];
+#pragma unroll
+  for (int i = 0; i < TM; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+
+  const int nchunks = (e.K + BK - 1) / BK;
+  load_chunk(0, 0);
+  for (int c = 0; c < nchunks; ++c) {
+    if (c + 1 < nchunks) {
+      load_chunk((c + 1) & 1, (c + 1) * BK);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const float* Ah = reinterpret_cast<const float*>(ssm + (c & 1) * S::STAGE_BYTES);
+    const float* Al = Ah + BM * S::AS;
+    const double* Bs = reinterpret_cast<const double*>(ssm + (c & 1) * S::STAGE_BYTES + S::A_BYTES);
+#pragma unroll
+    for (int kk = 0; kk < BK; kk += 8) {
+      unsigned bh[TN][2], bl[TN][2];
+#pragma unroll
+      for (int j = 0; j < TN; ++j)
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const float x = (float)Bs[(kk + t + 4 * q) * S::BS + wn + j * 8 + g];
+          const unsigned h = tf32_bits(x);
+          bh[j][q] = h;
+          bl[j][q] = tf32_bits(x - __uint_as_float(h));
+        }
+#pragma unroll
+      for (int i = 0; i < TM; ++i) {
+        unsigned ah[4], al[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int row = wm + i * 16 + g + 8 * (q & 1);
+          const int col = kk + t + 4 * (q >> 1);
+          ah[q] = __float_as_uint(Ah[row * S::AS + col]);
+          al[q] = __float_as_uint(Al[row * S::AS + col]);
+        }
+#pragma unroll
+        for (int j = 0; j < TN; ++j) {
+          mma_tf32(acc[i][j], al, bh[j]);
+          mma_tf32(acc[i][j], ah, bl[j]);
+          mma_tf32(acc[i][j], ah, bh[j]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+
+#pragma unroll
+  for (int i = 0; i < TM; ++i) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int r = wm + i * 16 + g + 8 * h;
+      if (r >= e.M) continue;
+#pragma unroll
+      for (int j = 0; j < TN; ++j) {
+        const int col = n0 + wn + j * 8 + 2 * t;
+        if (col < N)
+          *reinterpret_cast<double2*>(e.C + (size_t)r * ldc + col) =
+              make_double2((double)acc[i][j][2 * h], (double)acc[i][j][2 * h + 1]);
+      }
+    }
+  }
+}
+
 }  // namespace jsd

@@ -20,7 +20,8 @@ namespace jsd {
 
 enum EqKind { kNS = 0, kPerturbation = 1, kDual = 2 };
 
-__device__ __forceinline__ void load_twiddles(double2* dst, const double2* __restrict__ src, int n) {
+template <typename C>
+__device__ __forceinline__ void load_twiddles(C* dst, const C* __restrict__ src, int n) {
   for (int i = threadIdx.x; i < n - 1; i += blockDim.x) dst[i] = src[i];
 }
 
@@ -40,33 +41,35 @@ struct ZinvSrc {
   int nsets;
 };
 
-__global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, ZinvSrc src,
-                       double2* __restrict__ inter) {
-  extern __shared__ __align__(16) double2 zsm[];
+template <typename C>
+__global__ void k_zinv(Geo g, FftDesc fz, const C* __restrict__ tw, ZinvSrc src, C* __restrict__ inter) {
+  using Rl = typename real_of<C>::type;
+  extern __shared__ __align__(16) unsigned char zsm_raw[];
+  C* zsm = reinterpret_cast<C*>(zsm_raw);
   const int pz = g.pz;
   const int L = fline(pz);
   const int nl = kZinvLines * src.nsets;
-  double2* twl = zsm;
-  double2* bufa = twl + pz;
-  double2* bufb = bufa + nl * L;
+  C* twl = zsm;
+  C* bufa = twl + pz;
+  C* bufb = bufa + nl * L;
   const int kx = blockIdx.x;
   const int y = blockIdx.y;
   load_twiddles(twl, tw, pz);
-  for (int i = threadIdx.x; i < nl * L; i += blockDim.x) bufa[i] = make_double2(0.0, 0.0);
+  for (int i = threadIdx.x; i < nl * L; i += blockDim.x) bufa[i] = cmake<C>(0, 0);
   __syncthreads();
   for (int i = threadIdx.x; i < 6 * src.nsets * g.mz; i += blockDim.x) {
     const int f = i / g.mz;  // input index 0 .. 6 nsets - 1
     const int iz = i - f * g.mz;
     const int set = f / 6, fi = f - set * 6;
     const int kz = signed_mode(iz, g.mz);
-    const double2 sv = sym_at(g, src.f[f], y, kx, kz);
+    const C sv = to_c<C>(sym_at(g, src.f[f], y, kx, kz));
     const int pos = fpad(kz >= 0 ? kz : pz + kz);
-    double2* lines = bufa + (size_t)set * kZinvLines * L;
+    C* lines = bufa + (size_t)set * kZinvLines * L;
     lines[fi * L + pos] = sv;
-    if (fi < 3) lines[(6 + fi) * L + pos] = cmul_ik(sv, kz * g.az);
+    if (fi < 3) lines[(6 + fi) * L + pos] = cmul_ik(sv, (Rl)(kz * g.az));
   }
   __syncthreads();
-  double2* res = fft_lines<true>(bufa, bufb, nl, fz, twl);
+  C* res = fft_lines<true>(bufa, bufb, nl, fz, twl);
   const int K1 = g.kx_max + 1;
   for (int i = threadIdx.x; i < nl * pz; i += blockDim.x) {
     const int f = i / pz;
@@ -93,56 +96,54 @@ __global__ void k_zinv(Geo g, FftDesc fz, const double2* __restrict__ tw, ZinvSr
 constexpr int kXmidThreads = 256;
 constexpr int kXmidEPT = 4;  // points per thread: ZB * px <= kXmidEPT * kXmidThreads
 
-template <int ZB>
+template <typename C, int ZB>
 struct XmidSmem {
   static size_t bytes(const Geo& g) {
-    return sizeof(double2) * ((size_t)g.px + 2 * 2 * (size_t)ZB * fline(g.px));
+    return sizeof(C) * ((size_t)g.px + 2 * 2 * (size_t)ZB * fline(g.px));
   }
 };
-
-__device__ __forceinline__ void zero_lines(double2* line, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) line[i] = make_double2(0.0, 0.0);
-}
 
 // Write ZB complete packed lines (zeros included) for fields (fa, fb) of the ZB
 // columns starting at `line` (no barrier). Threads run x-major over (x, zl) so
 // neighbouring threads read neighbouring z of one kx row of the intermediate.
-template <int ZB>
-__device__ __forceinline__ void fill_pair(const Geo& g, double2* line, const double2* __restrict__ inter, int y, int z0,
-                                          int fa, bool dxa, int fb, bool dxb) {
+template <typename C, int ZB>
+__device__ __forceinline__ void fill_pair(const Geo& g, C* line, const C* __restrict__ inter, int y, int z0, int fa,
+                                          bool dxa, int fb, bool dxb) {
+  using Rl = typename real_of<C>::type;
   const int px = g.px, K = g.kx_max, K1 = K + 1, L = fline(px);
   for (int i = threadIdx.x; i < ZB * px; i += blockDim.x) {
     const int x = i / ZB;
     const int zl = i - x * ZB;
     const int z = z0 + zl;
-    double2 out = make_double2(0.0, 0.0);
+    C out = cmake<C>(0, 0);
     const bool lo = x <= K, hi = x >= px - K;
     if ((lo || hi) && z < g.pz) {
       const int kx = lo ? x : px - x;
-      double2 A = inter[(((size_t)fa * g.ny + y) * K1 + kx) * g.pz + z];
-      double2 B = inter[(((size_t)fb * g.ny + y) * K1 + kx) * g.pz + z];
-      const double k = kx * g.ax;
+      C A = inter[(((size_t)fa * g.ny + y) * K1 + kx) * g.pz + z];
+      C B = inter[(((size_t)fb * g.ny + y) * K1 + kx) * g.pz + z];
+      const Rl k = (Rl)(kx * g.ax);
       if (dxa) A = cmul_ik(A, k);
       if (dxb) B = cmul_ik(B, k);
-      if (x == 0) out = make_double2(A.x, B.x);
-      else if (lo) out = make_double2(A.x - B.y, A.y + B.x);
-      else out = make_double2(A.x + B.y, B.x - A.y);
+      if (x == 0) out = cmake<C>(A.x, B.x);
+      else if (lo) out = cmake<C>(A.x - B.y, A.y + B.x);
+      else out = cmake<C>(A.x + B.y, B.x - A.y);
     }
     line[zl * L + fpad(x)] = out;
   }
 }
 
 // fill a batch of two pairs (2 ZB lines); no barrier
-template <int ZB>
-__device__ __forceinline__ void fill_two_pairs(const Geo& g, double2* la, const double2* __restrict__ inter, int y,
-                                               int z0, int fa1, bool dxa1, int fb1, bool dxb1, int fa2, bool dxa2,
-                                               int fb2, bool dxb2) {
-  fill_pair<ZB>(g, la, inter, y, z0, fa1, dxa1, fb1, dxb1);
-  fill_pair<ZB>(g, la + ZB * fline(g.px), inter, y, z0, fa2, dxa2, fb2, dxb2);
+template <typename C, int ZB>
+__device__ __forceinline__ void fill_two_pairs(const Geo& g, C* la, const C* __restrict__ inter, int y, int z0,
+                                               int fa1, bool dxa1, int fb1, bool dxb1, int fa2, bool dxa2, int fb2,
+                                               bool dxb2) {
+  fill_pair<C, ZB>(g, la, inter, y, z0, fa1, dxa1, fb1, dxb1);
+  fill_pair<C, ZB>(g, la + ZB * fline(g.px), inter, y, z0, fa2, dxa2, fb2, dxb2);
 }
 
 // value of point i (line zl = i / px, position x) of pair set `set` in r
-__device__ __forceinline__ double2 pair_value(const double2* r, int set, int zb, int px, int i) {
+template <typename C>
+__device__ __forceinline__ C pair_value(const C* r, int set, int zb, int px, int i) {
   const int L = fline(px);
   const int zl = i / px;
   const int x = i - zl * px;
@@ -150,86 +151,91 @@ __device__ __forceinline__ double2 pair_value(const double2* r, int set, int zb,
 }
 
 // forward FFT of (h0 + i h1) and (h2 + 0 i) lines and the kx >= 0 outputs
-template <int ZB>
-__device__ __forceinline__ void forward_and_store(const Geo& g, const FftDesc& fx, const double2* twl, double2* la,
-                                                  double2* lb, double2* __restrict__ out3, int y, int z0) {
+template <typename C, int ZB>
+__device__ __forceinline__ void forward_and_store(const Geo& g, const FftDesc& fx, const C* twl, C* la, C* lb,
+                                                  C* __restrict__ out3, int y, int z0) {
+  using Rl = typename real_of<C>::type;
   const int px = g.px, L = fline(px), K1 = g.kx_max + 1;
-  double2* r = fft_lines<false>(la, lb, 2 * ZB, fx, twl);
+  C* r = fft_lines<false>(la, lb, 2 * ZB, fx, twl);
+  const Rl half = (Rl)0.5;
   for (int i = threadIdx.x; i < ZB * K1; i += blockDim.x) {
     const int kx = i / ZB;
     const int zl = i - kx * ZB;
     const int z = z0 + zl;
     if (z >= g.pz) continue;
-    const double2 a = r[zl * L + fpad(kx)];
-    const double2 b = r[zl * L + fpad(kx == 0 ? 0 : px - kx)];
+    const C a = r[zl * L + fpad(kx)];
+    const C b = r[zl * L + fpad(kx == 0 ? 0 : px - kx)];
     // H0 = (Z[k] + conj Z[-k]) / 2, H1 = (Z[k] - conj Z[-k]) / (2 i)
-    out3[(((size_t)0 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y - b.y));
-    out3[(((size_t)1 * g.ny + y) * K1 + kx) * g.pz + z] = make_double2(0.5 * (a.y + b.y), -0.5 * (a.x - b.x));
+    out3[(((size_t)0 * g.ny + y) * K1 + kx) * g.pz + z] = cmake<C>(half * (a.x + b.x), half * (a.y - b.y));
+    out3[(((size_t)1 * g.ny + y) * K1 + kx) * g.pz + z] = cmake<C>(half * (a.y + b.y), -half * (a.x - b.x));
     out3[(((size_t)2 * g.ny + y) * K1 + kx) * g.pz + z] = r[(ZB + zl) * L + fpad(kx)];
   }
 }
 
-template <int ZB>
-__global__ void __launch_bounds__(kXmidThreads) k_xmid(Geo g, FftDesc fx, const double2* __restrict__ tw,
-                                                       const double2* __restrict__ inter, double2* __restrict__ out3,
+template <typename C, int ZB>
+__global__ void __launch_bounds__(kXmidThreads) k_xmid(Geo g, FftDesc fx, const C* __restrict__ tw,
+                                                       const C* __restrict__ inter, C* __restrict__ out3,
                                                        const double* __restrict__ ubase,
-                                                       const double* __restrict__ dubase, double lam) {
-  extern __shared__ __align__(16) double2 xsm[];
+                                                       const double* __restrict__ dubase, double lam_d) {
+  using Rl = typename real_of<C>::type;
+  extern __shared__ __align__(16) unsigned char xsm_raw[];
+  C* xsm = reinterpret_cast<C*>(xsm_raw);
   const int px = g.px, L = fline(px);
-  double2* twl = xsm;
-  double2* la = twl + px;
-  double2* lb = la + 2 * ZB * L;
+  C* twl = xsm;
+  C* la = twl + px;
+  C* lb = la + 2 * ZB * L;
   const int z0 = blockIdx.x * ZB;
   const int y = blockIdx.y;
-  const double ub = ubase ? ubase[y] : 0.0;
-  const double dub = dubase ? dubase[y] : 0.0;
-  const double c = g.c_inv;
+  const Rl ub = ubase ? (Rl)ubase[y] : (Rl)0;
+  const Rl dub = dubase ? (Rl)dubase[y] : (Rl)0;
+  const Rl c = (Rl)g.c_inv;
+  const Rl lam = (Rl)lam_d, half = (Rl)0.5;
   const int npt = ZB * px;
   load_twiddles(twl, tw, px);
-  double U[kXmidEPT], V[kXmidEPT], W[kXmidEPT], DIV[kXmidEPT], A0[kXmidEPT], A1[kXmidEPT], A2[kXmidEPT];
+  Rl U[kXmidEPT], V[kXmidEPT], W[kXmidEPT], DIV[kXmidEPT], A0[kXmidEPT], A1[kXmidEPT], A2[kXmidEPT];
 
   // intermediate: 0 u, 1 v, 2 w, 3 du/dy, 4 dv/dy, 5 dw/dy, 6 du/dz, 7 dv/dz, 8 dw/dz
   // Batches of two pairs; consuming batch b overlaps filling batch b + 1 when
   // the FFT result sits in lb (odd number of passes).
-  fill_two_pairs<ZB>(g, la, inter, y, z0, 0, false, 1, false, 2, false, 0, true);
+  fill_two_pairs<C, ZB>(g, la, inter, y, z0, 0, false, 1, false, 2, false, 0, true);
   __syncthreads();
-  double2* r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
+  C* r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
 #pragma unroll
   for (int e = 0; e < kXmidEPT; ++e) {
     const int i = threadIdx.x + e * blockDim.x;
     if (i >= npt) break;
-    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
+    const C p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
     U[e] = p.x * c;
     V[e] = p.y * c;
     W[e] = q.x * c;
-    const double dxu = q.y * c;
+    const Rl dxu = q.y * c;
     DIV[e] = dxu;
     A0[e] = lam * U[e] * dxu + ub * dxu;
   }
   if (r == la) __syncthreads();
-  fill_two_pairs<ZB>(g, la, inter, y, z0, 4, false, 8, false, 1, true, 2, true);
+  fill_two_pairs<C, ZB>(g, la, inter, y, z0, 4, false, 8, false, 1, true, 2, true);
   __syncthreads();
   r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
 #pragma unroll
   for (int e = 0; e < kXmidEPT; ++e) {
     const int i = threadIdx.x + e * blockDim.x;
     if (i >= npt) break;
-    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
-    const double dyv = p.x * c, dzw = p.y * c, dxv = q.x * c, dxw = q.y * c;
+    const C p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
+    const Rl dyv = p.x * c, dzw = p.y * c, dxv = q.x * c, dxw = q.y * c;
     DIV[e] += dyv + dzw;
     A1[e] = lam * V[e] * dyv + lam * U[e] * dxv + ub * dxv;
     A2[e] = lam * W[e] * dzw + lam * U[e] * dxw + ub * dxw;
   }
   if (r == la) __syncthreads();
-  fill_two_pairs<ZB>(g, la, inter, y, z0, 3, false, 5, false, 6, false, 7, false);
+  fill_two_pairs<C, ZB>(g, la, inter, y, z0, 3, false, 5, false, 6, false, 7, false);
   __syncthreads();
   r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
 #pragma unroll
   for (int e = 0; e < kXmidEPT; ++e) {
     const int i = threadIdx.x + e * blockDim.x;
     if (i >= npt) break;
-    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
-    const double dyu = p.x * c, dyw = p.y * c, dzu = q.x * c, dzv = q.y * c;
+    const C p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);
+    const Rl dyu = p.x * c, dyw = p.y * c, dzu = q.x * c, dzv = q.y * c;
     A0[e] += lam * V[e] * dyu + lam * W[e] * dzu;
     A2[e] += lam * V[e] * dyw;
     A1[e] += lam * W[e] * dzv;
@@ -240,16 +246,16 @@ __global__ void __launch_bounds__(kXmidThreads) k_xmid(Geo g, FftDesc fx, const 
   for (int e = 0; e < kXmidEPT; ++e) {
     const int i = threadIdx.x + e * blockDim.x;
     if (i >= npt) break;
-    const double d = DIV[e];
-    const double h0 = -A0[e] + 0.5 * lam * d * U[e] - V[e] * dub + 0.5 * d * ub;
-    const double h1 = -A1[e] + 0.5 * lam * d * V[e];
-    const double h2 = -A2[e] + 0.5 * lam * d * W[e];
+    const Rl d = DIV[e];
+    const Rl h0 = -A0[e] + half * lam * d * U[e] - V[e] * dub + half * d * ub;
+    const Rl h1 = -A1[e] + half * lam * d * V[e];
+    const Rl h2 = -A2[e] + half * lam * d * W[e];
     const int zl = i / px, x = i - zl * px;
-    la[zl * L + fpad(x)] = make_double2(h0, h1);
-    la[(ZB + zl) * L + fpad(x)] = make_double2(h2, 0.0);
+    la[zl * L + fpad(x)] = cmake<C>(h0, h1);
+    la[(ZB + zl) * L + fpad(x)] = cmake<C>(h2, (Rl)0);
   }
   __syncthreads();
-  forward_and_store<ZB>(g, fx, twl, la, lb, out3, y, z0);
+  forward_and_store<C, ZB>(g, fx, twl, la, lb, out3, y, z0);
 }
 
 // ---------------------------------------------------------------------------
@@ -258,46 +264,48 @@ __global__ void __launch_bounds__(kXmidThreads) k_xmid(Geo g, FftDesc fx, const 
 //   hel_i = -(Ut . grad) v_i + sum_j v_j d_i Ut_j + [(div u) v_i + (div v) Ut_i] / 4
 // Intermediate lines 0..8 hold v (v, dv/dy, dv/dz), 9..17 the same for u.
 // ---------------------------------------------------------------------------
-template <int ZB>
-__global__ void __launch_bounds__(kXmidThreads) k_xmid_dual(Geo g, FftDesc fx, const double2* __restrict__ tw,
-                                                            const double2* __restrict__ inter,
-                                                            double2* __restrict__ out3,
+template <typename C, int ZB>
+__global__ void __launch_bounds__(kXmidThreads) k_xmid_dual(Geo g, FftDesc fx, const C* __restrict__ tw,
+                                                            const C* __restrict__ inter, C* __restrict__ out3,
                                                             const double* __restrict__ ubase,
                                                             const double* __restrict__ dubase) {
-  extern __shared__ __align__(16) double2 xsm[];
+  using Rl = typename real_of<C>::type;
+  extern __shared__ __align__(16) unsigned char xsm_raw[];
+  C* xsm = reinterpret_cast<C*>(xsm_raw);
   const int px = g.px, L = fline(px);
-  double2* twl = xsm;
-  double2* la = twl + px;
-  double2* lb = la + 2 * ZB * L;
+  C* twl = xsm;
+  C* la = twl + px;
+  C* lb = la + 2 * ZB * L;
   const int z0 = blockIdx.x * ZB;
   const int y = blockIdx.y;
-  const double ub = ubase[y];
-  const double dub = dubase[y];
-  const double c = g.c_inv;
+  const Rl ub = (Rl)ubase[y];
+  const Rl dub = (Rl)dubase[y];
+  const Rl c = (Rl)g.c_inv;
+  const Rl q4 = (Rl)0.25;
   const int npt = ZB * px;
   load_twiddles(twl, tw, px);
-  double V0[kXmidEPT], V1[kXmidEPT], V2[kXmidEPT], U0[kXmidEPT], U1[kXmidEPT], U2[kXmidEPT];
-  double A0[kXmidEPT], A1[kXmidEPT], A2[kXmidEPT], DV[kXmidEPT], DU[kXmidEPT];
+  Rl V0[kXmidEPT], V1[kXmidEPT], V2[kXmidEPT], U0[kXmidEPT], U1[kXmidEPT], U2[kXmidEPT];
+  Rl A0[kXmidEPT], A1[kXmidEPT], A2[kXmidEPT], DV[kXmidEPT], DU[kXmidEPT];
 #define JSD_EACH(body)                                                        \
   _Pragma("unroll") for (int e = 0; e < kXmidEPT; ++e) {                      \
     const int i = threadIdx.x + e * blockDim.x;                               \
     if (i >= npt) break;                                                      \
-    const double2 p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i); \
-    const double pa = p.x * c, pb = p.y * c, qa = q.x * c, qb = q.y * c;      \
+    const C p = pair_value(r, 0, ZB, px, i), q = pair_value(r, 1, ZB, px, i);  \
+    const Rl pa = p.x * c, pb = p.y * c, qa = q.x * c, qb = q.y * c;          \
     body                                                                      \
   }                                                                           \
   if (r == la) __syncthreads();
 #define JSD_BATCH(fa1, dxa1, fb1, dxb1, fa2, dxa2, fb2, dxb2)                   \
-  fill_two_pairs<ZB>(g, la, inter, y, z0, fa1, dxa1, fb1, dxb1, fa2, dxa2, fb2, dxb2); \
+  fill_two_pairs<C, ZB>(g, la, inter, y, z0, fa1, dxa1, fb1, dxb1, fa2, dxa2, fb2, dxb2); \
   __syncthreads();                                                            \
   r = fft_lines<true>(la, lb, 2 * ZB, fx, twl);
   // (v0, v1) + (v2, u0)
-  double2* r = la;
+  C* r = la;
   JSD_BATCH(0, false, 1, false, 2, false, 9, false)
   JSD_EACH(V0[e] = pa; V1[e] = pb; V2[e] = qa; U0[e] = qb;)
   // (u1, u2) + (dv0/dx, dv1/dx)
   JSD_BATCH(10, false, 11, false, 0, true, 1, true)
-  JSD_EACH(U1[e] = pa; U2[e] = pb; const double ut = ub + U0[e]; A0[e] = -ut * qa; A1[e] = -ut * qb; DV[e] = qa;)
+  JSD_EACH(U1[e] = pa; U2[e] = pb; const Rl ut = ub + U0[e]; A0[e] = -ut * qa; A1[e] = -ut * qb; DV[e] = qa;)
   // (dv2/dx, dv0/dy) + (dv1/dy, dv2/dy)
   JSD_BATCH(2, true, 3, false, 4, false, 5, false)
   JSD_EACH(A2[e] = -(ub + U0[e]) * pa; A0[e] -= U1[e] * pb; A1[e] -= U1[e] * qa; A2[e] -= U1[e] * qb;
@@ -318,16 +326,16 @@ __global__ void __launch_bounds__(kXmidThreads) k_xmid_dual(Geo g, FftDesc fx, c
   for (int e = 0; e < kXmidEPT; ++e) {
     const int i = threadIdx.x + e * blockDim.x;
     if (i >= npt) break;
-    const double du = DU[e], dv = DV[e];
-    const double h0 = A0[e] + 0.25 * du * V0[e] + 0.25 * dv * (ub + U0[e]);
-    const double h1 = A1[e] + dub * V0[e] + 0.25 * du * V1[e] + 0.25 * dv * U1[e];
-    const double h2 = A2[e] + 0.25 * du * V2[e] + 0.25 * dv * U2[e];
+    const Rl du = DU[e], dv = DV[e];
+    const Rl h0 = A0[e] + q4 * du * V0[e] + q4 * dv * (ub + U0[e]);
+    const Rl h1 = A1[e] + dub * V0[e] + q4 * du * V1[e] + q4 * dv * U1[e];
+    const Rl h2 = A2[e] + q4 * du * V2[e] + q4 * dv * U2[e];
     const int zl = i / px, x = i - zl * px;
-    la[zl * L + fpad(x)] = make_double2(h0, h1);
-    la[(ZB + zl) * L + fpad(x)] = make_double2(h2, 0.0);
+    la[zl * L + fpad(x)] = cmake<C>(h0, h1);
+    la[(ZB + zl) * L + fpad(x)] = cmake<C>(h2, (Rl)0);
   }
   __syncthreads();
-  forward_and_store<ZB>(g, fx, twl, la, lb, out3, y, z0);
+  forward_and_store<C, ZB>(g, fx, twl, la, lb, out3, y, z0);
 }
 
 // ---------------------------------------------------------------------------
@@ -354,15 +362,17 @@ __device__ __forceinline__ void write_terms(const Geo& g, int y, int ix, int iz,
 }
 
 // forward z pass: block (kx in [0, K], y).
-__global__ void k_zfwd(Geo g, FftDesc fz, const double2* __restrict__ tw, const double2* __restrict__ out3,
+template <typename C>
+__global__ void k_zfwd(Geo g, FftDesc fz, const C* __restrict__ tw, const C* __restrict__ out3,
                        double2* __restrict__ q, double2* __restrict__ H1, double2* __restrict__ hg,
                        double2* __restrict__ conv00) {
-  extern __shared__ __align__(16) double2 fsm[];
+  extern __shared__ __align__(16) unsigned char fsm_raw[];
+  C* fsm = reinterpret_cast<C*>(fsm_raw);
   const int pz = g.pz;
   const int L = fline(pz);
-  double2* twl = fsm;
-  double2* bufa = twl + pz;
-  double2* bufb = bufa + 3 * L;
+  C* twl = fsm;
+  C* bufa = twl + pz;
+  C* bufb = bufa + 3 * L;
   const int kx = blockIdx.x;
   const int y = blockIdx.y;
   const int K1 = g.kx_max + 1;
@@ -373,10 +383,11 @@ __global__ void k_zfwd(Geo g, FftDesc fz, const double2* __restrict__ tw, const 
     bufa[f * L + fpad(z)] = out3[(((size_t)f * g.ny + y) * K1 + kx) * pz + z];
   }
   __syncthreads();
-  double2* F = fft_lines<false>(bufa, bufb, 3, fz, twl);
+  C* F = fft_lines<false>(bufa, bufb, 3, fz, twl);
   const double cf = g.c_fwd;
   auto getF = [&](int f, int kz) -> double2 {
-    return cscale(F[f * L + fpad(kz >= 0 ? kz : pz + kz)], cf);
+    const C v = F[f * L + fpad(kz >= 0 ? kz : pz + kz)];
+    return make_double2((double)v.x * cf, (double)v.y * cf);
   };
   const int K = g.kx_max;
   // rows this block owns: kx itself; -kx for 1 <= kx < K; the -K slot when kx = K

@@ -34,7 +34,12 @@ class JsdDesc(ctypes.Structure):
         ("D", _dp), ("V", _dp), ("Vinv", _dp), ("lam", _dp), ("sgn", _dp),
         ("c0", _dp), ("cN", _dp), ("w0", _dp), ("wN", _dp), ("y_weights", _dp),
         ("rhs_ns", _dp), ("lhs_inv_ns", _dp),
+        ("precision", ctypes.c_int),
     ]
+
+
+JSD_PRECISION_FP64 = 0
+JSD_PRECISION_MIXED = 1
 
 
 EXPORTED = (
@@ -44,7 +49,7 @@ EXPORTED = (
     "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc",
 )
 
-PROF_CLASSES = {"gemm": 0, "zinv": 1, "xmid": 2, "zfwd": 3, "eigen": 4, "linear": 5}
+PROF_CLASSES = {"gemm": 0, "zinv": 1, "xmid": 2, "zfwd": 3, "eigen": 4, "linear": 5, "sgemm": 6}
 
 _lib = None
 

@@ -42,7 +42,7 @@ class StepPlan:
 
     def __init__(self, modes, phys_ref, lx, lz, kind, re_tau, dt, dt_explicit=None, linearise=False,
                  constant_mass_flux=False, flow_rate_target=0.0, base_u: Optional[np.ndarray] = None,
-                 fft_sizes=None, device="cuda"):
+                 fft_sizes=None, device="cuda", precision: str = "fp64"):
         if not torch.cuda.is_available():
             raise _native.NativeError("the velocity-vorticity step needs a CUDA device")
         self.lib = _native.load()
@@ -80,6 +80,10 @@ class StepPlan:
         d.lam, d.sgn, d.c0, d.cN = arr(t.lam), arr(t.sgn), arr(t.c0), arr(t.cN)
         d.w0, d.wN, d.y_weights = arr(t.w0), arr(t.wN), arr(t.y_weights)
         d.rhs_ns, d.lhs_inv_ns = arr(rhs_ns), arr(lhs_inv_ns)
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        d.precision = _native.JSD_PRECISION_MIXED if precision == "mixed" else _native.JSD_PRECISION_FP64
+        self.precision = precision
         self.desc = d
         h = ctypes.c_void_p()
         with torch.cuda.device(self.device):
