@@ -163,7 +163,7 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    from jax_spectral_dns._plan import StepPlan, to_device_layout, to_reference_layout
+    from jax_spectral_dns._plan import GraphedSteps, StepPlan, to_device_layout, to_reference_layout
     from jax_spectral_dns.seeds import mode_counts
 
     modes, phys = mode_counts(SHAPE)
@@ -187,16 +187,21 @@ def run_ours(args):
 
     def timed(plan, sampler=None):
         """W warm-up steps, then K steps timed with CUDA events on the
-        launching stream, barrier + synchronize on both sides."""
+        launching stream, barrier + synchronize on both sides. The K steps
+        are one CUDA-graph replay (captured before the timed region)."""
         state = u0_dev.clone()
         dpdx = torch.tensor([dpdx0], dtype=torch.float64, device=dev)
         ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         plan.step(state, dpdx, 0, args.warmup)
+        graph = GraphedSteps(plan, state, dpdx, args.warmup, args.steps) if args.graph else None
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
         ev0.record(stream)
-        plan.step(state, dpdx, args.warmup, args.steps)
+        if graph is not None:
+            graph.replay()
+        else:
+            plan.step(state, dpdx, args.warmup, args.steps)
         ev1.record(stream)
         torch.cuda.synchronize()
         barrier()
@@ -286,6 +291,7 @@ def run_ours(args):
                 per_kernel[k]["tflops"] = v["work"] / (v["ms"] / 1e3) / 1e12
             else:
                 per_kernel[k]["gbs"] = v["work"] / (v["ms"] / 1e3) / 1e9
+        adj = None if args.no_adjoint else adjoint_leg(dev)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             rate, sec, sample, threads = cpu_reference_leg(1, 0)
@@ -301,6 +307,7 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "modes": list(modes), "fft_sizes": list(plan.fft_sizes),
                        "reference_physical_grid": list(phys), "parallelism": f"replicas x{world}",
                        "l2": "working set per step ~1 GB > 126 MB L2 (no flush needed)",
+                       "cuda_graph": bool(args.graph),
                        "precision": head},
             "forms": forms_out,
             "mixed_over_fp64": (forms_out["mixed"]["steps_per_s"] / forms_out["fp64"]["steps_per_s"]
@@ -311,12 +318,45 @@ def run_ours(args):
                     "d2h_bytes_per_step": state_bytes, "api": "StepPlan.step on host (pinned) state"},
             "gpu_launches": plan.launches_per_step() * args.steps,
             "roofline": roofline, "kernels": per_kernel, "clocks": clocks.summary(),
-            "cpu_baseline": cpu, "finite": finite,
+            "cpu_baseline": cpu, "finite": finite, "adjoint": adj,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def adjoint_leg(dev, checkpoint_every=50):
+    """Gain gradients per second on the 32x65x32 adjoint configuration
+    (Re = 3000, Lx = 2 pi, Lz = pi, T = 15, dt = 0.01: 1500 steps), linear and
+    nonlinear (E0 = 1e-4), with checkpoints every K steps; timed with CUDA events
+    against a forward-only pass of the same horizon."""
+    import torch
+    from jax_spectral_dns.adjoint import GainProblem
+    from jax_spectral_dns._plan import to_device_layout
+    from jax_spectral_dns.seeds import mode_counts, seeded_velocity_hat
+
+    shape, lx, lz, re, dt, T = (32, 65, 32), 2 * 3.141592653589793, 3.141592653589793, 3000.0, 0.01, 15.0
+    modes, phys = mode_counts(shape)
+    out = {"config": "32x65x32 (33x65x33 modes), Re=3000, T=15, dt=0.01 (1500 steps), seeded |k|<=8",
+           "checkpoint_every": checkpoint_every}
+    for lin, e0 in ((True, 1e-6), (False, 1e-4)):
+        p = GainProblem(modes, phys, lx, lz, re, dt, T, lin, checkpoint_every=checkpoint_every, device=dev)
+        u0 = to_device_layout(seeded_velocity_hat(shape, (lx, lz), (8, 8), e0, seed=0), device=dev)
+        p.gain_and_dual(u0)  # warm-up
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        e[0].record()
+        p.forward_checkpoints(u0)
+        e[1].record()
+        e[2].record()
+        g, _, _ = p.gain_and_dual(u0)
+        e[3].record()
+        torch.cuda.synchronize()
+        fwd_s, grad_s = e[0].elapsed_time(e[1]) / 1e3, e[2].elapsed_time(e[3]) / 1e3
+        out["linear" if lin else "nonlinear"] = {"grads_per_s": 1.0 / grad_s, "grad_s": grad_s, "forward_s": fwd_s,
+                                                  "cost_over_forward": grad_s / fwd_s, "gain": float(g.item())}
+    return out
 
 
 def measure_fp64_peak(dev) -> float:
@@ -346,6 +386,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint gradients/s leg")
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="launch the timed steps directly instead of replaying a captured CUDA graph")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="headline form; 'both' times FP64 and mixed and reports mixed beside FP64")
     args = ap.parse_args()

@@ -98,6 +98,13 @@ int jsd_plan_destroy(jsd_plan* plan);
  * (navier_stokes.py:1778-1813, 1219-1775). */
 int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* stream);
 
+/* jsd_step that also records the trajectory: states (device, n_steps + 1
+ * consecutive states) receives the initial state and the state after each
+ * step. Replaces solve_scan with write_entire_output (navier_stokes.py:1960-1990),
+ * the forward run the dual needs (navier_stokes_perturbation_dual.py:850-939). */
+int jsd_step_trajectory(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* states,
+                        void* stream);
+
 /* Dual equations: register the forward trajectory u_0 .. u_{n_states-1}
  * (device, n_states consecutive states). Dual step t uses u_{n_states-1-t}
  * for all three stages (navier_stokes_perturbation_dual.py:591-602). */

@@ -808,6 +808,21 @@ int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_st
   return 0;
 }
 
+int jsd_step_trajectory(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* states,
+                        void* stream) {
+  if (!plan || !state || !dpdx || !states || n_steps < 0) return fail(JSD_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t bytes = 3 * (size_t)plan->g.ny * plan->g.nk * sizeof(double2);
+  char* out = static_cast<char*>(states);
+  JSD_CUDA(cudaMemcpyAsync(out, state, bytes, cudaMemcpyDeviceToDevice, s));
+  for (int t = 0; t < n_steps; ++t) {
+    int rc = jsd_step(plan, state, dpdx, first_step + t, 1, stream);
+    if (rc) return rc;
+    JSD_CUDA(cudaMemcpyAsync(out + (size_t)(t + 1) * bytes, state, bytes, cudaMemcpyDeviceToDevice, s));
+  }
+  return 0;
+}
+
 int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* stream) {
   if (!plan || !state) return fail(JSD_ERR_ARG, "null argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -46,7 +46,7 @@ EXPORTED = (
     "jsd_plan_create", "jsd_plan_destroy", "jsd_step", "jsd_set_history",
     "jsd_correct_mass_flux", "jsd_energy", "jsd_flow_rate", "jsd_nonlinear_terms",
     "jsd_workspace_bytes", "jsd_launches_per_step", "jsd_last_error", "jsd_abi_version",
-    "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc",
+    "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc", "jsd_step_trajectory",
 )
 
 PROF_CLASSES = {"gemm": 0, "zinv": 1, "xmid": 2, "zfwd": 3, "eigen": 4, "linear": 5, "sgemm": 6}
@@ -73,6 +73,7 @@ def load(path: str = LIB_PATH):
     lib.jsd_plan_destroy.argtypes = [vp]
     lib.jsd_step.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
     lib.jsd_set_history.argtypes = [vp, vp, ctypes.c_int]
+    lib.jsd_step_trajectory.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
     lib.jsd_correct_mass_flux.argtypes = [vp, vp, vp, vp]
     lib.jsd_energy.argtypes = [vp, vp, vp, vp]
     lib.jsd_flow_rate.argtypes = [vp, vp, vp, vp]

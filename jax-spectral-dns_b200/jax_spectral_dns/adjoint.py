@@ -37,7 +37,7 @@ import torch
 
 from . import _native
 from ._ops import operator_tables
-from ._plan import StepPlan, to_device_layout, to_reference_layout
+from ._plan import GraphedSteps, StepPlan, to_device_layout, to_reference_layout
 from .seeds import cheb_points
 
 
@@ -45,7 +45,7 @@ class GainProblem:
     """Forward and dual plans for a perturbation problem about U = u_max (1 - y^2)."""
 
     def __init__(self, modes, phys, lx, lz, re, dt, end_time, linearise, u_max=1.0, checkpoint_every=10,
-                 precision="fp64", device="cuda"):
+                 precision="fp64", device="cuda", use_graphs=True):
         self.modes, self.phys = tuple(modes), tuple(phys)
         self.lx, self.lz = float(lx), float(lz)
         self.re_tau = float(re) / u_max
@@ -65,6 +65,49 @@ class GainProblem:
         w = torch.as_tensor(operator_tables(ny).y_weights, dtype=torch.float64, device=device)
         # Euclidean gradient = energy gradient * 2 * (c^2 / 4) * w_y (device layout (3, Ny, Mx, Mz))
         self.metric = (0.5 * c * c * w).view(1, ny, 1, 1)
+        # fixed working buffers so segments can replay captured CUDA graphs
+        self.use_graphs = use_graphs
+        shape = (3, ny, self.modes[0], self.modes[2])
+        self.w_fwd = torch.zeros(shape, dtype=torch.complex128, device=device)
+        self.w_dual = torch.zeros(shape, dtype=torch.complex128, device=device)
+        self.w_dp = torch.zeros(1, dtype=torch.float64, device=device)
+        self.w_ddp = torch.zeros(1, dtype=torch.float64, device=device)
+        self.w_traj = torch.zeros((self.K + 1,) + shape, dtype=torch.complex128, device=device)
+        self._graphs = {}
+
+    def _run(self, key, make):
+        """Replay the captured graph for `key` (capture on first use)."""
+        if not self.use_graphs:
+            make(None)
+            return
+        g = self._graphs.get(key)
+        if g is None:
+            g = self._graphs[key] = make(True)
+        g.replay()
+
+    def _fwd_steps(self, n: int) -> None:
+        def make(capture):
+            if capture:
+                return GraphedSteps(self.fwd, self.w_fwd, self.w_dp, 0, n)
+            self.fwd.step(self.w_fwd, self.w_dp, 0, n)
+        self._run(("fwd", n), make)
+
+    def _fwd_traj(self, n: int) -> None:
+        def make(capture):
+            if capture:
+                return GraphedSteps(self.fwd, self.w_fwd, self.w_dp, 0, n, trajectory=self.w_traj)
+            traj = self.fwd.step_trajectory(self.w_fwd, self.w_dp, 0, n)
+            self.w_traj[: n + 1].copy_(traj)
+        self._run(("traj", n), make)
+
+    def _dual_steps(self, n: int) -> None:
+        def make(capture):
+            if not self.linearise:
+                self.dual.set_history(self.w_traj[: n + 1])
+            if capture:
+                return GraphedSteps(self.dual, self.w_dual, self.w_ddp, 0, n)
+            self.dual.step(self.w_dual, self.w_ddp, 0, n)
+        self._run(("dual", n), make)
 
     # ---- pieces ----------------------------------------------------------
     def energy(self, state: torch.Tensor) -> torch.Tensor:
@@ -72,41 +115,34 @@ class GainProblem:
 
     def forward_checkpoints(self, u0_dev: torch.Tensor):
         """Run all steps; return the final state and the states at steps 0, K, 2K, ..."""
-        st = u0_dev.clone()
-        dp = torch.zeros(1, dtype=torch.float64, device=st.device)
-        cps = [st.clone()]
+        self.w_fwd.copy_(u0_dev)
+        self.w_dp.zero_()
+        cps = [u0_dev.clone()]
         t = 0
         while t < self.n_steps:
             n = min(self.K, self.n_steps - t)
-            self.fwd.step(st, dp, t, n)
+            self._fwd_steps(n)
             t += n
             if t < self.n_steps:
-                cps.append(st.clone())
-        return st, cps
+                cps.append(self.w_fwd.clone())
+        return self.w_fwd.clone(), cps
 
     def backward_dual(self, uT: torch.Tensor, cps) -> torch.Tensor:
         """Dual run from -u(T) to t = 0, recomputing each segment's forward
         states from its checkpoint when the dual needs them."""
-        v = (-uT).contiguous()
-        dp = torch.zeros(1, dtype=torch.float64, device=v.device)
+        self.w_dual.copy_(-uT)
+        self.w_ddp.zero_()
         bounds = list(range(0, self.n_steps, self.K)) + [self.n_steps]
         for seg in range(len(bounds) - 2, -1, -1):
             s0, s1 = bounds[seg], bounds[seg + 1]
             n = s1 - s0
             if not self.linearise:
-                traj = torch.empty((n + 1,) + tuple(v.shape), dtype=v.dtype, device=v.device)
-                traj[0].copy_(cps[seg])
-                st = cps[seg].clone()
-                fdp = torch.zeros(1, dtype=torch.float64, device=v.device)
-                for k in range(n):
-                    self.fwd.step(st, fdp, s0 + k, 1)
-                    traj[k + 1].copy_(st)
-                self.dual.set_history(traj)
+                self.w_fwd.copy_(cps[seg])
+                self.w_dp.zero_()
+                self._fwd_traj(n)
             # dual step t of this segment uses the segment state n - t
-            self.dual.step(v, dp, 0, n)
-            if not self.linearise:
-                self.dual.set_history(None)
-        return v
+            self._dual_steps(n)
+        return self.w_dual.clone()
 
     def gain_and_dual(self, u0_dev: torch.Tensor):
         uT, cps = self.forward_checkpoints(u0_dev)

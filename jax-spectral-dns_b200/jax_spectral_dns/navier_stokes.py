@@ -188,6 +188,9 @@ class NavierStokesVelVort(Equation):
         if not keep_trajectory:
             plan.step(state, dpdx, first_step, n_steps)
             return None, None
+        if not plan.desc.constant_mass_flux:
+            traj = plan.step_trajectory(state, dpdx, first_step, n_steps)
+            return traj, dpdx.expand(n_steps + 1).clone()
         traj = torch.empty((n_steps + 1,) + tuple(state.shape), dtype=state.dtype, device=state.device)
         dps = torch.empty(n_steps + 1, dtype=torch.float64, device=state.device)
         traj[0].copy_(state)
