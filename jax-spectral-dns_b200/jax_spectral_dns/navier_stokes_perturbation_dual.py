@@ -83,6 +83,20 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
         if plan._history is not traj:
             plan.set_history(traj)
 
+    def update_with_nse(self) -> None:
+        """Forget the previous forward/dual runs after the forward initial field
+        changed (..._dual.py:634-641)."""
+        self.forward_equation.write_entire_output = True
+        self.forward_equation.write_intermediate_output = False
+        self.clear_field("velocity_hat")
+        self.dPdx = 0.0
+        self.forward_equation.dPdx = 0.0
+        self.velocity_field_u_history = None
+        self.dPdx_history = None
+        self._forward_done = False
+        self._backward_done = False
+        self.forward_equation._trajectory_device = None
+
     def is_forward_calculation_done(self) -> bool:
         return self._forward_done
 
@@ -95,6 +109,7 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
         nse = self.forward_equation
         self.velocity_u_hat_0 = nse.get_initial_field("velocity_hat")
         if not self._forward_done:
+            nse.set_initial_field("velocity_hat", nse.get_initial_field("velocity_hat"))
             nse.write_entire_output = True
             nse.end_time = -1.0 * self.end_time
             traj, dps, _ = nse.solve_scan()

@@ -202,6 +202,35 @@ def case_dual_nonlin():
                (4, 4), 1e-4, 6, False)
 
 
+def case_cg_opt():
+    """Reference ConjugateGradientDescentSolver, 5 iterations, linearised
+    pseudo-2D 5x33x5, Re=3000, T=0.2 (20 steps): gain per iteration and the
+    final initial field."""
+    from jax_spectral_dns.gradient_descent_solver import ConjugateGradientDescentSolver
+
+    shape, lx, lz = (4, 33, 4), 2 * math.pi, 2 * math.pi * 1e-3
+    re, dt, n = 3000.0, 0.01, 20
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (1, 0), 1e-6, seed=7)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=True)
+    nse.activate_jit()
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse, checkpointing=False)
+    gains = []
+
+    solver = ConjugateGradientDescentSolver(dual, max_iterations=5, step_size=1e-2)
+    # the optimise() loop without its plotting post-processing (gradient_descent_solver.py:114-124)
+    solver.initialise(True)
+    solver.update_done(solver.i)
+    while not solver.done:
+        solver.update()
+        gains.append(float(solver.value))
+        solver.i += 1
+        solver.update_done(solver.i)
+    final = np.asarray(solver.current_guess.get_data()).copy()
+    _save("cg_opt_5x33x5", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n,
+          u0=u0, gains=np.array(gains), final_guess=final, final_value=float(solver.value))
+
+
 CASES = {
     "lin_pert": case_lin_pert,
     "lin_pert_gain": case_lin_pert_gain,
@@ -211,6 +240,7 @@ CASES = {
     "ns_cpg": case_ns_cpg,
     "dual_lin": case_dual_lin,
     "dual_nonlin": case_dual_nonlin,
+    "cg_opt": case_cg_opt,
 }
 
 if __name__ == "__main__":
