@@ -316,7 +316,7 @@ def run_ours(args):
             "mixed_error_steps": args.warmup + args.steps,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "api": "StepPlan.step on host (pinned) state"},
-            "gpu_launches": plan.launches_per_step() * args.steps,
+            "gpu_launches": plan.launches(args.steps),
             "roofline": roofline, "kernels": per_kernel, "clocks": clocks.summary(),
             "cpu_baseline": cpu, "finite": finite, "adjoint": adj,
         }

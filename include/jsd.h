@@ -154,8 +154,12 @@ int jsd_nonlinear_terms(jsd_plan* plan, const void* state, int time_step, void* 
 /* Bytes of device workspace the plan holds. */
 size_t jsd_workspace_bytes(const jsd_plan* plan);
 
-/* Number of kernel launches one call of jsd_step issues per time step. */
+/* Number of kernel launches one call of jsd_step issues per time step after
+ * its first; the first step of each call issues jsd_launches_first_step_extra
+ * more (it derives omega_y, and dv/dy for linearised plans, from the caller's
+ * state; later stages carry both from the previous stage's solve). */
 int jsd_launches_per_step(const jsd_plan* plan);
+int jsd_launches_first_step_extra(const jsd_plan* plan);
 
 /* Optional timing of kernel classes with CUDA events (no effect unless
  * enabled). jsd_profile_read returns and clears, for one class, the summed

@@ -146,6 +146,9 @@ struct jsd_plan {
   std::vector<void*> allocs;
   const double2* history = nullptr;
   int n_history = 0;
+  // Carried between stages of one jsd_step call: vnt / omnt hold V^-1 v and
+  // V^-1 omega_y of the current state, dvn holds dv/dy of the current state.
+  bool ev_valid = false, om_valid = false, dv_valid = false;
   // optional per-kernel-class timing with CUDA events (jsd_profile_*)
   bool profiling = false;
   std::vector<cudaEvent_t> ev_free;
@@ -322,18 +325,21 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
   const bool linear = p->desc.linearise && p->desc.kind != JSD_KIND_NS;
   if (p->desc.kind == JSD_KIND_DUAL && !linear && !uhist)
     return fail(JSD_ERR_STATE, "dual step needs the forward state (jsd_set_history)");
+  const double2* dv_in = p->dv_valid ? p->dvn : p->Dfld + fs;
   if (linear) {
-    const double* src[1] = {(const double*)v};
-    double* dst[1] = {(double*)(p->Dfld + fs)};
-    int rc = launch_dfield(p, src, dst, 1, s);
-    if (rc) return rc;
+    if (!p->dv_valid) {
+      const double* src[1] = {(const double*)v};
+      double* dst[1] = {(double*)(p->Dfld + fs)};
+      int rc = launch_dfield(p, src, dst, 1, s);
+      if (rc) return rc;
+    }
     const int blk = 256;
     ProfScope ps(p, JSD_PROF_LINEAR, sizeof(double2) * 7.0 * fs, s);
     if (p->desc.kind == JSD_KIND_PERTURBATION)
-      k_linear_terms<kPerturbation><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, p->Dfld + fs, p->ub, p->dub,
+      k_linear_terms<kPerturbation><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, dv_in, p->ub, p->dub,
                                                                       p->q, p->H1, p->hg, conv);
     else
-      k_linear_terms<kDual><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, p->Dfld + fs, p->ub, p->dub, p->q,
+      k_linear_terms<kDual><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, dv_in, p->ub, p->dub, p->q,
                                                               p->H1, p->hg, conv);
     JSD_LAUNCHED("k_linear_terms");
     return 0;
@@ -343,15 +349,18 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
   {
     const double* src[6];
     double* dst[6];
+    int cnt = 0;
     for (int c = 0; c < 3; ++c) {
-      src[c] = (const double*)(state + c * fs);
-      dst[c] = (double*)(p->Dfld + c * fs);
-      if (dual) {
-        src[3 + c] = (const double*)(uhist + c * fs);
-        dst[3 + c] = (double*)(p->Dfld + (3 + c) * fs);
-      }
+      if (c == 1 && p->dv_valid) continue;  // dv/dy of the state is already in dvn
+      src[cnt] = (const double*)(state + c * fs);
+      dst[cnt++] = (double*)(p->Dfld + c * fs);
     }
-    int rc = launch_dfield(p, src, dst, 3 * nsets, s);
+    if (dual)
+      for (int c = 0; c < 3; ++c) {
+        src[cnt] = (const double*)(uhist + c * fs);
+        dst[cnt++] = (double*)(p->Dfld + (3 + c) * fs);
+      }
+    int rc = launch_dfield(p, src, dst, cnt, s);
     if (rc) return rc;
   }
   return p->mixed ? transforms<float2>(p, state, uhist, conv, s) : transforms<double2>(p, state, uhist, conv, s);
@@ -374,7 +383,7 @@ int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2*
     src.nsets = nsets;
     for (int c = 0; c < 3; ++c) {
       src.f[c] = state + c * fs;
-      src.f[3 + c] = p->Dfld + c * fs;
+      src.f[3 + c] = (c == 1 && p->dv_valid) ? p->dvn : p->Dfld + c * fs;
       if (dual) {
         src.f[6 + c] = uhist + c * fs;
         src.f[9 + c] = p->Dfld + (3 + c) * fs;
@@ -428,8 +437,10 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
   int rc = nonlinear(p, state, uhist, st, s);
   if (rc) return rc;
   const int blk = 256;
-  k_omega<<<grid_for(fs, blk), blk, 0, s>>>(g, u, w, p->om);
-  JSD_LAUNCHED("k_omega");
+  if (!p->om_valid) {
+    k_omega<<<grid_for(fs, blk), blk, 0, s>>>(g, u, w, p->om);
+    JSD_LAUNCHED("k_omega");
+  }
   // eigenbasis transforms
   {
     GemmBatch b = gemm_batch(p);
@@ -438,8 +449,8 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     add_entry(b, p->VinvD, (const double*)p->q, p->X1, ni, ny);
     add_entry(b, p->Vinv, (const double*)p->H1 + rowd, p->T + 0 * E, ni, ni);
     add_entry(b, p->Vinv, (const double*)p->hg + rowd, p->T + 1 * E, ni, ni);
-    add_entry(b, p->Vinv, (const double*)v + rowd, p->T + 2 * E, ni, ni);
-    add_entry(b, p->Vinv, (const double*)p->om + rowd, p->T + 3 * E, ni, ni);
+    if (!p->ev_valid) add_entry(b, p->Vinv, (const double*)v + rowd, p->T + 2 * E, ni, ni);
+    if (!p->om_valid) add_entry(b, p->Vinv, (const double*)p->om + rowd, p->T + 3 * E, ni, ni);
     rc = launch_gemm(p, b, ni, s);
     if (rc) return rc;
   }
@@ -451,8 +462,11 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     const size_t E = p->edoubles;
     // reads X1, 4 transformed fields, 2 old terms; writes 2 old terms, v~ twice, om~
     ProfScope ps(p, JSD_PROF_EIGEN, sizeof(double) * 13.0 * (double)E, s);
-    k_eigen_update<<<(N + kEigCols - 1) / kEigCols, kEigCols * kEigParts, 0, s>>>(g, t, sc, p->X1, p->T, p->T + E, p->T + 2 * E, p->T + 3 * E,
-                                                   (const double*)v, p->hv_old, p->hg_old, p->vnt, p->omnt);
+    // v~ and om~ are read and overwritten in place when carried from the last stage
+    const double* vt = p->ev_valid ? p->vnt : p->T + 2 * E;
+    const double* omt = p->om_valid ? p->omnt : p->T + 3 * E;
+    k_eigen_update<<<(N + kEigCols - 1) / kEigCols, kEigCols * kEigParts, 0, s>>>(
+        g, t, sc, p->X1, p->T, p->T + E, vt, omt, (const double*)v, p->hv_old, p->hg_old, p->vnt, p->omnt);
     JSD_LAUNCHED("k_eigen_update");
   }
   {
@@ -476,6 +490,8 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
   }
   k_reconstruct<<<grid_for(fs, blk), blk, 0, s>>>(g, p->dvn, p->om, p->uw00, u, v, w);
   JSD_LAUNCHED("k_reconstruct");
+  // the back-transform left V^-1 v, V^-1 omega_y and dv/dy of the new state
+  p->ev_valid = p->om_valid = p->dv_valid = true;
   return 0;
 }
 
@@ -490,6 +506,7 @@ int mass_flux(jsd_plan* p, double2* state, double* dpdx, cudaStream_t s) {
   k_roundtrip_shift<<<grid_for(fs, 256), 256, 0, s>>>(g, state, p->scal, p->tmp);
   JSD_LAUNCHED("k_roundtrip_shift");
   JSD_CUDA(cudaMemcpyAsync(state, p->tmp, fs * sizeof(double2), cudaMemcpyDeviceToDevice, s));
+  p->om_valid = false;  // u changed; v (and so V^-1 v, dv/dy) did not
   return 0;
 }
 
@@ -627,11 +644,25 @@ const char* jsd_last_error(void) { return g_last_error.c_str(); }
 
 size_t jsd_workspace_bytes(const jsd_plan* plan) { return plan ? plan->ws_bytes : 0; }
 
+int jsd_launches_first_step_extra(const jsd_plan* plan) {
+  if (!plan) return 0;
+  const bool linear = plan->desc.linearise && plan->desc.kind != JSD_KIND_NS;
+  // the first stage of a call derives omega_y (k_omega) and, for the linear
+  // terms, dv/dy (one GEMM) from the caller's state
+  const bool cmf = plan->desc.constant_mass_flux != 0;
+  return (cmf ? 0 : 1) + (linear ? 1 : 0);
+}
+
 int jsd_launches_per_step(const jsd_plan* plan) {
   if (!plan) return 0;
   const bool linear = plan->desc.linearise && plan->desc.kind != JSD_KIND_NS;
-  const int per_stage = linear ? 8 : 10;
-  return 3 * per_stage + (plan->desc.constant_mass_flux ? 3 : 0);
+  // steady state: each stage launches dfield (not for the linear terms, which take
+  // dv/dy carried from the last stage), nonlinear terms (3 transforms or 1 linear
+  // kernel), 2 GEMMs, eigen update, mean flow and reconstruct; omega_y is carried
+  // too, except after the mass-flux correction (3 launches) changed u
+  const int per_stage = linear ? 6 : 9;
+  const bool cmf = plan->desc.constant_mass_flux != 0;
+  return 3 * per_stage + (cmf ? 3 + 1 : 0);
 }
 
 int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
@@ -791,10 +822,8 @@ int jsd_set_history(jsd_plan* plan, const void* states, int n_states) {
   return 0;
 }
 
-int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* stream) {
-  if (!plan || !state || !dpdx || n_steps < 0) return fail(JSD_ERR_ARG, "null argument");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
-  double2* st = static_cast<double2*>(state);
+// n_steps full steps; uses (and refreshes) the carried eigen-space state
+int run_steps(jsd_plan* plan, double2* st, double* dpdx, int first_step, int n_steps, cudaStream_t s) {
   for (int t = 0; t < n_steps; ++t) {
     for (int k = 0; k < 3; ++k) {
       int rc = stage(plan, st, dpdx, k, first_step + t, s);
@@ -808,6 +837,12 @@ int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_st
   return 0;
 }
 
+int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* stream) {
+  if (!plan || !state || !dpdx || n_steps < 0) return fail(JSD_ERR_ARG, "null argument");
+  plan->ev_valid = plan->om_valid = plan->dv_valid = false;  // the caller may have changed the state
+  return run_steps(plan, static_cast<double2*>(state), dpdx, first_step, n_steps, static_cast<cudaStream_t>(stream));
+}
+
 int jsd_step_trajectory(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* states,
                         void* stream) {
   if (!plan || !state || !dpdx || !states || n_steps < 0) return fail(JSD_ERR_ARG, "null argument");
@@ -815,8 +850,9 @@ int jsd_step_trajectory(jsd_plan* plan, void* state, double* dpdx, int first_ste
   const size_t bytes = 3 * (size_t)plan->g.ny * plan->g.nk * sizeof(double2);
   char* out = static_cast<char*>(states);
   JSD_CUDA(cudaMemcpyAsync(out, state, bytes, cudaMemcpyDeviceToDevice, s));
+  plan->ev_valid = plan->om_valid = plan->dv_valid = false;
   for (int t = 0; t < n_steps; ++t) {
-    int rc = jsd_step(plan, state, dpdx, first_step + t, 1, stream);
+    int rc = run_steps(plan, static_cast<double2*>(state), dpdx, first_step + t, 1, s);
     if (rc) return rc;
     JSD_CUDA(cudaMemcpyAsync(out + (size_t)(t + 1) * bytes, state, bytes, cudaMemcpyDeviceToDevice, s));
   }
@@ -827,6 +863,7 @@ int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* strea
   if (!plan || !state) return fail(JSD_ERR_ARG, "null argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* dp = dpdx ? dpdx : plan->scal + 1;  // a scratch slot when the caller keeps no pressure gradient
+  plan->ev_valid = plan->om_valid = plan->dv_valid = false;
   return mass_flux(plan, static_cast<double2*>(state), dp, s);
 }
 
@@ -864,6 +901,7 @@ int jsd_nonlinear_terms(jsd_plan* plan, const void* state, int time_step, void* 
     if (idx < 0) return fail(JSD_ERR_ARG, "time step beyond the registered forward history");
     uhist = plan->history + (size_t)idx * 3 * fs;
   }
+  plan->ev_valid = plan->om_valid = plan->dv_valid = false;
   int rc = nonlinear(plan, static_cast<const double2*>(state), uhist, 0, s);
   if (rc) return rc;
   GemmBatch b = gemm_batch(plan);

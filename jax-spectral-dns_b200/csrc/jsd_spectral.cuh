@@ -513,9 +513,12 @@ constexpr int kEigParts = 4;    // warps per block, each walking a quarter of th
 
 __global__ void __launch_bounds__(kEigCols * kEigParts) k_eigen_update(
     Geo g, EigTables t, StageCoef sc, const double* __restrict__ X1, const double* __restrict__ H1t,
-    const double* __restrict__ hgt, const double* __restrict__ vt, const double* __restrict__ omt,
+    const double* __restrict__ hgt, const double* vt, const double* omt,
     const double* __restrict__ vfield, double* __restrict__ hv_old, double* __restrict__ hg_old,
-    double* __restrict__ vnt, double* __restrict__ omnt) {
+    double* vnt, double* omnt) {
+  // vt may alias vnt and omt may alias omnt (states carried from the previous
+  // stage are updated in place): each element is read by the thread that
+  // then overwrites it, and by no other thread
   __shared__ double red[kEigParts][6][kEigCols];
   const int N = 2 * g.nk;
   const int lane = threadIdx.x % kEigCols;

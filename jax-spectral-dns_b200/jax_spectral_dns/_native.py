@@ -47,6 +47,7 @@ EXPORTED = (
     "jsd_correct_mass_flux", "jsd_energy", "jsd_flow_rate", "jsd_nonlinear_terms",
     "jsd_workspace_bytes", "jsd_launches_per_step", "jsd_last_error", "jsd_abi_version",
     "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc", "jsd_step_trajectory",
+    "jsd_launches_first_step_extra",
 )
 
 PROF_CLASSES = {"gemm": 0, "zinv": 1, "xmid": 2, "zfwd": 3, "eigen": 4, "linear": 5, "sgemm": 6}
@@ -81,6 +82,7 @@ def load(path: str = LIB_PATH):
     lib.jsd_workspace_bytes.argtypes = [vp]
     lib.jsd_workspace_bytes.restype = ctypes.c_size_t
     lib.jsd_launches_per_step.argtypes = [vp]
+    lib.jsd_launches_first_step_extra.argtypes = [vp]
     lib.jsd_last_error.restype = ctypes.c_char_p
     lib.jsd_energy_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_double, ctypes.c_double, vp, vp, vp]

@@ -107,7 +107,14 @@ class StepPlan:
         return int(self.lib.jsd_workspace_bytes(self.handle))
 
     def launches_per_step(self) -> int:
+        """Kernel launches per step after the first of a `step` call."""
         return int(self.lib.jsd_launches_per_step(self.handle))
+
+    def launches(self, n_steps: int) -> int:
+        """Kernel launches of one `step(state, dpdx, t, n_steps)` call."""
+        if n_steps <= 0:
+            return 0
+        return n_steps * self.launches_per_step() + int(self.lib.jsd_launches_first_step_extra(self.handle))
 
     def step(self, state: torch.Tensor, dpdx: torch.Tensor, first_step: int, n_steps: int):
         """Advance a device-layout state in place; dpdx is a 1-element float64 device tensor."""

@@ -1,5 +1,6 @@
 """CUDA-graph replay of the step loop gives bit-identical results to direct
-launches (forward with constant mass flux, and the graphed adjoint segments)."""
+launches of the same calls (forward with constant mass flux, and the graphed
+adjoint segments)."""
 import numpy as np
 import pytest
 import torch
@@ -21,7 +22,10 @@ def test_graph_replay_matches_direct_steps(cuda):
                  flow_rate_target=q0)
     a = to_device_layout(d["u0"])
     da = torch.tensor([float(d["dpdx"][0])], dtype=torch.float64, device="cuda")
-    p.step(a, da, 0, 10)
+    # two calls of 5 steps, as the graph below: each call derives the carried
+    # eigen-space state from its input, so the chunking is part of the rounding
+    p.step(a, da, 0, 5)
+    p.step(a, da, 0, 5)
     b = to_device_layout(d["u0"])
     db = torch.tensor([float(d["dpdx"][0])], dtype=torch.float64, device="cuda")
     g = GraphedSteps(p, b, db, 0, 5)
