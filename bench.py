@@ -51,6 +51,29 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+KERNEL_NAMES = {"gemm": "k_dgemm", "sgemm": "k_sgemm3", "zinv": "k_zinv", "xmid": "k_xmid", "zfwd": "k_zfwd",
+                "eigen": "k_eigen_update"}
+
+
+def _ncu_traffic(kernel: str, form: str):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary of the benchmark workload, or None when there is none."""
+    import re
+    path = os.path.join(REPO, "profiles", f"{kernel}_channel_128x129x128.md")
+    try:
+        text = open(path).read()
+    except OSError:
+        return None
+    m = re.search(r"DRAM traffic per launch \(read \+ write, MB\):(.*)", text)
+    if not m:
+        return None
+    vals = dict(kv.split("=") for kv in m.group(1).split())
+    if form in vals:
+        return float(vals[form]) * 1e6
+    launches = [float(v) for k, v in vals.items() if k.startswith("launch")]
+    return sum(launches) / len(launches) * 1e6 if launches else None
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -277,13 +300,18 @@ def run_ours(args):
                             "frac": achieved / fp64_peak,
                             "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 has no "
                                            "entry in MEASURED_PEAKS.json)",
-                            "traffic": None, "share_of_kernel_time": k["ms"] / total_k}
+                            "traffic": _ncu_traffic("k_dgemm", head), "share_of_kernel_time": k["ms"] / total_k}
             else:
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e9
-                roofline = {"kernel": "k_" + dom, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"],
-                            "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                roofline = {"kernel": KERNEL_NAMES[dom], "bound": "hbm", "achieved": achieved,
+                            "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                             "peak_source": peak_src + " (MEASURED_PEAKS.json hbm_gbs)",
-                            "traffic": None, "share_of_kernel_time": k["ms"] / total_k}
+                            "traffic": _ncu_traffic(KERNEL_NAMES[dom], head),
+                            "algorithmic_bytes_per_launch": k["work"] / k["launches"],
+                            "share_of_kernel_time": k["ms"] / total_k}
+            if roofline["traffic"] is not None:
+                roofline["traffic_source"] = ("dram__bytes_read.sum + dram__bytes_write.sum per launch, "
+                                              f"profiles/{roofline['kernel'].split()[0]}_channel_128x129x128.md")
         per_kernel = {k: {"avg_us": 1e3 * v["ms"] / v["launches"], "launches": v["launches"],
                           "share": v["ms"] / total_k} for k, v in kernels.items()}
         for k, v in kernels.items():
