@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <string>
 #include <vector>
 
@@ -141,6 +142,7 @@ struct jsd_plan {
   double2 *conv = nullptr;     // 3 stages x 2 ny
   double2 *uw00 = nullptr;     // 2 ny
   double *X1 = nullptr, *T = nullptr, *hv_old = nullptr, *hg_old = nullptr, *vnt = nullptr, *omnt = nullptr;
+  double *vnt_alt = nullptr, *omnt_alt = nullptr;  // ping-pong partners of vnt / omnt
   double *partial = nullptr, *scal = nullptr;
   size_t ws_bytes = 0;
   std::vector<void*> allocs;
@@ -462,9 +464,12 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     const size_t E = p->edoubles;
     // reads X1, 4 transformed fields, 2 old terms; writes 2 old terms, v~ twice, om~
     ProfScope ps(p, JSD_PROF_EIGEN, sizeof(double) * 13.0 * (double)E, s);
-    // v~ and om~ are read and overwritten in place when carried from the last stage
+    // v~ and om~ carried from the last stage are read from vnt / omnt and the
+    // update goes to their ping-pong partners, which then become vnt / omnt
     const double* vt = p->ev_valid ? p->vnt : p->T + 2 * E;
     const double* omt = p->om_valid ? p->omnt : p->T + 3 * E;
+    if (p->ev_valid) std::swap(p->vnt, p->vnt_alt);
+    if (p->om_valid) std::swap(p->omnt, p->omnt_alt);
     k_eigen_update<<<(N + kEigCols - 1) / kEigCols, kEigCols * kEigParts, 0, s>>>(
         g, t, sc, p->X1, p->T, p->T + E, vt, omt, (const double*)v, p->hv_old, p->hg_old, p->vnt, p->omnt);
     JSD_LAUNCHED("k_eigen_update");
@@ -799,7 +804,7 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(dev_alloc(p, (void**)&p->uw00, n2 * sizeof(double2)));
   JSD_TRY(dev_alloc(p, (void**)&p->X1, p->edoubles * sizeof(double)));
   JSD_TRY(dev_alloc(p, (void**)&p->T, 4 * p->edoubles * sizeof(double)));
-  for (double** f : {&p->hv_old, &p->hg_old, &p->vnt, &p->omnt})
+  for (double** f : {&p->hv_old, &p->hg_old, &p->vnt, &p->omnt, &p->vnt_alt, &p->omnt_alt})
     JSD_TRY(dev_alloc(p, (void**)f, p->edoubles * sizeof(double)));
   JSD_TRY(dev_alloc(p, (void**)&p->partial, (size_t)ny * sizeof(double)));
   JSD_TRY(dev_alloc(p, (void**)&p->scal, 8 * sizeof(double)));

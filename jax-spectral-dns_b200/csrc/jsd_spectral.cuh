@@ -510,15 +510,13 @@ struct StageCoef {
 
 constexpr int kEigCols = 32;    // columns per block (one warp-wide row segment)
 constexpr int kEigParts = 4;    // warps per block, each walking a quarter of the eigen rows
+constexpr int kEigBatch = 4;    // rows whose loads are issued together (loads in flight per thread: 7 x batch)
 
-__global__ void __launch_bounds__(kEigCols * kEigParts) k_eigen_update(
+__global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
     Geo g, EigTables t, StageCoef sc, const double* __restrict__ X1, const double* __restrict__ H1t,
-    const double* __restrict__ hgt, const double* vt, const double* omt,
+    const double* __restrict__ hgt, const double* __restrict__ vt, const double* __restrict__ omt,
     const double* __restrict__ vfield, double* __restrict__ hv_old, double* __restrict__ hg_old,
-    double* vnt, double* omnt) {
-  // vt may alias vnt and omt may alias omnt (states carried from the previous
-  // stage are updated in place): each element is read by the thread that
-  // then overwrites it, and by no other thread
+    double* __restrict__ vnt, double* __restrict__ omnt) {
   __shared__ double red[kEigParts][6][kEigCols];
   const int N = 2 * g.nk;
   const int lane = threadIdx.x % kEigCols;
@@ -540,32 +538,53 @@ __global__ void __launch_bounds__(kEigCols * kEigParts) k_eigen_update(
   const double br = sc.beta * sc.dt / sc.re;
   double d0p = 0, dNp = 0, d0a = 0, dNa = 0, d0b = 0, dNb = 0;
   if (active) {
-#pragma unroll 4
-    for (int j = j0; j < j1; ++j) {
-      const size_t o = (size_t)j * N + c;
-      const double L = t.lam[j] - k2;
-      const double R = 1.0 + ar * L;
-      const double H = 1.0 - br * L;
-      const double ih = 1.0 / H;
-      const double ihl = ih / L;
-      const double hv = -X1[o] - k2 * H1t[o];
-      const double hvo = sc.first ? 0.0 : hv_old[o];
-      const double phi = L * vt[o] + t.c0[j] * v0 + t.cN[j] * vN;
-      const double vp = (R * phi + sc.dt_e * (sc.gamma * hv + sc.xi * hvo)) * ihl;
-      const double va = br * t.c0[j] * ihl;
-      const double w0 = t.w0[j], wN = t.wN[j], sg = t.sgn[j];
-      d0p += w0 * vp;
-      dNp += wN * vp;
-      d0a += w0 * va;
-      dNa += wN * va;
-      d0b += w0 * sg * va;
-      dNb += wN * sg * va;
-      vnt[o] = vp;
-      hv_old[o] = hv;
-      const double hg = hgt[o];
-      const double hgo = sc.first ? 0.0 : hg_old[o];
-      omnt[o] = (R * omt[o] + sc.dt_e * (sc.gamma * hg + sc.xi * hgo)) * ih;
-      hg_old[o] = hg;
+    for (int jb = j0; jb < j1; jb += kEigBatch) {
+      // all loads of the batch first (independent rows), then the arithmetic
+      double x1[kEigBatch], h1[kEigBatch], hg[kEigBatch], vv[kEigBatch], om[kEigBatch], hvo[kEigBatch],
+          hgo[kEigBatch];
+#pragma unroll
+      for (int b = 0; b < kEigBatch; ++b) {
+        const int j = jb + b;
+        x1[b] = h1[b] = hg[b] = vv[b] = om[b] = hvo[b] = hgo[b] = 0.0;
+        if (j < j1) {
+          const size_t o = (size_t)j * N + c;
+          x1[b] = X1[o];
+          h1[b] = H1t[o];
+          hg[b] = hgt[o];
+          vv[b] = vt[o];
+          om[b] = omt[o];
+          if (!sc.first) {
+            hvo[b] = hv_old[o];
+            hgo[b] = hg_old[o];
+          }
+        }
+      }
+#pragma unroll
+      for (int b = 0; b < kEigBatch; ++b) {
+        const int j = jb + b;
+        if (j >= j1) break;
+        const size_t o = (size_t)j * N + c;
+        const double L = t.lam[j] - k2;
+        const double R = 1.0 + ar * L;
+        const double H = 1.0 - br * L;
+        const double ih = 1.0 / H;
+        const double ihl = ih / L;
+        const double hv = -x1[b] - k2 * h1[b];
+        const double phi = L * vv[b] + t.c0[j] * v0 + t.cN[j] * vN;
+        const double vp = (R * phi + sc.dt_e * (sc.gamma * hv + sc.xi * hvo[b])) * ihl;
+        const double va = br * t.c0[j] * ihl;
+        const double w0 = t.w0[j], wN = t.wN[j], sg = t.sgn[j];
+        d0p += w0 * vp;
+        dNp += wN * vp;
+        d0a += w0 * va;
+        dNa += wN * va;
+        d0b += w0 * sg * va;
+        dNb += wN * sg * va;
+        vnt[o] = vp;
+        hv_old[o] = hv;
+        omnt[o] = (R * om[b] + sc.dt_e * (sc.gamma * hg[b] + sc.xi * hgo[b])) * ih;
+        hg_old[o] = hg[b];
+      }
     }
   }
   red[part][0][lane] = d0p;
@@ -588,12 +607,20 @@ __global__ void __launch_bounds__(kEigCols * kEigParts) k_eigen_update(
   const double ra = -sum[0], rb = -sum[1];
   const double a = (sum[5] * ra - sum[4] * rb) / det;
   const double b = (-sum[3] * ra + sum[2] * rb) / det;
-  for (int j = j0; j < j1; ++j) {
-    const size_t o = (size_t)j * N + c;
-    const double L = t.lam[j] - k2;
-    const double H = 1.0 - br * L;
-    const double va = br * t.c0[j] / (H * L);
-    vnt[o] += (a + b * t.sgn[j]) * va;
+  for (int jb = j0; jb < j1; jb += kEigBatch) {
+    double vp[kEigBatch];
+#pragma unroll
+    for (int q = 0; q < kEigBatch; ++q)
+      vp[q] = (jb + q < j1) ? vnt[(size_t)(jb + q) * N + c] : 0.0;
+#pragma unroll
+    for (int q = 0; q < kEigBatch; ++q) {
+      const int j = jb + q;
+      if (j >= j1) break;
+      const double L = t.lam[j] - k2;
+      const double H = 1.0 - br * L;
+      const double va = br * t.c0[j] / (H * L);
+      vnt[(size_t)j * N + c] = vp[q] + (a + b * t.sgn[j]) * va;
+    }
   }
 }
 
