@@ -18,6 +18,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <type_traits>
 #include <utility>
 #include <string>
 #include <vector>
@@ -27,6 +28,7 @@
 #include "jsd_fft.cuh"
 #include "jsd_gemm.cuh"
 #include "jsd_spectral.cuh"
+#include "jsd_spectral_sq.cuh"
 
 using namespace jsd;
 
@@ -66,8 +68,35 @@ bool smooth_radix(int n) {
   return n == 1;
 }
 
+// sides S of the square FFT lengths S * S with register-resident kernels
+constexpr int kSquareSides[] = {3, 4, 5, 7, 10, 14};
+
+int square_side(int n) {
+  for (int sd : kSquareSides)
+    if (sd * sd == n) return sd;
+  return 0;
+}
+
+// Call f(std::integral_constant<int, S>) for a supported square side S.
+template <typename F>
+bool with_square_side(int sd, F&& f) {
+  switch (sd) {
+    case 3: f(std::integral_constant<int, 3>{}); return true;
+    case 4: f(std::integral_constant<int, 4>{}); return true;
+    case 5: f(std::integral_constant<int, 5>{}); return true;
+    case 7: f(std::integral_constant<int, 7>{}); return true;
+    case 10: f(std::integral_constant<int, 10>{}); return true;
+    case 14: f(std::integral_constant<int, 14>{}); return true;
+    default: return false;
+  }
+}
+
+// smallest square length with kernels, else the smallest 2,3,5,7-smooth one
 int choose_fft_size(int m) {
-  int n = 3 * (m / 2) + 1;
+  const int need = 3 * (m / 2) + 1;
+  for (int sd : kSquareSides)
+    if (sd * sd >= need) return sd * sd;
+  int n = need;
   while (!smooth_radix(n)) ++n;
   return n;
 }
@@ -129,6 +158,9 @@ struct jsd_plan {
   // device operator tables
   double2 *twx = nullptr, *twz = nullptr;
   float2 *twx32 = nullptr, *twz32 = nullptr;
+  int sqx = 0, sqz = 0;  // square sides of the FFT lengths (0: shared-memory kernels)
+  double2 *tsqx = nullptr, *tsqz = nullptr;  // w_N^e, e = 0..N-1, for the square kernels
+  float2 *tsqx32 = nullptr, *tsqz32 = nullptr;
   float *Dhi = nullptr, *Dlo = nullptr;  // TF32 split of D (mixed precision)
   bool mixed = false;
   double *Dm = nullptr, *VinvD = nullptr, *Vinv = nullptr, *Vfull = nullptr, *DVfull = nullptr;
@@ -395,10 +427,41 @@ int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2*
     const size_t sm = sizeof(C) * ((size_t)g.pz + 2 * (size_t)nl * fline(g.pz));
     const double bytes = sizeof(double2) * 6.0 * nsets * fs + sizeof(C) * (double)nl * ny * K1 * g.pz;
     ProfScope ps(p, JSD_PROF_ZINV, bytes, s);
-    k_zinv<C><<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, twz, src, inter);
-    JSD_LAUNCHED("k_zinv");
+    if (p->sqz) {
+      const C* tab = p->mixed ? (const C*)p->tsqz32 : (const C*)p->tsqz;
+      with_square_side(p->sqz, [&](auto side) {
+        constexpr int S = decltype(side)::value;
+        const int per_block = kSqWarps * SqLane<S>::G;
+        k_zinv_sq<C, S><<<(ny * K1 + per_block - 1) / per_block, kSqWarps * 32, zinv_sq_smem<C, S>(), s>>>(
+            g, tab, src, inter);
+      });
+      JSD_LAUNCHED("k_zinv_sq");
+    } else {
+      k_zinv<C><<<dim3(K1, ny), 256, sm, s>>>(g, p->fz, twz, src, inter);
+      JSD_LAUNCHED("k_zinv");
+    }
   }
-  if (dual) {
+  // the square x pass holds S points x 7 (11 for the dual) products per lane:
+  // in FP64 at S >= 10 that exceeds the register file, so the shared-memory
+  // kernel runs instead
+  if (p->sqx && (sizeof(C) == sizeof(float2) || p->sqx <= 7)) {
+    const C* tab = p->mixed ? (const C*)p->tsqx32 : (const C*)p->tsqx;
+    ProfScope ps(p, JSD_PROF_XMID, sizeof(C) * (double)(kZinvLines * nsets + 3) * ny * K1 * g.pz, s);
+    const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
+    const bool pert = p->desc.kind == JSD_KIND_PERTURBATION;
+    with_square_side(p->sqx, [&](auto side) {
+      constexpr int S = decltype(side)::value;
+      constexpr int ZC = XmidSq<C, S>::ZC;
+      const dim3 grid((g.pz + ZC - 1) / ZC, ny);
+      if (dual)
+        k_xmid_dual_sq<C, S><<<grid, kSqWarps * 32, XmidSq<C, S>::smem(g, 2 * kZinvLines), s>>>(
+            g, tab, inter, out3, p->ub, p->dub);
+      else
+        k_xmid_sq<C, S><<<grid, kSqWarps * 32, XmidSq<C, S>::smem(g, kZinvLines), s>>>(
+            g, tab, inter, out3, pert ? p->ub : nullptr, pert ? p->dub : nullptr, lam);
+    });
+    JSD_LAUNCHED("k_xmid_sq");
+  } else if (dual) {
     const size_t sm = XmidSmem<C, kXmidZB>::bytes(g);
     ProfScope ps(p, JSD_PROF_XMID, sizeof(C) * (double)(2 * kZinvLines + 3) * ny * K1 * g.pz, s);
     k_xmid_dual<C, kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
@@ -416,8 +479,19 @@ int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2*
   {
     const size_t sm = sizeof(C) * ((size_t)g.pz + 6 * (size_t)fline(g.pz));
     ProfScope ps(p, JSD_PROF_ZFWD, sizeof(C) * 3.0 * ny * K1 * g.pz + sizeof(double2) * 3.0 * fs, s);
-    k_zfwd<C><<<dim3(K1, ny), 128, sm, s>>>(g, p->fz, twz, out3, p->q, p->H1, p->hg, conv);
-    JSD_LAUNCHED("k_zfwd");
+    if (p->sqz) {
+      const C* tab = p->mixed ? (const C*)p->tsqz32 : (const C*)p->tsqz;
+      with_square_side(p->sqz, [&](auto side) {
+        constexpr int S = decltype(side)::value;
+        const int per_block = kSqWarps * SqLane<S>::G;
+        k_zfwd_sq<C, S><<<(ny * K1 + per_block - 1) / per_block, kSqWarps * 32, zfwd_sq_smem<C, S>(), s>>>(
+            g, tab, out3, p->q, p->H1, p->hg, conv);
+      });
+      JSD_LAUNCHED("k_zfwd_sq");
+    } else {
+      k_zfwd<C><<<dim3(K1, ny), 128, sm, s>>>(g, p->fz, twz, out3, p->q, p->H1, p->hg, conv);
+      JSD_LAUNCHED("k_zfwd");
+    }
   }
   return 0;
 }
@@ -531,6 +605,20 @@ int set_smem_limits() {
   JSD_CUDA(cudaFuncSetAttribute(k_dgemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<48>::BYTES));
   JSD_CUDA(cudaFuncSetAttribute(k_dgemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<64>::BYTES));
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  cudaError_t err = cudaSuccess;
+  for (int sd : kSquareSides)
+    with_square_side(sd, [&](auto side) {
+      constexpr int S = decltype(side)::value;
+      const void* fns[] = {(const void*)k_zinv_sq<double2, S>,      (const void*)k_zinv_sq<float2, S>,
+                           (const void*)k_zfwd_sq<double2, S>,      (const void*)k_zfwd_sq<float2, S>,
+                           (const void*)k_xmid_sq<double2, S>,      (const void*)k_xmid_sq<float2, S>,
+                           (const void*)k_xmid_dual_sq<double2, S>, (const void*)k_xmid_dual_sq<float2, S>};
+      for (const void* fn : fns) {
+        const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+        if (e != cudaSuccess) err = e;
+      }
+    });
+  JSD_CUDA(err);
   done = true;
   return 0;
 }
@@ -706,7 +794,7 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   g.c_fwd = std::sqrt((double)d->px_ref * (double)d->pz_ref) / (s * (double)g.px * (double)g.pz);
   p->dpdx_scale = std::sqrt(((double)d->px_ref * (two_pi / d->lx) * (two_pi / d->lx)) *
                             ((double)d->pz_ref * (two_pi / d->lz) * (two_pi / d->lz)));
-  if ((size_t)kXmidZB * g.px > (size_t)kXmidEPT * kXmidThreads) {
+  if (!square_side(g.px) && (size_t)kXmidZB * g.px > (size_t)kXmidEPT * kXmidThreads) {
     destroy(p);
     return fail(JSD_ERR_ARG, "x FFT length too large for the x-pass kernel (max " +
                                  std::to_string(kXmidEPT * kXmidThreads / kXmidZB) + ")");
@@ -754,6 +842,21 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
 
   JSD_TRY(upload(p, &p->twx, twx.data(), twx.size()));
   JSD_TRY(upload(p, &p->twz, twz.data(), twz.size()));
+  p->sqx = square_side(g.px);
+  p->sqz = square_side(g.pz);
+  for (int axis = 0; axis < 2; ++axis) {
+    const int n = axis == 0 ? g.px : g.pz;
+    if (!(axis == 0 ? p->sqx : p->sqz)) continue;
+    std::vector<double2> tab(n);
+    std::vector<float2> tab32(n);
+    for (int e = 0; e < n; ++e) {
+      const long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)e / (long double)n;
+      tab[e] = make_double2((double)cosl(ang), (double)sinl(ang));
+      tab32[e] = make_float2((float)tab[e].x, (float)tab[e].y);
+    }
+    JSD_TRY(upload(p, axis == 0 ? &p->tsqx : &p->tsqz, tab.data(), tab.size()));
+    JSD_TRY(upload(p, axis == 0 ? &p->tsqx32 : &p->tsqz32, tab32.data(), tab32.size()));
+  }
   if (p->mixed) {
     std::vector<float2> tx(twx.size()), tz(twz.size());
     for (size_t i = 0; i < twx.size(); ++i) tx[i] = make_float2((float)twx[i].x, (float)twx[i].y);

@@ -30,7 +30,7 @@ __host__ __device__ __forceinline__ int fpad(int i) { return i + (i >> 5); }
 __host__ __device__ __forceinline__ int fline(int n) { return n + (n >> 5) + 1; }
 
 // cos(2 pi m / R) and sin(2 pi m / R) for R = 3, 5, 7 (m = 0..R-1)
-__device__ __forceinline__ void root_table(int r, int m, double& c, double& s) {
+__host__ __device__ __forceinline__ void root_table(int r, int m, double& c, double& s) {
   if (r == 3) {
     const double C[3] = {1.0, -0.5, -0.5};
     const double S[3] = {0.0, 0.86602540378443864676, -0.86602540378443864676};
@@ -56,7 +56,7 @@ __device__ __forceinline__ void root_table(int r, int m, double& c, double& s) {
 //   y[R-q] = x_0 + sum_t a_t cos(2 pi q t / R) +- i sum_t b_t sin(2 pi q t / R)
 // (upper signs forward), h^2 complex-by-real products per half instead of R^2.
 template <int R, bool INV, typename C>
-__device__ __forceinline__ void dft_odd(C* x) {
+__host__ __device__ __forceinline__ void dft_odd(C* x) {
   using Rl = typename real_of<C>::type;
   constexpr int H = (R - 1) / 2;
   C a[H], b[H];
@@ -92,7 +92,7 @@ __device__ __forceinline__ void dft_odd(C* x) {
 }
 
 template <bool INV, typename C>
-__device__ __forceinline__ void dft2(C* x) {
+__host__ __device__ __forceinline__ void dft2(C* x) {
   const C a = x[0], b = x[1];
   x[0] = cadd(a, b);
   x[1] = csub(a, b);
@@ -100,12 +100,12 @@ __device__ __forceinline__ void dft2(C* x) {
 
 // multiply by -i (forward) or +i (inverse)
 template <bool INV, typename C>
-__device__ __forceinline__ C rot90(C a) {
+__host__ __device__ __forceinline__ C rot90(C a) {
   return INV ? cmake<C>(-a.y, a.x) : cmake<C>(a.y, -a.x);
 }
 
 template <bool INV, typename C>
-__device__ __forceinline__ void dft4(C* x) {
+__host__ __device__ __forceinline__ void dft4(C* x) {
   const C s02 = cadd(x[0], x[2]), d02 = csub(x[0], x[2]);
   const C s13 = cadd(x[1], x[3]), d13 = rot90<INV>(csub(x[1], x[3]));
   x[0] = cadd(s02, s13);
@@ -115,7 +115,7 @@ __device__ __forceinline__ void dft4(C* x) {
 }
 
 template <bool INV, typename C>
-__device__ __forceinline__ void dft8(C* x) {
+__host__ __device__ __forceinline__ void dft8(C* x) {
   using Rl = typename real_of<C>::type;
   const Rl h = (Rl)0.70710678118654752440;
   C e[4] = {x[0], x[2], x[4], x[6]};

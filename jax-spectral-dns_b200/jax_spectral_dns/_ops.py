@@ -114,6 +114,21 @@ def mean_flow_matrices(ny: int, re_tau: float, dt: float):
     return np.ascontiguousarray(np.array(rhs)), np.ascontiguousarray(np.array(lhs_inv))
 
 
+# sides S of the square FFT lengths S * S that have register-resident kernels
+SQUARE_FFT_SIDES = (3, 4, 5, 7, 10, 14)
+
+
+def device_fft_size(m: int) -> int:
+    """FFT length the device uses for m modes: the smallest S * S >= 3K + 1 with
+    a register-resident square-FFT kernel, else the smallest 2,3,5,7-smooth
+    length >= 3K + 1."""
+    need = 3 * (m // 2) + 1
+    for s in SQUARE_FFT_SIDES:
+        if s * s >= need:
+            return s * s
+    return smooth_fft_size(m)
+
+
 def smooth_fft_size(m: int) -> int:
     """Smallest length >= 3K + 1 (K = m // 2) whose prime factors are 2, 3, 5, 7;
     any such length dealiases quadratic products exactly."""

@@ -13,7 +13,7 @@ import numpy as np
 import torch
 
 from . import _native
-from ._ops import fourier_scale, mean_flow_matrices, operator_tables, smooth_fft_size
+from ._ops import device_fft_size, fourier_scale, mean_flow_matrices, operator_tables
 
 
 def _ptr(a: np.ndarray):
@@ -61,7 +61,7 @@ class StepPlan:
         d = _native.JsdDesc()
         d.mx, d.ny, d.mz = mx, ny, mz
         d.px_ref, d.pz_ref = int(phys_ref[0]), int(phys_ref[-1])
-        px, pz = fft_sizes if fft_sizes is not None else (smooth_fft_size(mx), smooth_fft_size(mz))
+        px, pz = fft_sizes if fft_sizes is not None else (device_fft_size(mx), device_fft_size(mz))
         d.px_fft, d.pz_fft = int(px), int(pz)
         self.fft_sizes = (int(px), int(pz))
         d.lx, d.lz = float(lx), float(lz)
