@@ -320,6 +320,8 @@ def run_ours(args):
             else:
                 per_kernel[k]["gbs"] = v["work"] / (v["ms"] / 1e3) / 1e9
         adj = None if args.no_adjoint else adjoint_leg(dev)
+        mixed_check = None if args.no_mixed_check else mixed_check_leg(dev)
+        ascent = None if args.no_ascent else ascent_leg(dev)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             rate, sec, sample, threads = cpu_reference_leg(1, 0)
@@ -346,7 +348,8 @@ def run_ours(args):
                     "d2h_bytes_per_step": state_bytes, "api": "StepPlan.step on host (pinned) state"},
             "gpu_launches": plan.launches(args.steps),
             "roofline": roofline, "kernels": per_kernel, "clocks": clocks.summary(),
-            "cpu_baseline": cpu, "finite": finite, "adjoint": adj,
+            "cpu_baseline": cpu, "finite": finite, "adjoint": adj, "perturbation_48x65x48": mixed_check,
+            "gain_ascent": ascent,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -354,10 +357,10 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def adjoint_leg(dev, checkpoint_every=50):
+def adjoint_leg(dev, checkpoints=(10, 50, 150)):
     """Gain gradients per second on the 32x65x32 adjoint configuration
     (Re = 3000, Lx = 2 pi, Lz = pi, T = 15, dt = 0.01: 1500 steps), linear and
-    nonlinear (E0 = 1e-4), with checkpoints every K steps; timed with CUDA events
+    nonlinear (E0 = 1e-4), for checkpoints every K steps; timed with CUDA events
     against a forward-only pass of the same horizon."""
     import torch
     from jax_spectral_dns.adjoint import GainProblem
@@ -367,24 +370,112 @@ def adjoint_leg(dev, checkpoint_every=50):
     shape, lx, lz, re, dt, T = (32, 65, 32), 2 * 3.141592653589793, 3.141592653589793, 3000.0, 0.01, 15.0
     modes, phys = mode_counts(shape)
     out = {"config": "32x65x32 (33x65x33 modes), Re=3000, T=15, dt=0.01 (1500 steps), seeded |k|<=8",
-           "checkpoint_every": checkpoint_every}
+           "unit": "gradients/s"}
     for lin, e0 in ((True, 1e-6), (False, 1e-4)):
-        p = GainProblem(modes, phys, lx, lz, re, dt, T, lin, checkpoint_every=checkpoint_every, device=dev)
         u0 = to_device_layout(seeded_velocity_hat(shape, (lx, lz), (8, 8), e0, seed=0), device=dev)
-        p.gain_and_dual(u0)  # warm-up
-        torch.cuda.synchronize()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-        e[0].record()
-        p.forward_checkpoints(u0)
-        e[1].record()
-        e[2].record()
-        g, _, _ = p.gain_and_dual(u0)
-        e[3].record()
-        torch.cuda.synchronize()
-        fwd_s, grad_s = e[0].elapsed_time(e[1]) / 1e3, e[2].elapsed_time(e[3]) / 1e3
-        out["linear" if lin else "nonlinear"] = {"grads_per_s": 1.0 / grad_s, "grad_s": grad_s, "forward_s": fwd_s,
-                                                  "cost_over_forward": grad_s / fwd_s, "gain": float(g.item())}
+        per_k = {}
+        for K in checkpoints:
+            p = GainProblem(modes, phys, lx, lz, re, dt, T, lin, checkpoint_every=K, device=dev)
+            p.gain_and_dual(u0)  # warm-up (captures the segment graphs)
+            torch.cuda.synchronize()
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            e[0].record()
+            p.forward_checkpoints(u0)
+            e[1].record()
+            e[2].record()
+            g, _, _ = p.gain_and_dual(u0)
+            e[3].record()
+            torch.cuda.synchronize()
+            fwd_s, grad_s = e[0].elapsed_time(e[1]) / 1e3, e[2].elapsed_time(e[3]) / 1e3
+            per_k[str(K)] = {"grads_per_s": 1.0 / grad_s, "grad_s": grad_s, "forward_s": fwd_s,
+                             "cost_over_forward": grad_s / fwd_s, "gain": float(g.item())}
+            del p
+            torch.cuda.empty_cache()
+        out["linear" if lin else "nonlinear"] = per_k
     return out
+
+
+def mixed_check_leg(dev, n_steps=2000, every=20):
+    """Nonlinear perturbation about the laminar base U = 1 - y^2: Re = 5000,
+    48x65x48 grid (49x65x49 modes), Lx = 2 pi, Lz = pi, dt = 0.005, 2000 steps,
+    seeded solenoidal field over |kx|, |kz| <= 8 with E0 = 1e-3; run in the FP64
+    and the mixed form, energy recorded every `every` steps. Reports steps/s of
+    both forms and the largest relative energy difference of the mixed history
+    from the FP64 one (the FP64 form is pinned to the oracle by the tests)."""
+    import torch
+    from jax_spectral_dns import _native
+    from jax_spectral_dns._plan import GraphedSteps, StepPlan, to_device_layout
+    from jax_spectral_dns.seeds import cheb_points, mode_counts, seeded_velocity_hat
+
+    shape, lx, lz, re, dt = (48, 65, 48), 2 * 3.141592653589793, 3.141592653589793, 5000.0, 0.005
+    modes, phys = mode_counts(shape)
+    u0 = to_device_layout(seeded_velocity_hat(shape, (lx, lz), (8, 8), 1e-3, seed=0), device=dev)
+    base = 1 - cheb_points(modes[1]) ** 2
+    out = {"config": "48x65x48 (49x65x49 modes), Re=5000, Lx=2pi, Lz=pi, dt=0.005, 2000 steps, E0=1e-3, "
+                     "laminar base", "steps": n_steps}
+    hist = {}
+    for pr in ("fp64", "mixed"):
+        plan = StepPlan(modes, phys, lx, lz, _native.JSD_KIND_PERTURBATION, re, dt, linearise=False,
+                        base_u=base, precision=pr, device=dev)
+        st, dp = u0.clone(), torch.zeros(1, dtype=torch.float64, device=dev)
+        g = GraphedSteps(plan, st, dp, 0, every)
+        energies = [plan.energy(st)]
+        for _ in range(n_steps // every):
+            g.replay()
+            energies.append(plan.energy(st))
+        hist[pr] = torch.cat(energies).cpu().numpy()
+        # timing on a fresh copy: one graph of all steps, no energy evaluations inside
+        st.copy_(u0)
+        dp.zero_()
+        gt = GraphedSteps(plan, st, dp, 0, n_steps)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        gt.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        out[pr] = {"steps_per_s": n_steps / (e0.elapsed_time(e1) / 1e3), "fft_sizes": list(plan.fft_sizes),
+                   "energy_final": float(hist[pr][-1])}
+        del gt, g, plan
+    rel = abs(hist["mixed"] / hist["fp64"] - 1)
+    out["mixed_over_fp64"] = out["mixed"]["steps_per_s"] / out["fp64"]["steps_per_s"]
+    out["energy_history_max_rel_err"] = float(rel.max())
+    out["energy_growth"] = float(hist["fp64"][-1] / hist["fp64"][0])
+    return out
+
+
+def ascent_leg(dev, iterations=20):
+    """Gain ascent on the 32x65x32 linear adjoint configuration (Re = 3000,
+    T = 15, dt = 0.01, E0 = 1e-6) through the drop-in classes: dual problem from
+    the forward perturbation equation and the conjugate-gradient solver, 20
+    iterations. Reports the gain history and seconds per iteration."""
+    import torch
+    from jax_spectral_dns.domain import PhysicalDomain
+    from jax_spectral_dns.field import FourierField, VectorField
+    from jax_spectral_dns.gradient_descent_solver import ConjugateGradientDescentSolver
+    from jax_spectral_dns.navier_stokes_perturbation import NavierStokesVelVortPerturbation
+    from jax_spectral_dns.navier_stokes_perturbation_dual import NavierStokesVelVortPerturbationDual
+    from jax_spectral_dns.seeds import seeded_velocity_hat
+
+    shape, lx, lz, re, dt, T = (32, 65, 32), 2 * 3.141592653589793, 3.141592653589793, 3000.0, 0.01, 15.0
+    dom = PhysicalDomain.create(shape, (True, False, True), scale_factors=(lx, 1.0, lz), aliasing=3 / 2)
+    u0 = torch.as_tensor(seeded_velocity_hat(shape, (lx, lz), (8, 8), 1e-6, seed=0), device=dev)
+    vel = VectorField.FromData(FourierField, dom, u0, name="velocity_hat")
+    nse = NavierStokesVelVortPerturbation(vel, Re=re, dt=dt, end_time=T, linearise=True)
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse)
+    solver = ConjugateGradientDescentSolver(dual, max_iterations=iterations, step_size=1e-2)
+    solver.initialise()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while not solver.is_done(solver.i):
+        solver.update()
+        solver.i += 1
+    torch.cuda.synchronize()
+    sec = time.perf_counter() - t0
+    return {"config": "32x65x32, Re=3000, T=15, dt=0.01, linear, E0=1e-6, ConjugateGradientDescentSolver",
+            "iterations": solver.i, "seconds_per_iteration": sec / max(1, solver.i),
+            "gains": [float(g) for g in solver.history],
+            "note": "host wall clock around whole iterations (forward run, dual run, projection, renormalisation)"}
 
 
 def run_ensemble(args):
@@ -445,6 +536,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint gradients/s leg")
+    ap.add_argument("--no-mixed-check", action="store_true",
+                    help="skip the 48x65x48 perturbation leg (FP64 vs mixed energy history)")
+    ap.add_argument("--no-ascent", action="store_true", help="skip the 20-iteration gain-ascent leg")
     ap.add_argument("--ensemble", type=int, default=0, help="run the ensemble benchmark with this many runs")
     ap.add_argument("--ensemble-horizon-scale", type=float, default=0.1)
     ap.add_argument("--ensemble-streams", type=int, default=16)
