@@ -237,7 +237,7 @@ def run_ours(args):
         time.sleep(0.3)  # let the sampler start before the GPU is loaded
         for pr in forms:
             plans[pr] = StepPlan(modes, phys, LX, LZ, 0, RE_TAU, DT, constant_mass_flux=True, flow_rate_target=q0,
-                                 device=dev, precision=pr)
+                                 device=dev, precision=pr, autotune=args.autotune)
             ms, state, dpdx = timed(plans[pr])
             results[pr] = {"ms": ms, "state": state, "dpdx": dpdx, "energy": plans[pr].energy(state).item()}
     finite = all(bool(torch.isfinite(torch.view_as_real(r["state"])).all()) for r in results.values())
@@ -327,7 +327,9 @@ def run_ours(args):
             rate, sec, sample, threads = cpu_reference_leg(1, 0)
             cpu = {"value": rate, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample}
         forms_out = {pr: {"steps_per_s": world * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
-                          "energy_after": r["energy"]} for pr, r in results.items()}
+                          "energy_after": r["energy"],
+                          "gemm_configs": {site: cfg for site, (cfg, _) in plans[pr].gemm_configs().items()}}
+                     for pr, r in results.items()}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -539,6 +541,8 @@ def main():
     ap.add_argument("--no-mixed-check", action="store_true",
                     help="skip the 48x65x48 perturbation leg (FP64 vs mixed energy history)")
     ap.add_argument("--no-ascent", action="store_true", help="skip the 20-iteration gain-ascent leg")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default GEMM tile configurations instead of autotuning them at plan creation")
     ap.add_argument("--ensemble", type=int, default=0, help="run the ensemble benchmark with this many runs")
     ap.add_argument("--ensemble-horizon-scale", type=float, default=0.1)
     ap.add_argument("--ensemble-streams", type=int, default=16)

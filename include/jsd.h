@@ -154,6 +154,25 @@ int jsd_nonlinear_terms(jsd_plan* plan, const void* state, int time_step, void* 
 /* Bytes of device workspace the plan holds. */
 size_t jsd_workspace_bytes(const jsd_plan* plan);
 
+/* Autotuner (no counterpart in the reference, where XLA picks its own
+ * kernels): times every FP64 tensor-core tile configuration of the library on
+ * the plan's three GEMM call sites (y-derivatives, eigenbasis transforms in,
+ * back-transforms out) with the plan's own sizes and workspace, and keeps the
+ * fastest per site. Overwrites workspace only (no state); synchronises the
+ * stream, so it must not be called during stream capture. */
+int jsd_autotune(jsd_plan* plan, void* stream);
+
+/* Tile configuration in use at GEMM call site `site` (0 y-derivatives,
+ * 1 eigenbasis in, 2 eigenbasis out), or -1 for a bad argument; if times_ms is
+ * not null it receives the autotuner's per-configuration times (7 floats, 0
+ * for configurations not timed). */
+int jsd_gemm_config(const jsd_plan* plan, int site, float* times_ms);
+
+/* Use tile configuration `config` (0..6) at GEMM call site `site`. Every
+ * configuration sums over K in the same order, so results do not depend on
+ * the choice. No counterpart in the reference. */
+int jsd_set_gemm_config(jsd_plan* plan, int site, int config);
+
 /* Number of kernel launches one call of jsd_step issues per time step after
  * its first; the first step of each call issues jsd_launches_first_step_extra
  * more (it derives omega_y, and dv/dy for linearised plans, from the caller's

@@ -158,6 +158,8 @@ struct jsd_plan {
   // device operator tables
   double2 *twx = nullptr, *twz = nullptr;
   float2 *twx32 = nullptr, *twz32 = nullptr;
+  int gemm_cfg[3] = {2, 2, 2};  // DMMA tile configuration per call site (GemmSite)
+  float tune_ms[3][kDgemmConfigs] = {};  // autotuner timings per site and configuration (0: not timed)
   int sqx = 0, sqz = 0;  // square sides of the FFT lengths (0: shared-memory kernels)
   double2 *tsqx = nullptr, *tsqz = nullptr;  // w_N^e, e = 0..N-1, for the square kernels
   float2 *tsqx32 = nullptr, *tsqz32 = nullptr;
@@ -255,21 +257,20 @@ double gemm_flops(const GemmBatch& b) {
   return f;
 }
 
-int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, cudaStream_t s) {
-  ProfScope ps(const_cast<jsd_plan*>(p), JSD_PROF_GEMM, gemm_flops(b), s);
-  // pick the row tile that wastes least
-  const int t48 = (max_m + 47) / 48 * 48, t64 = (max_m + 63) / 64 * 64;
-  const dim3 block(128);
-  if (t48 < t64) {
-    const dim3 grid((b.N + 63) / 64, (max_m + 47) / 48, b.count);
-    k_dgemm<48><<<grid, block, GemmSmem<48>::BYTES, s>>>(b);
-  } else {
-    const dim3 grid((b.N + 63) / 64, (max_m + 63) / 64, b.count);
-    k_dgemm<64><<<grid, block, GemmSmem<64>::BYTES, s>>>(b);
-  }
+// GEMM call sites with their own tile configuration
+enum GemmSite { kSiteDfield = 0, kSiteEigIn = 1, kSiteEigOut = 2, kGemmSites = 3 };
+
+int launch_gemm_cfg(const jsd_plan* p, const GemmBatch& b, int max_m, int cfg, cudaStream_t s) {
+  with_dgemm_cfg(cfg, [&](auto c) {
+    using Cfg = decltype(c);
+    const dim3 grid((b.N + Cfg::BN - 1) / Cfg::BN, (max_m + Cfg::BM - 1) / Cfg::BM, b.count);
+    k_dgemm_t<Cfg><<<grid, Cfg::THREADS, Cfg::BYTES, s>>>(b);
+  });
   JSD_LAUNCHED("k_dgemm");
   return 0;
 }
+
+int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, GemmSite site, cudaStream_t s);
 
 GemmBatch gemm_batch(const jsd_plan* p);
 void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M, int K, double alpha = 1.0);
@@ -281,7 +282,7 @@ int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int
   if (!p->mixed) {
     GemmBatch b = gemm_batch(p);
     for (int i = 0; i < count; ++i) add_entry(b, p->Dm, src[i], dst[i], ny, ny, 1.0);
-    return launch_gemm(p, b, ny, s);
+    return launch_gemm(p, b, ny, kSiteDfield, s);
   }
   SplitGemmBatch b;
   memset(&b, 0, sizeof(b));
@@ -323,6 +324,11 @@ void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M,
   e.M = M;
   e.K = K;
   e.alpha = alpha;
+}
+
+int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, GemmSite site, cudaStream_t s) {
+  ProfScope ps(const_cast<jsd_plan*>(p), JSD_PROF_GEMM, gemm_flops(b), s);
+  return launch_gemm_cfg(p, b, max_m, p->gemm_cfg[site], s);
 }
 
 int grid_for(size_t total, int block) {
@@ -527,7 +533,7 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     add_entry(b, p->Vinv, (const double*)p->hg + rowd, p->T + 1 * E, ni, ni);
     if (!p->ev_valid) add_entry(b, p->Vinv, (const double*)v + rowd, p->T + 2 * E, ni, ni);
     if (!p->om_valid) add_entry(b, p->Vinv, (const double*)p->om + rowd, p->T + 3 * E, ni, ni);
-    rc = launch_gemm(p, b, ni, s);
+    rc = launch_gemm(p, b, ni, kSiteEigIn, s);
     if (rc) return rc;
   }
   {
@@ -564,7 +570,7 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     add_entry(b, p->Vfull, p->vnt, (double*)v, ny, ni);
     add_entry(b, p->DVfull, p->vnt, (double*)p->dvn, ny, ni);
     add_entry(b, p->Vfull, p->omnt, (double*)p->om, ny, ni);
-    rc = launch_gemm(p, b, ny, s);
+    rc = launch_gemm(p, b, ny, kSiteEigOut, s);
     if (rc) return rc;
   }
   k_reconstruct<<<grid_for(fs, blk), blk, 0, s>>>(g, p->dvn, p->om, p->uw00, u, v, w);
@@ -602,8 +608,14 @@ int set_smem_limits() {
   JSD_CUDA(cudaFuncSetAttribute(k_zfwd<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_zfwd<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_sgemm3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sgemm3Smem::BYTES));
-  JSD_CUDA(cudaFuncSetAttribute(k_dgemm<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<48>::BYTES));
-  JSD_CUDA(cudaFuncSetAttribute(k_dgemm<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GemmSmem<64>::BYTES));
+  for (int c = 0; c < kDgemmConfigs; ++c) {
+    cudaError_t e = cudaSuccess;
+    with_dgemm_cfg(c, [&](auto cfg) {
+      using Cfg = decltype(cfg);
+      e = cudaFuncSetAttribute(k_dgemm_t<Cfg>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::BYTES);
+    });
+    JSD_CUDA(e);
+  }
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   cudaError_t err = cudaSuccess;
   for (int sd : kSquareSides)
@@ -736,6 +748,79 @@ int jsd_profile_read(jsd_plan* plan, int kernel_class, double* total_ms, long lo
 const char* jsd_last_error(void) { return g_last_error.c_str(); }
 
 size_t jsd_workspace_bytes(const jsd_plan* plan) { return plan ? plan->ws_bytes : 0; }
+
+int jsd_autotune(jsd_plan* plan, void* stream) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Geo& g = plan->g;
+  const int ny = g.ny, ni = g.ny - 2;
+  const size_t fs = (size_t)ny * g.nk;
+  const size_t E = plan->edoubles;
+  const size_t rowd = 2 * (size_t)g.nk;
+  // the timed products read these workspace fields: give them defined values
+  for (double2* f : {plan->q, plan->H1, plan->hg})
+    JSD_CUDA(cudaMemsetAsync(f, 0, fs * sizeof(double2), s));
+  for (double* f : {plan->vnt, plan->omnt}) JSD_CUDA(cudaMemsetAsync(f, 0, E * sizeof(double), s));
+  cudaEvent_t e0, e1;
+  JSD_CUDA(cudaEventCreate(&e0));
+  JSD_CUDA(cudaEventCreate(&e1));
+  int rc = 0;
+  for (int site = 0; site < kGemmSites && rc == 0; ++site) {
+    if (site == kSiteDfield && plan->mixed) continue;  // the mixed form's y-derivatives run k_sgemm3
+    GemmBatch b = gemm_batch(plan);
+    int max_m = ny;
+    if (site == kSiteDfield) {
+      // steady-state stage: D on u and w
+      add_entry(b, plan->Dm, (const double*)plan->q, (double*)plan->Dfld, ny, ny);
+      add_entry(b, plan->Dm, (const double*)plan->H1, (double*)(plan->Dfld + 2 * fs), ny, ny);
+    } else if (site == kSiteEigIn) {
+      add_entry(b, plan->VinvD, (const double*)plan->q, plan->X1, ni, ny);
+      add_entry(b, plan->Vinv, (const double*)plan->H1 + rowd, plan->T, ni, ni);
+      add_entry(b, plan->Vinv, (const double*)plan->hg + rowd, plan->T + E, ni, ni);
+      max_m = ni;
+    } else {
+      add_entry(b, plan->Vfull, plan->vnt, (double*)plan->tmp, ny, ni);
+      add_entry(b, plan->DVfull, plan->vnt, (double*)plan->dvn, ny, ni);
+      add_entry(b, plan->Vfull, plan->omnt, (double*)plan->om, ny, ni);
+    }
+    float best = 3.0e38f;
+    for (int c = 0; c < kDgemmConfigs && rc == 0; ++c) {
+      rc = launch_gemm_cfg(plan, b, max_m, c, s);  // warm-up
+      if (rc) break;
+      if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(JSD_ERR_CUDA, "cudaEventRecord");
+      for (int r = 0; r < 5 && rc == 0; ++r) rc = launch_gemm_cfg(plan, b, max_m, c, s);
+      if (rc) break;
+      float ms = 0.f;
+      if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = fail(JSD_ERR_CUDA, "autotune timing");
+        break;
+      }
+      plan->tune_ms[site][c] = ms / 5.f;
+      if (ms < best) {
+        best = ms;
+        plan->gemm_cfg[site] = c;
+      }
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
+}
+
+int jsd_set_gemm_config(jsd_plan* plan, int site, int config) {
+  if (!plan || site < 0 || site >= kGemmSites || config < 0 || config >= kDgemmConfigs)
+    return fail(JSD_ERR_ARG, "bad GEMM site or configuration");
+  plan->gemm_cfg[site] = config;
+  return 0;
+}
+
+int jsd_gemm_config(const jsd_plan* plan, int site, float* times_ms) {
+  if (!plan || site < 0 || site >= kGemmSites) return -1;
+  if (times_ms)
+    for (int c = 0; c < kDgemmConfigs; ++c) times_ms[c] = plan->tune_ms[site][c];
+  return plan->gemm_cfg[site];
+}
 
 int jsd_launches_first_step_extra(const jsd_plan* plan) {
   if (!plan) return 0;
@@ -1014,7 +1099,7 @@ int jsd_nonlinear_terms(jsd_plan* plan, const void* state, int time_step, void* 
   if (rc) return rc;
   GemmBatch b = gemm_batch(plan);
   add_entry(b, plan->Dm, (const double*)plan->q, (double*)plan->tmp, g.ny, g.ny);
-  rc = launch_gemm(plan, b, g.ny, s);
+  rc = launch_gemm(plan, b, g.ny, kSiteEigIn, s);
   if (rc) return rc;
   k_assemble_hv<<<grid_for(fs, 256), 256, 0, s>>>(g, plan->tmp, plan->H1, static_cast<double2*>(h_v));
   JSD_LAUNCHED("k_assemble_hv");

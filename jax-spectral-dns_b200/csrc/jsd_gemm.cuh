@@ -8,8 +8,9 @@
 // each application is C (M x N) = alpha * A (M x K) * B (K x N).
 //
 // One launch runs a small batch of such products (different A, B, C, M, K;
-// shared N and strides). CTA tile BM x 64, K chunk 16, two-stage cp.async
-// pipeline, 4 warps of (BM/2) x 32. A is stored with a zero-padded leading
+// shared N and strides). Tile shapes and pipeline depth are template
+// parameters (DgemmCfg); the plan picks one per call site, by the autotuner
+// when asked. A is stored with a zero-padded leading
 // dimension (multiple of 16); rows of B beyond K and columns beyond N are
 // zero-filled by the copy, so no out-of-range element is read.
 #pragma once
@@ -48,23 +49,28 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                : "d"(a), "d"(b));
 }
 
-template <int BM>
-struct GemmSmem {
-  static constexpr int BN = 64, BK = 16;
-  static constexpr int AS = BK + 4;   // A row stride (doubles): conflict-free fragment loads
-  static constexpr int BS = BN + 8;   // B row stride (doubles)
+// Tile configuration: BM x BN CTA tile, WM x WN warps (warp tile
+// (BM / WM) x (BN / WN), a multiple of 8 x 8), K chunk 16, ST-stage cp.async
+// pipeline. B rows are padded to BN + 4 doubles and A rows to 20 doubles, so
+// the DMMA fragment loads of a half-warp hit distinct banks.
+template <int BM_, int BN_, int WM_, int WN_, int ST_>
+struct DgemmCfg {
+  static constexpr int BM = BM_, BN = BN_, WM = WM_, WN = WN_, ST = ST_, BK = 16;
+  static constexpr int THREADS = 32 * WM * WN;
+  static constexpr int TM = BM / WM / 8, TN = BN / WN / 8;
+  static constexpr int AS = BK + 4;
+  static constexpr int BS = BN + 4;
   static constexpr int A_ELEMS = BM * AS;
   static constexpr int B_ELEMS = BK * BS;
   static constexpr int STAGE = A_ELEMS + B_ELEMS;
-  static constexpr size_t BYTES = 2 * STAGE * sizeof(double);
+  static constexpr size_t BYTES = (size_t)ST * STAGE * sizeof(double);
+  static_assert(TM * WM * 8 == BM && TN * WN * 8 == BN, "warp tiles must be multiples of 8 x 8");
 };
 
-template <int BM>
-__global__ void __launch_bounds__(128) k_dgemm(GemmBatch batch) {
-  using S = GemmSmem<BM>;
-  constexpr int BN = S::BN, BK = S::BK;
-  constexpr int TM = BM / 16;  // m8 tiles per warp (warp tile BM/2 rows)
-  constexpr int TN = 4;        // n8 tiles per warp (warp tile 32 cols)
+template <class Cfg>
+__global__ void __launch_bounds__(Cfg::THREADS) k_dgemm_t(GemmBatch batch) {
+  constexpr int BM = Cfg::BM, BN = Cfg::BN, BK = Cfg::BK, ST = Cfg::ST;
+  constexpr int TM = Cfg::TM, TN = Cfg::TN, NT = Cfg::THREADS;
   extern __shared__ __align__(16) double gsm[];
 
   const GemmEntry& e = batch.e[blockIdx.z];
@@ -75,29 +81,29 @@ __global__ void __launch_bounds__(128) k_dgemm(GemmBatch batch) {
   const int lda = batch.lda, ldb = batch.ldb, ldc = batch.ldc;
   const int tid = threadIdx.x;
   const int warp = tid >> 5, lane = tid & 31;
-  const int wm = (warp >> 1) * (BM / 2);
-  const int wn = (warp & 1) * 32;
+  const int wm = (warp / Cfg::WN) * (BM / Cfg::WM);
+  const int wn = (warp % Cfg::WN) * (BN / Cfg::WN);
+  // m8 tiles of this warp that hold at least one row of C (warp-uniform)
+  int live_tm = (e.M - (m0 + wm) + 7) / 8;
+  live_tm = live_tm < 0 ? 0 : (live_tm > TM ? TM : live_tm);
 
   auto load_chunk = [&](int stage, int k0) {
-    double* As = gsm + stage * S::STAGE;
-    double* Bs = As + S::A_ELEMS;
-    // A: BM rows x 16 doubles = BM * 8 copies of 16 bytes
-    for (int c = tid; c < BM * (BK / 2); c += 128) {
+    double* As = gsm + stage * Cfg::STAGE;
+    double* Bs = As + Cfg::A_ELEMS;
+    for (int c = tid; c < BM * (BK / 2); c += NT) {
       const int r = c / (BK / 2), cc = (c % (BK / 2)) * 2;
       const int gr = m0 + r;
       const bool ok = gr < e.M;
       const double* src = e.A + (size_t)(ok ? gr : 0) * lda + k0 + cc;
-      cp_async16(As + r * S::AS + cc, src, ok ? 16 : 0);
+      cp_async16(As + r * Cfg::AS + cc, src, ok ? 16 : 0);
     }
-    // B: 16 rows x 64 doubles = 512 copies
-    for (int c = tid; c < BK * (BN / 2); c += 128) {
+    for (int c = tid; c < BK * (BN / 2); c += NT) {
       const int r = c / (BN / 2), cc = (c % (BN / 2)) * 2;
       const int gk = k0 + r, gn = n0 + cc;
       const bool ok = (gk < e.K) && (gn < N);
       const double* src = e.B + (ok ? ((size_t)gk * ldb + gn) : 0);
-      cp_async16(Bs + r * S::BS + cc, src, ok ? 16 : 0);
+      cp_async16(Bs + r * Cfg::BS + cc, src, ok ? 16 : 0);
     }
-    cp_async_commit();
   };
 
   double acc[TM][TN][2];
@@ -107,31 +113,37 @@ __global__ void __launch_bounds__(128) k_dgemm(GemmBatch batch) {
     for (int j = 0; j < TN; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   const int nchunks = (e.K + BK - 1) / BK;
-  load_chunk(0, 0);
+  // prologue: chunks 0 .. ST-2 in flight (one commit group each, empty groups past the end)
+#pragma unroll
+  for (int c = 0; c < ST - 1; ++c) {
+    if (c < nchunks) load_chunk(c, c * BK);
+    cp_async_commit();
+  }
   for (int c = 0; c < nchunks; ++c) {
-    if (c + 1 < nchunks) {
-      load_chunk((c + 1) & 1, (c + 1) * BK);
-      cp_async_wait<1>();
-    } else {
-      cp_async_wait<0>();
-    }
+    cp_async_wait<ST - 2>();
     __syncthreads();
-    const double* As = gsm + (c & 1) * S::STAGE;
-    const double* Bs = As + S::A_ELEMS;
+    // the stage refilled now was last read in iteration c - 1, which every warp has finished
+    const int nc = c + ST - 1;
+    if (nc < nchunks) load_chunk(nc % ST, nc * BK);
+    cp_async_commit();
+    const double* As = gsm + (c % ST) * Cfg::STAGE;
+    const double* Bs = As + Cfg::A_ELEMS;
 #pragma unroll
     for (int kk = 0; kk < BK; kk += 4) {
       double af[TM], bf[TN];
 #pragma unroll
-      for (int i = 0; i < TM; ++i) af[i] = As[(wm + i * 8 + (lane >> 2)) * S::AS + kk + (lane & 3)];
+      for (int i = 0; i < TM; ++i) af[i] = As[(wm + i * 8 + (lane >> 2)) * Cfg::AS + kk + (lane & 3)];
 #pragma unroll
-      for (int j = 0; j < TN; ++j) bf[j] = Bs[(kk + (lane & 3)) * S::BS + wn + j * 8 + (lane >> 2)];
+      for (int j = 0; j < TN; ++j) bf[j] = Bs[(kk + (lane & 3)) * Cfg::BS + wn + j * 8 + (lane >> 2)];
 #pragma unroll
       for (int i = 0; i < TM; ++i)
+        if (i < live_tm) {
 #pragma unroll
-        for (int j = 0; j < TN; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+          for (int j = 0; j < TN; ++j) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
     }
-    __syncthreads();
   }
+  cp_async_wait<0>();
 
   const double alpha = e.alpha;
 #pragma unroll
@@ -146,6 +158,32 @@ __global__ void __launch_bounds__(128) k_dgemm(GemmBatch batch) {
             make_double2(alpha * acc[i][j][0], alpha * acc[i][j][1]);
       }
     }
+  }
+}
+
+// Candidate configurations (index = configuration id used by the plan and
+// the autotuner).
+using DgemmC0 = DgemmCfg<48, 64, 2, 2, 2>;
+using DgemmC1 = DgemmCfg<64, 64, 2, 2, 2>;
+using DgemmC2 = DgemmCfg<64, 64, 2, 2, 3>;
+using DgemmC3 = DgemmCfg<64, 128, 2, 2, 3>;
+using DgemmC4 = DgemmCfg<128, 64, 4, 2, 3>;
+using DgemmC5 = DgemmCfg<64, 128, 2, 4, 3>;
+using DgemmC6 = DgemmCfg<128, 128, 4, 4, 2>;
+constexpr int kDgemmConfigs = 7;
+
+// f(Cfg{}) for configuration id `id`
+template <typename F>
+__host__ bool with_dgemm_cfg(int id, F&& f) {
+  switch (id) {
+    case 0: f(DgemmC0{}); return true;
+    case 1: f(DgemmC1{}); return true;
+    case 2: f(DgemmC2{}); return true;
+    case 3: f(DgemmC3{}); return true;
+    case 4: f(DgemmC4{}); return true;
+    case 5: f(DgemmC5{}); return true;
+    case 6: f(DgemmC6{}); return true;
+    default: return false;
   }
 }
 

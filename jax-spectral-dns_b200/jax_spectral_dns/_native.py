@@ -47,8 +47,13 @@ EXPORTED = (
     "jsd_correct_mass_flux", "jsd_energy", "jsd_flow_rate", "jsd_nonlinear_terms",
     "jsd_workspace_bytes", "jsd_launches_per_step", "jsd_last_error", "jsd_abi_version",
     "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc", "jsd_step_trajectory",
-    "jsd_launches_first_step_extra",
+    "jsd_launches_first_step_extra", "jsd_autotune", "jsd_gemm_config",
+    "jsd_set_gemm_config",
 )
+
+# GEMM call sites of a plan (jsd_gemm_config) and the number of DMMA tile configurations
+GEMM_SITES = {"dfield": 0, "eig_in": 1, "eig_out": 2}
+DGEMM_CONFIGS = 7
 
 PROF_CLASSES = {"gemm": 0, "zinv": 1, "xmid": 2, "zfwd": 3, "eigen": 4, "linear": 5, "sgemm": 6}
 
@@ -87,6 +92,9 @@ def load(path: str = LIB_PATH):
     lib.jsd_energy_noalloc.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                        ctypes.c_double, ctypes.c_double, vp, vp, vp]
     lib.jsd_profile_enable.argtypes = [vp, ctypes.c_int]
+    lib.jsd_autotune.argtypes = [vp, vp]
+    lib.jsd_gemm_config.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    lib.jsd_set_gemm_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.jsd_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED:

@@ -42,7 +42,7 @@ class StepPlan:
 
     def __init__(self, modes, phys_ref, lx, lz, kind, re_tau, dt, dt_explicit=None, linearise=False,
                  constant_mass_flux=False, flow_rate_target=0.0, base_u: Optional[np.ndarray] = None,
-                 fft_sizes=None, device="cuda", precision: str = "fp64"):
+                 fft_sizes=None, device="cuda", precision: str = "fp64", autotune: bool = False):
         if not torch.cuda.is_available():
             raise _native.NativeError("the velocity-vorticity step needs a CUDA device")
         self.lib = _native.load()
@@ -89,6 +89,8 @@ class StepPlan:
         with torch.cuda.device(self.device):
             _native.check(self.lib.jsd_plan_create(ctypes.byref(d), ctypes.byref(h)), "jsd_plan_create")
         self.handle = h
+        if autotune:
+            self.autotune()
         self.scale = fourier_scale(lx, lz)
         self._scalar = torch.zeros(4, dtype=torch.float64, device=self.device)
         self._history = None
@@ -105,6 +107,27 @@ class StepPlan:
     # --- calls ------------------------------------------------------------
     def workspace_bytes(self) -> int:
         return int(self.lib.jsd_workspace_bytes(self.handle))
+
+    def autotune(self) -> dict:
+        """Time every FP64 tensor-core tile configuration at each GEMM call site
+        on this plan's sizes and keep the fastest (jsd_autotune)."""
+        with torch.cuda.device(self.device):
+            _native.check(self.lib.jsd_autotune(self.handle, _stream_ptr()), "jsd_autotune")
+            torch.cuda.synchronize(self.device)
+        return self.gemm_configs()
+
+    def set_gemm_config(self, site: str, config: int) -> None:
+        _native.check(self.lib.jsd_set_gemm_config(self.handle, _native.GEMM_SITES[site], int(config)),
+                      "jsd_set_gemm_config")
+
+    def gemm_configs(self) -> dict:
+        """{site: (configuration id, [per-configuration autotune ms])}."""
+        out = {}
+        for name, site in _native.GEMM_SITES.items():
+            times = (ctypes.c_float * _native.DGEMM_CONFIGS)()
+            cfg = int(self.lib.jsd_gemm_config(self.handle, site, times))
+            out[name] = (cfg, [float(t) for t in times])
+        return out
 
     def launches_per_step(self) -> int:
         """Kernel launches per step after the first of a `step` call."""
