@@ -328,7 +328,9 @@ def run_ours(args):
             cpu = {"value": rate, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample}
         forms_out = {pr: {"steps_per_s": world * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
                           "energy_after": r["energy"],
-                          "gemm_configs": {site: cfg for site, (cfg, _) in plans[pr].gemm_configs().items()}}
+                          "gemm_configs": {site: cfg for site, (cfg, _) in plans[pr].gemm_configs().items()},
+                          "xmid_variant": plans[pr].xmid_variant()[0],
+                          "xmid_variant_ms": plans[pr].xmid_variant()[1]}
                      for pr, r in results.items()}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,

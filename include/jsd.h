@@ -158,7 +158,8 @@ size_t jsd_workspace_bytes(const jsd_plan* plan);
  * kernels): times every FP64 tensor-core tile configuration of the library on
  * the plan's three GEMM call sites (y-derivatives, eigenbasis transforms in,
  * back-transforms out) with the plan's own sizes and workspace, and keeps the
- * fastest per site. Overwrites workspace only (no state); synchronises the
+ * fastest per site, and likewise chooses among the x-pass kernel variants of
+ * the nonlinear terms. Overwrites workspace only (no state); synchronises the
  * stream, so it must not be called during stream capture. */
 int jsd_autotune(jsd_plan* plan, void* stream);
 
@@ -172,6 +173,16 @@ int jsd_gemm_config(const jsd_plan* plan, int site, float* times_ms);
  * configuration sums over K in the same order, so results do not depend on
  * the choice. No counterpart in the reference. */
 int jsd_set_gemm_config(jsd_plan* plan, int site, int config);
+
+/* x-pass kernel of the nonlinear terms in use: 0 register FFT with S lanes per
+ * x line, 1 register FFT with 2 S lanes per line, 2 shared-memory FFT; if
+ * times_ms is not null it receives the autotuner's times of the three (0 for
+ * variants not timed or not available). No counterpart in the reference. */
+int jsd_xmid_variant(const jsd_plan* plan, float* times_ms);
+
+/* Force x-pass variant 0, 1 or 2 (JSD_ERR_ARG when it does not apply to the
+ * plan's FFT length, precision or equation). No counterpart in the reference. */
+int jsd_set_xmid_variant(jsd_plan* plan, int variant);
 
 /* Number of kernel launches one call of jsd_step issues per time step after
  * its first; the first step of each call issues jsd_launches_first_step_extra

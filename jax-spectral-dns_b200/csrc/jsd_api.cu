@@ -159,6 +159,8 @@ struct jsd_plan {
   double2 *twx = nullptr, *twz = nullptr;
   float2 *twx32 = nullptr, *twz32 = nullptr;
   int gemm_cfg[3] = {2, 2, 2};  // DMMA tile configuration per call site (GemmSite)
+  int xmid_variant = 2;         // x-pass kernel (launch_xmid), set at creation, autotuned on request
+  float xmid_ms[3] = {};        // autotuner timings of the x-pass variants (0: not timed)
   float tune_ms[3][kDgemmConfigs] = {};  // autotuner timings per site and configuration (0: not timed)
   int sqx = 0, sqz = 0;  // square sides of the FFT lengths (0: shared-memory kernels)
   double2 *tsqx = nullptr, *tsqz = nullptr;  // w_N^e, e = 0..N-1, for the square kernels
@@ -406,6 +408,70 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
   return p->mixed ? transforms<float2>(p, state, uhist, conv, s) : transforms<double2>(p, state, uhist, conv, s);
 }
 
+// x-pass variants: 0 register square FFT (S lanes per line), 1 half-split
+// register FFT (2 S lanes per line, even S, not the dual), 2 shared-memory FFT.
+// The S-lane form holds S points x 7 (11 for the dual) products per lane, more
+// than the register file in FP64 beyond S = 7.
+bool xmid_available(const jsd_plan* p, int v) {
+  const bool dual = p->desc.kind == JSD_KIND_DUAL;
+  const int S = p->sqx;
+  if (v == 0) return S && (p->mixed || S <= 7);
+  if (v == 1) return S && S % 2 == 0 && !dual;
+  if (v == 2) return smooth_radix(p->g.px) && (size_t)kXmidZB * p->g.px <= (size_t)kXmidEPT * kXmidThreads;
+  return false;
+}
+
+int default_xmid_variant(const jsd_plan* p) {
+  if (p->mixed && xmid_available(p, 0)) return 0;
+  if (xmid_available(p, 1)) return 1;
+  if (xmid_available(p, 0)) return 0;
+  return 2;
+}
+
+template <typename C>
+int launch_xmid(jsd_plan* p, int variant, C* inter, C* out3, cudaStream_t s) {
+  const Geo& g = p->g;
+  const int ny = g.ny;
+  const bool dual = p->desc.kind == JSD_KIND_DUAL;
+  const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
+  const bool pert = p->desc.kind == JSD_KIND_PERTURBATION;
+  const double* ub = pert ? p->ub : nullptr;
+  const double* dub = pert ? p->dub : nullptr;
+  if (!xmid_available(p, variant)) return fail(JSD_ERR_ARG, "x-pass variant not available for this plan");
+  if (variant == 2) {
+    const C* twx = p->mixed ? (const C*)p->twx32 : (const C*)p->twx;
+    const size_t sm = XmidSmem<C, kXmidZB>::bytes(g);
+    const dim3 grid((g.pz + kXmidZB - 1) / kXmidZB, ny);
+    if (dual)
+      k_xmid_dual<C, kXmidZB><<<grid, kXmidThreads, sm, s>>>(g, p->fx, twx, inter, out3, p->ub, p->dub);
+    else
+      k_xmid<C, kXmidZB><<<grid, kXmidThreads, sm, s>>>(g, p->fx, twx, inter, out3, ub, dub, lam);
+    JSD_LAUNCHED("k_xmid");
+    return 0;
+  }
+  const C* tab = p->mixed ? (const C*)p->tsqx32 : (const C*)p->tsqx;
+  with_square_side(p->sqx, [&](auto side) {
+    constexpr int S = decltype(side)::value;
+    if (variant == 0) {
+      constexpr int ZC = XmidSq<C, S>::ZC;
+      const dim3 grid((g.pz + ZC - 1) / ZC, ny);
+      if (dual)
+        k_xmid_dual_sq<C, S><<<grid, kSqWarps * 32, XmidSq<C, S>::smem(g, 2 * kZinvLines), s>>>(
+            g, tab, inter, out3, p->ub, p->dub);
+      else
+        k_xmid_sq<C, S><<<grid, kSqWarps * 32, XmidSq<C, S>::smem(g, kZinvLines), s>>>(g, tab, inter, out3, ub,
+                                                                                      dub, lam);
+    } else if constexpr (S % 2 == 0) {
+      constexpr int ZC = XmidH2<C, S>::ZC;
+      const dim3 grid((g.pz + ZC - 1) / ZC, ny);
+      k_xmid_h2<C, S><<<grid, kSqWarps * 32, XmidH2<C, S>::smem(g, kZinvLines), s>>>(g, tab, inter, out3, ub, dub,
+                                                                                    lam);
+    }
+  });
+  JSD_LAUNCHED("k_xmid_sq");
+  return 0;
+}
+
 template <typename C>
 int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2* conv, cudaStream_t s) {
   const Geo& g = p->g;
@@ -447,40 +513,10 @@ int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2*
       JSD_LAUNCHED("k_zinv");
     }
   }
-  // the square x pass holds S points x 7 (11 for the dual) products per lane:
-  // in FP64 at S >= 10 that exceeds the register file, so the shared-memory
-  // kernel runs instead
-  if (p->sqx && (sizeof(C) == sizeof(float2) || p->sqx <= 7)) {
-    const C* tab = p->mixed ? (const C*)p->tsqx32 : (const C*)p->tsqx;
+  {
     ProfScope ps(p, JSD_PROF_XMID, sizeof(C) * (double)(kZinvLines * nsets + 3) * ny * K1 * g.pz, s);
-    const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
-    const bool pert = p->desc.kind == JSD_KIND_PERTURBATION;
-    with_square_side(p->sqx, [&](auto side) {
-      constexpr int S = decltype(side)::value;
-      constexpr int ZC = XmidSq<C, S>::ZC;
-      const dim3 grid((g.pz + ZC - 1) / ZC, ny);
-      if (dual)
-        k_xmid_dual_sq<C, S><<<grid, kSqWarps * 32, XmidSq<C, S>::smem(g, 2 * kZinvLines), s>>>(
-            g, tab, inter, out3, p->ub, p->dub);
-      else
-        k_xmid_sq<C, S><<<grid, kSqWarps * 32, XmidSq<C, S>::smem(g, kZinvLines), s>>>(
-            g, tab, inter, out3, pert ? p->ub : nullptr, pert ? p->dub : nullptr, lam);
-    });
-    JSD_LAUNCHED("k_xmid_sq");
-  } else if (dual) {
-    const size_t sm = XmidSmem<C, kXmidZB>::bytes(g);
-    ProfScope ps(p, JSD_PROF_XMID, sizeof(C) * (double)(2 * kZinvLines + 3) * ny * K1 * g.pz, s);
-    k_xmid_dual<C, kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
-        g, p->fx, twx, inter, out3, p->ub, p->dub);
-    JSD_LAUNCHED("k_xmid_dual");
-  } else {
-    const size_t sm = XmidSmem<C, kXmidZB>::bytes(g);
-    ProfScope ps(p, JSD_PROF_XMID, sizeof(C) * (double)(kZinvLines + 3) * ny * K1 * g.pz, s);
-    const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
-    const bool pert = p->desc.kind == JSD_KIND_PERTURBATION;
-    k_xmid<C, kXmidZB><<<dim3((g.pz + kXmidZB - 1) / kXmidZB, ny), kXmidThreads, sm, s>>>(
-        g, p->fx, twx, inter, out3, pert ? p->ub : nullptr, pert ? p->dub : nullptr, lam);
-    JSD_LAUNCHED("k_xmid");
+    int rc = launch_xmid<C>(p, p->xmid_variant, inter, out3, s);
+    if (rc) return rc;
   }
   {
     const size_t sm = sizeof(C) * ((size_t)g.pz + 6 * (size_t)fline(g.pz));
@@ -625,6 +661,12 @@ int set_smem_limits() {
                            (const void*)k_zfwd_sq<double2, S>,      (const void*)k_zfwd_sq<float2, S>,
                            (const void*)k_xmid_sq<double2, S>,      (const void*)k_xmid_sq<float2, S>,
                            (const void*)k_xmid_dual_sq<double2, S>, (const void*)k_xmid_dual_sq<float2, S>};
+      if constexpr (S % 2 == 0) {
+        for (const void* fn : {(const void*)k_xmid_h2<double2, S>, (const void*)k_xmid_h2<float2, S>}) {
+          const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
+          if (e != cudaSuccess) err = e;
+        }
+      }
       for (const void* fn : fns) {
         const cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, big);
         if (e != cudaSuccess) err = e;
@@ -803,9 +845,52 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
       }
     }
   }
+  // x-pass kernel variants (nonlinear plans)
+  const bool linear = plan->desc.linearise && plan->desc.kind != JSD_KIND_NS;
+  if (rc == 0 && !linear) {
+    float best = 3.0e38f;
+    for (int v = 0; v < 3 && rc == 0; ++v) {
+      if (!xmid_available(plan, v)) continue;
+      auto run = [&]() {
+        return plan->mixed ? launch_xmid<float2>(plan, v, (float2*)plan->inter, (float2*)plan->out3, s)
+                           : launch_xmid<double2>(plan, v, (double2*)plan->inter, (double2*)plan->out3, s);
+      };
+      rc = run();  // warm-up
+      if (rc) break;
+      if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(JSD_ERR_CUDA, "cudaEventRecord");
+      for (int r = 0; r < 3 && rc == 0; ++r) rc = run();
+      if (rc) break;
+      float ms = 0.f;
+      if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = fail(JSD_ERR_CUDA, "autotune timing");
+        break;
+      }
+      plan->xmid_ms[v] = ms / 3.f;
+      if (ms < best) {
+        best = ms;
+        plan->xmid_variant = v;
+      }
+    }
+  }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
+}
+
+int jsd_xmid_variant(const jsd_plan* plan, float* times_ms) {
+  if (!plan) return -1;
+  if (times_ms)
+    for (int v = 0; v < 3; ++v) times_ms[v] = plan->xmid_ms[v];
+  return plan->xmid_variant;
+}
+
+int jsd_set_xmid_variant(jsd_plan* plan, int variant) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  if (variant < 0 || variant > 2 || !xmid_available(plan, variant))
+    return fail(JSD_ERR_ARG, "x-pass variant not available for this plan");
+  plan->xmid_variant = variant;
+  return 0;
 }
 
 int jsd_set_gemm_config(jsd_plan* plan, int site, int config) {
@@ -929,6 +1014,7 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(upload(p, &p->twz, twz.data(), twz.size()));
   p->sqx = square_side(g.px);
   p->sqz = square_side(g.pz);
+  p->xmid_variant = default_xmid_variant(p);
   for (int axis = 0; axis < 2; ++axis) {
     const int n = axis == 0 ? g.px : g.pz;
     if (!(axis == 0 ? p->sqx : p->sqz)) continue;

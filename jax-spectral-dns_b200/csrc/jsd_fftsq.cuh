@@ -150,6 +150,72 @@ __device__ __forceinline__ void sq_fft_tab(C* x, const C* tab, C* xb, int t, boo
   __syncwarp();
 }
 
+// Half-split form for even S = 2H: a line on 2S lanes, lane (t, h) holding
+// the H elements at positions t + S (2 j + h), j = 0..H-1.
+//   stage 1, decimation in time over m = 2 j + h: lane h transforms its own
+//     H values (E for h = 0, O for h = 1), swaps them with its partner lane
+//     (same t, other h), and forms Y[h H + k] = E[k] +- w_S^k O[k], times
+//     w_N^(t (h H + k)), into the exchange buffer;
+//   stage 2, decimation in frequency: lane (t, h) reads row t and forms
+//     c[n] = b[n] + b[n+H] (h = 0) or (b[n] - b[n+H]) w_S^n (h = 1), whose
+//     H-point DFT is X[t + S (2 j + h)].
+// Input and output positions of a lane coincide, as in sq_fft. tab = w_N^e.
+// Stage-1 butterfly of the half-split form for one k: own = this lane's
+// H-point DFT value at k, other = the partner lane's.
+template <int S, bool INV, typename C>
+__host__ __device__ __forceinline__ C sq2_butterfly(C own, C other, int k, const C* tab, int t, int h) {
+  constexpr int H = S / 2;
+  const C E = h ? other : own;
+  C O = h ? own : other;
+  C w = tab[S * k];
+  if (INV) w.y = -w.y;
+  O = cmul(O, w);
+  const C y = h ? csub(E, O) : cadd(E, O);
+  C tw = tab[t * (h * H + k)];
+  if (INV) tw.y = -tw.y;
+  return cmul(y, tw);
+}
+
+// Stage 2 of the half-split form: read row t of the exchange buffer, combine
+// for output parity h, H-point DFT; x[j] = X[t + S (2 j + h)] on exit.
+template <int S, bool INV, typename C>
+__host__ __device__ __forceinline__ void sq2_stage2(C* x, const C* xb, const C* tab, int t, int h) {
+  constexpr int H = S / 2;
+#pragma unroll
+  for (int n = 0; n < H; ++n) {
+    const C b0 = xb[t * (S + 1) + n], b1 = xb[t * (S + 1) + n + H];
+    if (h) {
+      C w = tab[S * n];
+      if (INV) w.y = -w.y;
+      x[n] = cmul(csub(b0, b1), w);
+    } else {
+      x[n] = cadd(b0, b1);
+    }
+  }
+  dft_reg<H, INV>(x);
+}
+
+template <int S, bool INV, typename C>
+__device__ __forceinline__ void sq2_fft(C* x, const C* tab, C* xb, int t, int h, int partner, bool live) {
+  constexpr int H = S / 2;
+  static_assert(2 * H == S, "half-split transform needs an even side");
+  dft_reg<H, INV>(x);
+#pragma unroll
+  for (int k = 0; k < H; ++k) {
+    C o;
+    o.x = __shfl_sync(0xffffffffu, x[k].x, partner);
+    o.y = __shfl_sync(0xffffffffu, x[k].y, partner);
+    x[k] = sq2_butterfly<S, INV>(x[k], o, k, tab, t, h);
+  }
+  if (live) {
+#pragma unroll
+    for (int k = 0; k < H; ++k) xb[(h * H + k) * (S + 1) + t] = x[k];
+  }
+  __syncwarp();
+  if (live) sq2_stage2<S, INV>(x, xb, tab, t, h);
+  __syncwarp();
+}
+
 // Lane t's twiddles w_N^(t j), j = 1..S-1, from the table w_N^e, e = 0..N-1.
 template <int S, typename C>
 __host__ __device__ __forceinline__ void sq_twiddles(C* tw, const C* __restrict__ table, int t) {

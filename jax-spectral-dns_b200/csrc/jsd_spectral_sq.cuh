@@ -198,12 +198,11 @@ __device__ __forceinline__ void cp_async_elem(C* smem, const C* gmem, bool ok) {
 
 // Block-wide: start asynchronous copies of the input tile [f][zl][kx]
 // (kx >= 0) of nfields fields; the caller waits (cp_async_wait<0>) and syncs.
-template <typename C, int S>
+template <typename C, int ZC>
 __device__ __forceinline__ void xsq_stage_tile(const Geo& g, const C* __restrict__ inter, C* tile, int nfields,
                                                int y, int z0) {
-  constexpr int ZC = XmidSq<C, S>::ZC;
   constexpr int RSTEP = kSqWarps * 32 / ZC;  // tile rows per pass of the block
-  const int K1 = g.kx_max + 1, KP = XmidSq<C, S>::kp(K1);
+  const int K1 = g.kx_max + 1, KP = K1 | 1;
   if (threadIdx.x < RSTEP * ZC) {
     const int zl = threadIdx.x % ZC;
     const int z = z0 + zl;
@@ -285,9 +284,8 @@ __device__ __forceinline__ void xsq_forward(const Geo& g, const C* tab, C* xb, C
 }
 
 // Block-wide: coalesced store of the output tile.
-template <typename C, int S>
+template <typename C, int ZC>
 __device__ __forceinline__ void xsq_store(const Geo& g, const C* otile, C* __restrict__ out3, int y, int z0) {
-  constexpr int ZC = XmidSq<C, S>::ZC;
   constexpr int RSTEP = kSqWarps * 32 / ZC;
   const int K1 = g.kx_max + 1;
   if (threadIdx.x >= RSTEP * ZC) return;
@@ -335,7 +333,7 @@ __global__ void __launch_bounds__(kSqWarps * 32, xsq_min_blocks<C>()) k_xmid_sq(
   const Rl ub = ubase ? (Rl)ubase[y] : (Rl)0;
   const Rl dub = dubase ? (Rl)dubase[y] : (Rl)0;
   const Rl c = (Rl)g.c_inv, lam = (Rl)lam_d, half = (Rl)0.5;
-  xsq_stage_tile<C, S>(g, inter, tile, kZinvLines, y, z0);
+  xsq_stage_tile<C, ZC>(g, inter, tile, kZinvLines, y, z0);
   // twiddle table w_N^e in shared memory (read by stage 1 of every transform)
   C* stab = otile + 3 * K1 * ZC + kSqWarps * G * XB;
   for (int e = threadIdx.x; e < S * S; e += blockDim.x) stab[e] = twtab[e];
@@ -404,7 +402,7 @@ __global__ void __launch_bounds__(kSqWarps * 32, xsq_min_blocks<C>()) k_xmid_sq(
   }
   xsq_forward<C, S>(g, stab, xb, otile, zl, t, live && z0 + zl < g.pz, x, z2);
   __syncthreads();
-  xsq_store<C, S>(g, otile, out3, y, z0);
+  xsq_store<C, ZC>(g, otile, out3, y, z0);
 }
 
 // Adjoint products, as in k_xmid_dual (lam = 1; dual v, frozen forward u,
@@ -429,7 +427,7 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_xmid_dual_sq(Geo g, const C* 
   const Rl ub = (Rl)ubase[y];
   const Rl dub = (Rl)dubase[y];
   const Rl c = (Rl)g.c_inv, q4 = (Rl)0.25;
-  xsq_stage_tile<C, S>(g, inter, tile, 2 * kZinvLines, y, z0);
+  xsq_stage_tile<C, ZC>(g, inter, tile, 2 * kZinvLines, y, z0);
   // twiddle table w_N^e in shared memory (read by stage 1 of every transform)
   C* stab = otile + 3 * K1 * ZC + kSqWarps * G * XB;
   for (int e = threadIdx.x; e < S * S; e += blockDim.x) stab[e] = twtab[e];
@@ -480,7 +478,181 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_xmid_dual_sq(Geo g, const C* 
 #undef JSD_EACH
   xsq_forward<C, S>(g, stab, xb, otile, zl, t, live && z0 + zl < g.pz, x, z2);
   __syncthreads();
-  xsq_store<C, S>(g, otile, out3, y, z0);
+  xsq_store<C, ZC>(g, otile, out3, y, z0);
+}
+
+// ---------------------------------------------------------------------------
+// x pass, half-split lanes (even S): a z column's lines on 2 S lanes, H = S / 2
+// points per lane (sq2_fft). Half the registers per lane of k_xmid_sq, so the
+// FP64 products fit without spilling.
+// ---------------------------------------------------------------------------
+template <int S>
+struct SqLane2 {
+  static constexpr int H = S / 2, L = 2 * S, G = 32 / L;  // lines per warp
+  int warp, gi, t, h, partner;
+  bool live;
+  __device__ __forceinline__ SqLane2() {
+    const int lane = threadIdx.x & 31;
+    warp = threadIdx.x >> 5;
+    gi = lane / L;
+    const int r = lane - gi * L;
+    h = r / S;
+    t = r - h * S;
+    live = gi < G;
+    if (!live) {
+      gi = 0;
+      h = 0;
+      t = 0;
+    }
+    partner = live ? (h ? lane - S : lane + S) : lane;
+  }
+};
+
+template <typename C, int S>
+struct XmidH2 {
+  static constexpr int G = SqLane2<S>::G;
+  static constexpr int ZC = kSqWarps * G;
+  static size_t smem(const Geo& g, int nfields) {
+    const int K1 = g.kx_max + 1;
+    return sizeof(C) * ((size_t)nfields * ZC * (K1 | 1) + 3 * (size_t)K1 * ZC + (size_t)kSqWarps * G * sq_xbuf<S>() +
+                        (size_t)S * S);
+  }
+};
+
+// packed line of fields (fa, fb) at this lane's positions t + S (2 j + h)
+template <typename C, int S, int ZC>
+__device__ __forceinline__ void xh2_fill(const Geo& g, const C* tile, int zl, int t, int h, bool live, C* x, int fa,
+                                         bool dxa, int fb, bool dxb) {
+  using Rl = typename real_of<C>::type;
+  constexpr int N = S * S, H = S / 2;
+  const int K = g.kx_max, KP = (K + 1) | 1;
+  const C* ta = tile + (fa * ZC + zl) * KP;
+  const C* tb = tile + (fb * ZC + zl) * KP;
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const int p = t + S * (2 * j + h);
+    const bool lo = p <= K, hi = p >= N - K;
+    C out = cmake<C>(0, 0);
+    if (live && (lo || hi)) {
+      const int kx = lo ? p : N - p;
+      C A = ta[kx], B = tb[kx];
+      const Rl k = (Rl)(kx * g.ax);
+      if (dxa) A = cmul_ik(A, k);
+      if (dxb) B = cmul_ik(B, k);
+      if (p == 0) out = cmake<C>(A.x, B.x);
+      else if (lo) out = cmake<C>(A.x - B.y, A.y + B.x);
+      else out = cmake<C>(A.x + B.y, B.x - A.y);
+    }
+    x[j] = out;
+  }
+}
+
+template <typename C, int S>
+__global__ void __launch_bounds__(kSqWarps * 32) k_xmid_h2(Geo g, const C* __restrict__ twtab,
+                                                           const C* __restrict__ inter, C* __restrict__ out3,
+                                                           const double* __restrict__ ubase,
+                                                           const double* __restrict__ dubase, double lam_d) {
+  using Rl = typename real_of<C>::type;
+  constexpr int N = S * S, H = S / 2, G = SqLane2<S>::G, ZC = XmidH2<C, S>::ZC, XB = sq_xbuf<S>();
+  extern __shared__ __align__(16) unsigned char sq_raw[];
+  const int K = g.kx_max, K1 = K + 1, KP = K1 | 1;
+  C* tile = reinterpret_cast<C*>(sq_raw);
+  C* otile = tile + kZinvLines * ZC * KP;
+  const SqLane2<S> ln;
+  C* xb = otile + 3 * K1 * ZC + (ln.warp * G + ln.gi) * XB;
+  C* stab = otile + 3 * K1 * ZC + kSqWarps * G * XB;
+  const int z0 = blockIdx.x * ZC, y = blockIdx.y;
+  const int zl = ln.warp * G + ln.gi;
+  const Rl ub = ubase ? (Rl)ubase[y] : (Rl)0;
+  const Rl dub = dubase ? (Rl)dubase[y] : (Rl)0;
+  const Rl c = (Rl)g.c_inv, lam = (Rl)lam_d, half = (Rl)0.5;
+  xsq_stage_tile<C, ZC>(g, inter, tile, kZinvLines, y, z0);
+  for (int e = threadIdx.x; e < N; e += blockDim.x) stab[e] = twtab[e];
+  cp_async_wait<0>();
+  __syncthreads();
+  const bool live = ln.live;
+  const int t = ln.t, h = ln.h, pr = ln.partner;
+  Rl U[H], V[H], W[H], DIV[H], A0[H], A1[H], A2[H];
+  C x[H];
+  xh2_fill<C, S, ZC>(g, tile, zl, t, h, live, x, 0, false, 1, false);  // (u, v)
+  sq2_fft<S, true>(x, stab, xb, t, h, pr, live);
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    U[j] = x[j].x * c;
+    V[j] = x[j].y * c;
+  }
+  xh2_fill<C, S, ZC>(g, tile, zl, t, h, live, x, 2, false, 0, true);  // (w, du/dx)
+  sq2_fft<S, true>(x, stab, xb, t, h, pr, live);
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    W[j] = x[j].x * c;
+    const Rl dxu = x[j].y * c;
+    DIV[j] = dxu;
+    A0[j] = lam * U[j] * dxu + ub * dxu;
+  }
+  xh2_fill<C, S, ZC>(g, tile, zl, t, h, live, x, 1, true, 2, true);  // (dv/dx, dw/dx)
+  sq2_fft<S, true>(x, stab, xb, t, h, pr, live);
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const Rl dxv = x[j].x * c, dxw = x[j].y * c;
+    A1[j] = lam * U[j] * dxv + ub * dxv;
+    A2[j] = lam * U[j] * dxw + ub * dxw;
+  }
+  xh2_fill<C, S, ZC>(g, tile, zl, t, h, live, x, 4, false, 8, false);  // (dv/dy, dw/dz)
+  sq2_fft<S, true>(x, stab, xb, t, h, pr, live);
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const Rl dyv = x[j].x * c, dzw = x[j].y * c;
+    DIV[j] += dyv + dzw;
+    A1[j] += lam * V[j] * dyv;
+    A2[j] += lam * W[j] * dzw;
+  }
+  xh2_fill<C, S, ZC>(g, tile, zl, t, h, live, x, 3, false, 5, false);  // (du/dy, dw/dy)
+  sq2_fft<S, true>(x, stab, xb, t, h, pr, live);
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const Rl dyu = x[j].x * c, dyw = x[j].y * c;
+    A0[j] += lam * V[j] * dyu;
+    A2[j] += lam * V[j] * dyw;
+  }
+  xh2_fill<C, S, ZC>(g, tile, zl, t, h, live, x, 6, false, 7, false);  // (du/dz, dv/dz)
+  sq2_fft<S, true>(x, stab, xb, t, h, pr, live);
+  C z2[H];
+#pragma unroll
+  for (int j = 0; j < H; ++j) {
+    const Rl dzu = x[j].x * c, dzv = x[j].y * c;
+    const Rl a0 = A0[j] + lam * W[j] * dzu;
+    const Rl a1 = A1[j] + lam * W[j] * dzv;
+    const Rl d = DIV[j];
+    const Rl h0 = -a0 + half * lam * d * U[j] - V[j] * dub + half * d * ub;
+    const Rl h1 = -a1 + half * lam * d * V[j];
+    const Rl h2 = -A2[j] + half * lam * d * W[j];
+    x[j] = cmake<C>(h0, h1);
+    z2[j] = cmake<C>(h2, (Rl)0);
+  }
+  // forward transforms and the kx >= 0 outputs of the column
+  const bool colok = live && z0 + zl < g.pz;
+  sq2_fft<S, false>(x, stab, xb, t, h, pr, colok);
+  sq2_fft<S, false>(z2, stab, xb, t, h, pr, colok);
+  if (colok) {
+#pragma unroll
+    for (int j = 0; j < H; ++j) {
+      const int p = t + S * (2 * j + h);
+      xb[p] = x[j];
+      if (p <= K) otile[(2 * K1 + p) * ZC + zl] = z2[j];
+    }
+  }
+  __syncwarp();
+  if (colok) {
+    for (int kx = h * S + t; kx <= K; kx += 2 * S) {
+      const C a = xb[kx];
+      const C b = xb[kx == 0 ? 0 : N - kx];
+      otile[(0 * K1 + kx) * ZC + zl] = cmake<C>(half * (a.x + b.x), half * (a.y - b.y));
+      otile[(1 * K1 + kx) * ZC + zl] = cmake<C>(half * (a.y + b.y), -half * (a.x - b.x));
+    }
+  }
+  __syncthreads();
+  xsq_store<C, ZC>(g, otile, out3, y, z0);
 }
 
 }  // namespace jsd

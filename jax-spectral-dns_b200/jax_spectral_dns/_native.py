@@ -48,7 +48,7 @@ EXPORTED = (
     "jsd_workspace_bytes", "jsd_launches_per_step", "jsd_last_error", "jsd_abi_version",
     "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc", "jsd_step_trajectory",
     "jsd_launches_first_step_extra", "jsd_autotune", "jsd_gemm_config",
-    "jsd_set_gemm_config",
+    "jsd_set_gemm_config", "jsd_xmid_variant", "jsd_set_xmid_variant",
 )
 
 # GEMM call sites of a plan (jsd_gemm_config) and the number of DMMA tile configurations
@@ -95,6 +95,8 @@ def load(path: str = LIB_PATH):
     lib.jsd_autotune.argtypes = [vp, vp]
     lib.jsd_gemm_config.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_set_gemm_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+    lib.jsd_xmid_variant.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    lib.jsd_set_xmid_variant.argtypes = [vp, ctypes.c_int]
     lib.jsd_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED:

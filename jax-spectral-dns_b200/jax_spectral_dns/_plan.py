@@ -120,6 +120,15 @@ class StepPlan:
         _native.check(self.lib.jsd_set_gemm_config(self.handle, _native.GEMM_SITES[site], int(config)),
                       "jsd_set_gemm_config")
 
+    def xmid_variant(self):
+        """(x-pass variant in use, [autotune ms of variants 0, 1, 2])."""
+        times = (ctypes.c_float * 3)()
+        v = int(self.lib.jsd_xmid_variant(self.handle, times))
+        return v, [float(t) for t in times]
+
+    def set_xmid_variant(self, variant: int) -> None:
+        _native.check(self.lib.jsd_set_xmid_variant(self.handle, int(variant)), "jsd_set_xmid_variant")
+
     def gemm_configs(self) -> dict:
         """{site: (configuration id, [per-configuration autotune ms])}."""
         out = {}

@@ -1,6 +1,7 @@
 """The register-resident square FFT (jsd_fftsq.cuh) on the host: prime-factor
 S-point DFTs and the two-stage S*S transform, lanes emulated one after another,
-against a direct DFT in long double. Compiles host code with nvcc; no GPU."""
+and the half-split form (a line on 2 S lanes), against a direct DFT in long
+double. Compiles host code with nvcc; no GPU."""
 import os
 import shutil
 import subprocess
@@ -24,7 +25,8 @@ def test_square_fft_matches_direct_dft(tmp_path):
                     os.path.join(HERE, "host_kernels", "fftsq_check.cu")], check=True, capture_output=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
     rows = [ln.split() for ln in out if ln.strip()]
-    sizes = {int(r[0]) for r in rows}
-    assert {2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 15, 20, 21, 24, 28, 30} <= sizes
+    sizes = {r[0] for r in rows}
+    assert {str(s) for s in (2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 15, 20, 21, 24, 28, 30)} <= sizes
+    assert {"h4", "h6", "h8", "h10", "h14"} <= sizes  # half-split forms
     for s, fwd, inv in rows:
         assert float(fwd) < 1e-14 and float(inv) < 1e-14, (s, fwd, inv)

@@ -60,3 +60,33 @@ def test_autotuned_plan_steps_identically(cuda, precision):
     a = _steps(plain, u0, 3)
     b = _steps(tuned, u0, 3)
     assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+def test_every_xmid_variant_matches_reference(cuda, variant):
+    """x-pass kernels (S-lane register FFT, half-split register FFT,
+    shared-memory FFT) on the golden nonlinear perturbation case, FP64."""
+    d = golden("nonlin_pert_9x33x9")
+    p = _plan(d["shape"], d["lengths"], d["re"], d["dt"])
+    p.set_xmid_variant(variant)
+    assert p.xmid_variant()[0] == variant
+    st = _steps(p, d["u0"], 20)
+    assert rel(to_reference_layout(st).cpu().numpy(), d["u20"]) < TOL
+
+
+def test_xmid_variants_agree_in_mixed_precision(cuda):
+    shape, lx, lz, re, dt = (48, 65, 48), 2 * np.pi, np.pi, 5000.0, 0.005
+    u0 = seeded_velocity_hat(shape, (lx, lz), (8, 8), 1e-3, seed=5)
+    out = []
+    for v in (0, 1, 2):
+        p = _plan(shape, (lx, lz), re, dt, precision="mixed")
+        p.set_xmid_variant(v)
+        out.append(to_reference_layout(_steps(p, u0, 5)).cpu().numpy())
+    assert rel(out[1], out[0]) < 1e-6 and rel(out[2], out[0]) < 1e-6
+
+
+def test_autotune_chooses_an_available_xmid_variant(cuda):
+    shape, lx, lz, re, dt = (48, 65, 48), 2 * np.pi, np.pi, 5000.0, 0.005
+    p = _plan(shape, (lx, lz), re, dt, autotune=True)
+    v, times = p.xmid_variant()
+    assert times[v] > 0 and times[v] == min(t for t in times if t > 0)
