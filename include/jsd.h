@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define JSD_ABI_VERSION 1
+#define JSD_ABI_VERSION 2  /* 2: jsd_desc gained n_batch, re_tau_batch */
 
 enum jsd_status {
   JSD_OK = 0,
@@ -76,6 +76,16 @@ typedef struct jsd_desc {
   const double* lhs_inv_ns;/* [3*(2ny)^2] (0,0) implicit inverses per RK stage */
   int precision;           /* JSD_PRECISION_FP64, or JSD_PRECISION_MIXED: FP32 transforms and products,
                               split-TF32 tensor-core y-derivatives; solves stay FP64 */
+  /* Batch of independent runs on the same box (no counterpart in the
+   * reference, which steps one field at a time). n_batch <= 1: one run.
+   * n_batch > 1: every field holds the runs side by side, plane by plane,
+   *     element (c, y, run, ix, iz) at (((c * Ny + y) * n_batch + run) * Mx + ix) * Mz + iz,
+   * so each y-operator is one product over all runs; re_tau_batch[n_batch]
+   * gives each run's Reynolds number and rhs_ns / lhs_inv_ns hold n_batch
+   * consecutive sets of 3 matrices. NS and perturbation equations without
+   * mass-flux control. */
+  int n_batch;
+  const double* re_tau_batch;
 } jsd_desc;
 
 enum jsd_precision { JSD_PRECISION_FP64 = 0, JSD_PRECISION_MIXED = 1 };
@@ -121,6 +131,19 @@ int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* strea
  * double `out`. Replaces VectorField.no_hat().energy() (field.py:607-611,
  * 1468-1474). */
 int jsd_energy(jsd_plan* plan, const void* state, double* out, void* stream);
+
+/* Kinetic energy of every active run of a batch plan: out[run], run <
+ * jsd_batch_active (device pointer). The single-run entry points (jsd_energy,
+ * jsd_flow_rate, jsd_correct_mass_flux, jsd_nonlinear_terms) reject batch
+ * plans. No counterpart in the reference. */
+int jsd_energy_runs(jsd_plan* plan, const void* state, double* out, void* stream);
+
+/* Step only the first n_runs runs of a batch plan from now on (1 <= n_runs <=
+ * n_batch): the caller keeps its state packed for n_runs runs, i.e. drops
+ * finished runs from the end of the run order. Runs keep their Reynolds
+ * numbers. No counterpart in the reference. */
+int jsd_set_batch_active(jsd_plan* plan, int n_runs);
+int jsd_batch_active(const jsd_plan* plan);
 
 /* Kinetic energy of a state without a plan and without allocating anything.
  * No counterpart in the reference. For callers that cannot allocate device

@@ -158,6 +158,8 @@ struct jsd_plan {
   // device operator tables
   double2 *twx = nullptr, *twz = nullptr;
   float2 *twx32 = nullptr, *twz32 = nullptr;
+  int nb_max = 1;               // runs the workspace is sized for (g.nb = runs stepped now)
+  double* re_run = nullptr;     // Reynolds number per run of a batch (device)
   int gemm_cfg[3] = {2, 2, 2};  // DMMA tile configuration per call site (GemmSite)
   int xmid_variant = 2;         // x-pass kernel (launch_xmid), set at creation, autotuned on request
   float xmid_ms[3] = {};        // autotuner timings of the x-pass variants (0: not timed)
@@ -288,7 +290,7 @@ int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int
   }
   SplitGemmBatch b;
   memset(&b, 0, sizeof(b));
-  b.N = 2 * p->g.nk;
+  b.N = 2 * p->g.nk * p->g.nb;
   b.lda = p->lda;
   b.ldb = b.N;
   b.ldc = b.N;
@@ -311,7 +313,7 @@ int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int
 GemmBatch gemm_batch(const jsd_plan* p) {
   GemmBatch b;
   memset(&b, 0, sizeof(b));
-  b.N = 2 * p->g.nk;
+  b.N = 2 * p->g.nk * p->g.nb;
   b.lda = p->lda;
   b.ldb = b.N;
   b.ldc = b.N;
@@ -339,6 +341,13 @@ int grid_for(size_t total, int block) {
   return (int)(g < 1 ? 1 : g);
 }
 
+// Geometry seen by kernels that work plane by plane: one plane per (y, run).
+Geo planes_of(const Geo& g) {
+  Geo gp = g;
+  gp.ny = g.ny * g.nb;
+  return gp;
+}
+
 // h_v = -D q - k^2 H1 (only for the nonlinear-term hook)
 __global__ void k_assemble_hv(Geo g, const double2* __restrict__ dq, const double2* __restrict__ h1,
                               double2* __restrict__ hv) {
@@ -358,12 +367,13 @@ int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2*
 // nonlinear terms of `state` into p->q, p->H1, p->hg and conv00 slot `stage`
 int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage, cudaStream_t s) {
   const Geo& g = p->g;
-  const size_t fs = (size_t)g.ny * g.nk;
+  const Geo gp = planes_of(g);
+  const size_t fs = (size_t)gp.ny * g.nk;
   const double2* u = state;
   const double2* v = state + fs;
   const double2* w = state + 2 * fs;
   const int ny = g.ny;
-  double2* conv = p->conv + (size_t)stage * 2 * ny;
+  double2* conv = p->conv + (size_t)stage * 2 * gp.ny;
   const bool linear = p->desc.linearise && p->desc.kind != JSD_KIND_NS;
   if (p->desc.kind == JSD_KIND_DUAL && !linear && !uhist)
     return fail(JSD_ERR_STATE, "dual step needs the forward state (jsd_set_history)");
@@ -378,10 +388,10 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
     const int blk = 256;
     ProfScope ps(p, JSD_PROF_LINEAR, sizeof(double2) * 7.0 * fs, s);
     if (p->desc.kind == JSD_KIND_PERTURBATION)
-      k_linear_terms<kPerturbation><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, dv_in, p->ub, p->dub,
+      k_linear_terms<kPerturbation><<<grid_for(fs, blk), blk, 0, s>>>(gp, u, v, w, dv_in, p->ub, p->dub,
                                                                       p->q, p->H1, p->hg, conv);
     else
-      k_linear_terms<kDual><<<grid_for(fs, blk), blk, 0, s>>>(g, u, v, w, dv_in, p->ub, p->dub, p->q,
+      k_linear_terms<kDual><<<grid_for(fs, blk), blk, 0, s>>>(gp, u, v, w, dv_in, p->ub, p->dub, p->q,
                                                               p->H1, p->hg, conv);
     JSD_LAUNCHED("k_linear_terms");
     return 0;
@@ -430,7 +440,7 @@ int default_xmid_variant(const jsd_plan* p) {
 
 template <typename C>
 int launch_xmid(jsd_plan* p, int variant, C* inter, C* out3, cudaStream_t s) {
-  const Geo& g = p->g;
+  const Geo g = planes_of(p->g);
   const int ny = g.ny;
   const bool dual = p->desc.kind == JSD_KIND_DUAL;
   const double lam = (p->desc.kind == JSD_KIND_NS || !p->desc.linearise) ? 1.0 : 0.0;
@@ -474,7 +484,7 @@ int launch_xmid(jsd_plan* p, int variant, C* inter, C* out3, cudaStream_t s) {
 
 template <typename C>
 int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2* conv, cudaStream_t s) {
-  const Geo& g = p->g;
+  const Geo g = planes_of(p->g);
   const size_t fs = (size_t)g.ny * g.nk;
   const int ny = g.ny;
   const bool dual = p->desc.kind == JSD_KIND_DUAL;
@@ -540,7 +550,8 @@ int transforms(jsd_plan* p, const double2* state, const double2* uhist, double2*
 
 int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cudaStream_t s) {
   const Geo& g = p->g;
-  const size_t fs = (size_t)g.ny * g.nk;
+  const Geo gp = planes_of(g);
+  const size_t fs = (size_t)gp.ny * g.nk;
   const int ny = g.ny, ni = g.ny - 2;
   double2* u = state;
   double2* v = state + fs;
@@ -556,14 +567,14 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
   if (rc) return rc;
   const int blk = 256;
   if (!p->om_valid) {
-    k_omega<<<grid_for(fs, blk), blk, 0, s>>>(g, u, w, p->om);
+    k_omega<<<grid_for(fs, blk), blk, 0, s>>>(gp, u, w, p->om);
     JSD_LAUNCHED("k_omega");
   }
   // eigenbasis transforms
   {
     GemmBatch b = gemm_batch(p);
     const size_t E = p->edoubles;
-    const size_t rowd = 2 * (size_t)g.nk;  // doubles per y-row
+    const size_t rowd = 2 * (size_t)g.nk * g.nb;  // doubles per Chebyshev row
     add_entry(b, p->VinvD, (const double*)p->q, p->X1, ni, ny);
     add_entry(b, p->Vinv, (const double*)p->H1 + rowd, p->T + 0 * E, ni, ni);
     add_entry(b, p->Vinv, (const double*)p->hg + rowd, p->T + 1 * E, ni, ni);
@@ -573,10 +584,10 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     if (rc) return rc;
   }
   {
-    EigTables t{p->lam, p->c0, p->cN, p->sgn, p->w0, p->wN};
+    EigTables t{p->lam, p->c0, p->cN, p->sgn, p->w0, p->wN, p->re_run};
     StageCoef sc{kAlpha[st], kBeta[st], kGamma[st], kXi[st], p->desc.dt, p->desc.dt_explicit, p->desc.re_tau,
                  st == 0 ? 1 : 0};
-    const int N = 2 * g.nk;
+    const int N = 2 * g.nk * g.nb;
     const size_t E = p->edoubles;
     // reads X1, 4 transformed fields, 2 old terms; writes 2 old terms, v~ twice, om~
     ProfScope ps(p, JSD_PROF_EIGEN, sizeof(double) * 13.0 * (double)E, s);
@@ -594,10 +605,11 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     const size_t n2 = 2 * (size_t)ny;
     const double* rns = p->rhs_ns + (size_t)st * n2 * n2;
     const double* lns = p->lhs_inv_ns + (size_t)st * n2 * n2;
-    const double2* conv = p->conv + (size_t)st * 2 * ny;
-    const double2* conv_old = st == 0 ? nullptr : p->conv + (size_t)(st - 1) * 2 * ny;
+    const double2* conv = p->conv + (size_t)st * 2 * gp.ny;
+    const double2* conv_old = st == 0 ? nullptr : p->conv + (size_t)(st - 1) * 2 * gp.ny;
     const double dte = p->desc.dt_explicit;
-    k_mean_flow<<<1, kMeanFlowThreads, sizeof(double2) * 2 * n2, s>>>(g, rns, lns, u, w, conv, conv_old, dpdx, p->dpdx_scale,
+    // per-run matrices: rns / lns point at run 0's stage-st matrices, the kernel offsets by run
+    k_mean_flow<<<g.nb, kMeanFlowThreads, sizeof(double2) * 2 * n2, s>>>(g, rns, lns, u, w, conv, conv_old, dpdx, p->dpdx_scale,
                                                         dte * kGamma[st], dte * kXi[st], p->uw00);
     JSD_LAUNCHED("k_mean_flow");
   }
@@ -740,6 +752,7 @@ int jsd_energy_noalloc(const void* state, int mx, int ny, int mz, int px_ref, in
   g.kx_max = mx / 2;
   g.kz_max = mz / 2;
   g.nk = mx * mz;
+  g.nb = 1;
   const double two_pi = 2.0 * M_PI;
   const double s = (lx / two_pi) * (lz / two_pi);
   g.c_inv = s / std::sqrt((double)px_ref * (double)pz_ref);
@@ -796,9 +809,9 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Geo& g = plan->g;
   const int ny = g.ny, ni = g.ny - 2;
-  const size_t fs = (size_t)ny * g.nk;
+  const size_t fs = (size_t)ny * g.nk * g.nb;
   const size_t E = plan->edoubles;
-  const size_t rowd = 2 * (size_t)g.nk;
+  const size_t rowd = 2 * (size_t)g.nk * g.nb;
   // the timed products read these workspace fields: give them defined values
   for (double2* f : {plan->q, plan->H1, plan->hg})
     JSD_CUDA(cudaMemsetAsync(f, 0, fs * sizeof(double2), s));
@@ -941,6 +954,14 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   if (d->kind != JSD_KIND_NS && (!d->base_u || !d->base_du))
     return fail(JSD_ERR_ARG, "perturbation and dual equations need the base profile");
   if (d->re_tau == 0.0 || d->dt == 0.0 || d->dt_explicit == 0.0) return fail(JSD_ERR_ARG, "zero Re or dt");
+  const int nb = d->n_batch > 1 ? d->n_batch : 1;
+  if (nb > 1) {
+    if (d->kind == JSD_KIND_DUAL || d->constant_mass_flux)
+      return fail(JSD_ERR_ARG, "batches of runs support the NS and perturbation equations without mass-flux control");
+    if (!d->re_tau_batch) return fail(JSD_ERR_ARG, "a batch needs re_tau_batch");
+    for (int r = 0; r < nb; ++r)
+      if (d->re_tau_batch[r] == 0.0) return fail(JSD_ERR_ARG, "zero Re in re_tau_batch");
+  }
   int rc = set_smem_limits();
   if (rc) return rc;
 
@@ -956,6 +977,8 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   g.px = d->px_fft > 0 ? d->px_fft : choose_fft_size(d->mx);
   g.pz = d->pz_fft > 0 ? d->pz_fft : choose_fft_size(d->mz);
   g.nk = d->mx * d->mz;
+  g.nb = nb;
+  p->nb_max = nb;
   const double two_pi = 2.0 * M_PI;
   g.ax = two_pi / d->lx;
   g.az = two_pi / d->lz;
@@ -980,9 +1003,9 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   }
   const int ny = d->ny, ni = ny - 2;
   p->lda = (ny + 15) / 16 * 16;
-  p->fdoubles = 2 * (size_t)ny * g.nk;
-  p->edoubles = 2 * (size_t)ni * g.nk;
-  const size_t fs = (size_t)ny * g.nk;
+  p->fdoubles = 2 * (size_t)ny * g.nk * nb;
+  p->edoubles = 2 * (size_t)ni * g.nk * nb;
+  const size_t fs = (size_t)ny * g.nk * nb;  // complex entries per field (all runs)
   const size_t n2 = 2 * (size_t)ny;
 
   std::vector<double> VinvD((size_t)ni * ny, 0.0), Vfull((size_t)ny * ni, 0.0), DVfull((size_t)ny * ni, 0.0);
@@ -1058,8 +1081,9 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(upload(p, &p->w0, d->w0, ni));
   JSD_TRY(upload(p, &p->wN, d->wN, ni));
   JSD_TRY(upload(p, &p->yw, d->y_weights, ny));
-  JSD_TRY(upload(p, &p->rhs_ns, d->rhs_ns, 3 * n2 * n2));
-  JSD_TRY(upload(p, &p->lhs_inv_ns, d->lhs_inv_ns, 3 * n2 * n2));
+  JSD_TRY(upload(p, &p->rhs_ns, d->rhs_ns, (size_t)nb * 3 * n2 * n2));
+  JSD_TRY(upload(p, &p->lhs_inv_ns, d->lhs_inv_ns, (size_t)nb * 3 * n2 * n2));
+  if (nb > 1) JSD_TRY(upload(p, &p->re_run, d->re_tau_batch, (size_t)nb));
   if (d->base_u) JSD_TRY(upload(p, &p->ub, d->base_u, ny));
   if (d->base_du) JSD_TRY(upload(p, &p->dub, d->base_du, ny));
 
@@ -1069,21 +1093,21 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(dev_alloc(p, (void**)&p->Dfld, 3 * (size_t)nsets * fs * sizeof(double2)));
   if (!linear) {
     const size_t csz = p->mixed ? sizeof(float2) : sizeof(double2);
-    JSD_TRY(dev_alloc(p, (void**)&p->inter, (size_t)kZinvLines * nsets * ny * K1 * g.pz * csz));
-    JSD_TRY(dev_alloc(p, (void**)&p->out3, 3 * (size_t)ny * K1 * g.pz * csz));
+    JSD_TRY(dev_alloc(p, (void**)&p->inter, (size_t)kZinvLines * nsets * ny * nb * K1 * g.pz * csz));
+    JSD_TRY(dev_alloc(p, (void**)&p->out3, 3 * (size_t)ny * nb * K1 * g.pz * csz));
   }
   for (double2** f : {&p->q, &p->H1, &p->hg, &p->om, &p->dvn, &p->tmp})
     JSD_TRY(dev_alloc(p, (void**)f, fs * sizeof(double2)));
-  JSD_TRY(dev_alloc(p, (void**)&p->conv, 3 * n2 * sizeof(double2)));
-  JSD_TRY(dev_alloc(p, (void**)&p->uw00, n2 * sizeof(double2)));
+  JSD_TRY(dev_alloc(p, (void**)&p->conv, 3 * n2 * nb * sizeof(double2)));
+  JSD_TRY(dev_alloc(p, (void**)&p->uw00, n2 * nb * sizeof(double2)));
   JSD_TRY(dev_alloc(p, (void**)&p->X1, p->edoubles * sizeof(double)));
   JSD_TRY(dev_alloc(p, (void**)&p->T, 4 * p->edoubles * sizeof(double)));
   for (double** f : {&p->hv_old, &p->hg_old, &p->vnt, &p->omnt, &p->vnt_alt, &p->omnt_alt})
     JSD_TRY(dev_alloc(p, (void**)f, p->edoubles * sizeof(double)));
-  JSD_TRY(dev_alloc(p, (void**)&p->partial, (size_t)ny * sizeof(double)));
+  JSD_TRY(dev_alloc(p, (void**)&p->partial, (size_t)ny * nb * sizeof(double)));
   JSD_TRY(dev_alloc(p, (void**)&p->scal, 8 * sizeof(double)));
   // conv entries are only written at (0,0); clear once so every read is defined
-  JSD_CUDA(cudaMemset(p->conv, 0, 3 * n2 * sizeof(double2)));
+  JSD_CUDA(cudaMemset(p->conv, 0, 3 * n2 * nb * sizeof(double2)));
 #undef JSD_TRY
   *out = p;
   return 0;
@@ -1126,7 +1150,7 @@ int jsd_step_trajectory(jsd_plan* plan, void* state, double* dpdx, int first_ste
                         void* stream) {
   if (!plan || !state || !dpdx || !states || n_steps < 0) return fail(JSD_ERR_ARG, "null argument");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  const size_t bytes = 3 * (size_t)plan->g.ny * plan->g.nk * sizeof(double2);
+  const size_t bytes = 3 * (size_t)plan->g.ny * plan->g.nk * plan->g.nb * sizeof(double2);
   char* out = static_cast<char*>(states);
   JSD_CUDA(cudaMemcpyAsync(out, state, bytes, cudaMemcpyDeviceToDevice, s));
   plan->ev_valid = plan->om_valid = plan->dv_valid = false;
@@ -1140,6 +1164,7 @@ int jsd_step_trajectory(jsd_plan* plan, void* state, double* dpdx, int first_ste
 
 int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* stream) {
   if (!plan || !state) return fail(JSD_ERR_ARG, "null argument");
+  if (plan->g.nb > 1) return fail(JSD_ERR_ARG, "single-run entry point called on a batch plan (see jsd_energy_runs)");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* dp = dpdx ? dpdx : plan->scal + 1;  // a scratch slot when the caller keeps no pressure gradient
   plan->ev_valid = plan->om_valid = plan->dv_valid = false;
@@ -1148,6 +1173,7 @@ int jsd_correct_mass_flux(jsd_plan* plan, void* state, double* dpdx, void* strea
 
 int jsd_energy(jsd_plan* plan, const void* state, double* out, void* stream) {
   if (!plan || !state || !out) return fail(JSD_ERR_ARG, "null argument");
+  if (plan->g.nb > 1) return fail(JSD_ERR_ARG, "single-run entry point called on a batch plan (see jsd_energy_runs)");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Geo& g = plan->g;
   k_plane_sums<<<g.ny, 256, 0, s>>>(g, static_cast<const double2*>(state), 3, 0, plan->partial);
@@ -1157,8 +1183,32 @@ int jsd_energy(jsd_plan* plan, const void* state, double* out, void* stream) {
   return 0;
 }
 
+int jsd_energy_runs(jsd_plan* plan, const void* state, double* out, void* stream) {
+  if (!plan || !state || !out) return fail(JSD_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Geo& g = plan->g;
+  const Geo gp = planes_of(g);
+  k_plane_sums<<<gp.ny, 256, 0, s>>>(gp, static_cast<const double2*>(state), 3, 0, plan->partial);
+  JSD_LAUNCHED("k_plane_sums");
+  k_weighted_total_runs<<<(g.nb + 127) / 128, 128, 0, s>>>(g.ny, g.nb, plan->yw, plan->partial,
+                                                           0.25 * g.c_inv * g.c_inv, out);
+  JSD_LAUNCHED("k_weighted_total_runs");
+  return 0;
+}
+
+int jsd_set_batch_active(jsd_plan* plan, int n_runs) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  if (n_runs < 1 || n_runs > plan->nb_max) return fail(JSD_ERR_ARG, "active runs must be in [1, n_batch]");
+  plan->g.nb = n_runs;
+  plan->ev_valid = plan->om_valid = plan->dv_valid = false;
+  return 0;
+}
+
+int jsd_batch_active(const jsd_plan* plan) { return plan ? plan->g.nb : 0; }
+
 int jsd_flow_rate(jsd_plan* plan, const void* u_field, double* out, void* stream) {
   if (!plan || !u_field || !out) return fail(JSD_ERR_ARG, "null argument");
+  if (plan->g.nb > 1) return fail(JSD_ERR_ARG, "single-run entry point called on a batch plan (see jsd_energy_runs)");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Geo& g = plan->g;
   k_plane_sums<<<g.ny, 256, 0, s>>>(g, static_cast<const double2*>(u_field), 1, 1, plan->partial);
@@ -1170,6 +1220,7 @@ int jsd_flow_rate(jsd_plan* plan, const void* u_field, double* out, void* stream
 
 int jsd_nonlinear_terms(jsd_plan* plan, const void* state, int time_step, void* h_v, void* h_g, void* stream) {
   if (!plan || !state || !h_v || !h_g) return fail(JSD_ERR_ARG, "null argument");
+  if (plan->g.nb > 1) return fail(JSD_ERR_ARG, "single-run entry point called on a batch plan (see jsd_energy_runs)");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Geo& g = plan->g;
   const size_t fs = (size_t)g.ny * g.nk;

@@ -1,7 +1,8 @@
 // Shared device helpers for the velocity-vorticity channel step.
 //
 // Spectral fields are stored plane by plane: element (y, ix, iz) of a field
-// lives at ((y * mx + ix) * mz + iz) as an interleaved complex double (re, im).
+// lives at ((y * mx + ix) * mz + iz) as an interleaved complex double (re, im)
+// (for a batch of runs, y is the plane index y_cheb * nb + run).
 // A vector field is three such fields back to back. Wavenumber indices follow
 // the FFT order of the reference ([0..K, -K..-1]); y index 0 is y = +1.
 #pragma once
@@ -19,6 +20,9 @@ struct Geo {
   double ax, az;     // wavenumber units 2 pi / Lx, 2 pi / Lz
   double c_inv;      // s / sqrt(Px_ref Pz_ref): coefficient -> physical value
   double c_fwd;      // sqrt(Px_ref Pz_ref) / (s px pz): unnormalised DFT -> coefficient
+  int nb;            // runs stepped together (1: a single run). A batch stores each field
+                     // as [y][run][kx][kz]: plane p = y * nb + run, and a Chebyshev row
+                     // holds nb * nk modes. Kernels that only see planes get ny = planes.
 };
 
 // complex helpers for double2 (FP64 path) and float2 (FP32 transforms of the

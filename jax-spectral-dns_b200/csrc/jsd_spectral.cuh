@@ -186,8 +186,8 @@ __global__ void __launch_bounds__(kXmidThreads) k_xmid(Geo g, FftDesc fx, const 
   C* lb = la + 2 * ZB * L;
   const int z0 = blockIdx.x * ZB;
   const int y = blockIdx.y;
-  const Rl ub = ubase ? (Rl)ubase[y] : (Rl)0;
-  const Rl dub = dubase ? (Rl)dubase[y] : (Rl)0;
+  const Rl ub = ubase ? (Rl)ubase[y / g.nb] : (Rl)0;
+  const Rl dub = dubase ? (Rl)dubase[y / g.nb] : (Rl)0;
   const Rl c = (Rl)g.c_inv;
   const Rl lam = (Rl)lam_d, half = (Rl)0.5;
   const int npt = ZB * px;
@@ -278,8 +278,8 @@ __global__ void __launch_bounds__(kXmidThreads) k_xmid_dual(Geo g, FftDesc fx, c
   C* lb = la + 2 * ZB * L;
   const int z0 = blockIdx.x * ZB;
   const int y = blockIdx.y;
-  const Rl ub = (Rl)ubase[y];
-  const Rl dub = (Rl)dubase[y];
+  const Rl ub = (Rl)ubase[y / g.nb];
+  const Rl dub = (Rl)dubase[y / g.nb];
   const Rl c = (Rl)g.c_inv;
   const Rl q4 = (Rl)0.25;
   const int npt = ZB * px;
@@ -455,7 +455,7 @@ __global__ void k_linear_terms(Geo g, const double2* __restrict__ u, const doubl
     int sx, sz;
     bool cj;
     truncation_source(g, ix, iz, sx, sz, cj);
-    const double ub = ubase[y], dub = dubase[y];
+    const double ub = ubase[y / g.nb], dub = dubase[y / g.nb];
     double2 Pa[3], Pb[3];
     linear_pre<KIND>(g, u, v, w, dv, y, sx, sz, ub, dub, Pa);
     linear_pre<KIND>(g, u, v, w, dv, y, -sx, -sz, ub, dub, Pb);
@@ -500,6 +500,7 @@ struct EigTables {
   const double* sgn;
   const double* w0;
   const double* wN;
+  const double* re_run;  // Reynolds number per run of a batch (nullptr: StageCoef::re)
 };
 
 struct StageCoef {
@@ -518,24 +519,26 @@ __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
     const double* __restrict__ vfield, double* __restrict__ hv_old, double* __restrict__ hg_old,
     double* __restrict__ vnt, double* __restrict__ omnt) {
   __shared__ double red[kEigParts][6][kEigCols];
-  const int N = 2 * g.nk;
+  const int N = 2 * g.nk * g.nb;  // columns: real and imaginary parts of every mode of every run
   const int lane = threadIdx.x % kEigCols;
   const int part = threadIdx.x / kEigCols;
   const int c = blockIdx.x * kEigCols + lane;
   const bool active = c < N;
   const int n = g.ny - 2;
   const int j0 = (n * part) / kEigParts, j1 = (n * (part + 1)) / kEigParts;
-  double k2 = 0.0, v0 = 0.0, vN = 0.0;
+  double k2 = 0.0, v0 = 0.0, vN = 0.0, re = sc.re;
   if (active) {
-    const int kp = c >> 1;
+    const int run = (c >> 1) / g.nk;
+    const int kp = (c >> 1) - run * g.nk;
     const int ix = kp / g.mz, iz = kp - (kp / g.mz) * g.mz;
     const double kx = kx_of(g, ix), kz = kz_of(g, iz);
     k2 = kx * kx + kz * kz;
     v0 = vfield[c];
     vN = vfield[(size_t)(g.ny - 1) * N + c];
+    if (t.re_run) re = t.re_run[run];
   }
-  const double ar = sc.alpha * sc.dt / sc.re;
-  const double br = sc.beta * sc.dt / sc.re;
+  const double ar = sc.alpha * sc.dt / re;
+  const double br = sc.beta * sc.dt / re;
   double d0p = 0, dNp = 0, d0a = 0, dNa = 0, d0b = 0, dNb = 0;
   if (active) {
     for (int jb = j0; jb < j1; jb += kEigBatch) {
@@ -629,7 +632,8 @@ __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
 // (navier_stokes.py:1417-1504) with its own matrices:
 //   x_new = Linv_ns (R_ns x + dt_e gamma N + dt_e xi N_old),
 //   N = [-conv00_x - dpdx * scale, -conv00_z]
-// One block of 2 Ny threads (rows). conv_old == nullptr means zero.
+// One block per run (g.ny = Chebyshev points, g.nb runs; conv entries per plane,
+// matrices and uw00 per run). conv_old == nullptr means zero.
 // ---------------------------------------------------------------------------
 constexpr int kMeanFlowThreads = 1024;
 
@@ -639,12 +643,18 @@ __global__ void __launch_bounds__(kMeanFlowThreads) k_mean_flow(
     const double* __restrict__ dpdx, double dpdx_scale, double dt_gamma, double dt_xi, double2* __restrict__ uw00) {
   extern __shared__ __align__(16) double2 msm[];
   const int n = g.ny, n2 = 2 * g.ny;
+  // block = run of a batch: its matrices, its planes (y * nb + run) and conv entries
+  const int run = blockIdx.x, nb = g.nb;
+  rhs_ns += (size_t)run * 3 * n2 * n2;
+  lhs_inv_ns += (size_t)run * 3 * n2 * n2;
+  uw00 += (size_t)run * n2;
   double2* xv = msm;       // current (U00, W00)
   double2* rv = xv + n2;   // right-hand side
   const double dp = dpdx ? dpdx[0] * dpdx_scale : 0.0;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  auto cidx = [&](int i) { return (i < n) ? i * nb + run : n * nb + (i - n) * nb + run; };
   for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-    xv[i] = (i < n) ? u[sidx(g, i, 0, 0)] : w[sidx(g, i - n, 0, 0)];
+    xv[i] = (i < n) ? u[sidx(g, i * nb + run, 0, 0)] : w[sidx(g, (i - n) * nb + run, 0, 0)];
   }
   __syncthreads();
   // one warp per row, lanes along the row (coalesced)
@@ -661,8 +671,9 @@ __global__ void __launch_bounds__(kMeanFlowThreads) k_mean_flow(
     }
     if (lane == 0) {
       const double src = (i < n) ? -dp : 0.0;
-      const double2 nn = make_double2(-conv[i].x + src, -conv[i].y);
-      const double2 no = conv_old ? make_double2(-conv_old[i].x + src, -conv_old[i].y) : make_double2(src, 0.0);
+      const double2 nn = make_double2(-conv[cidx(i)].x + src, -conv[cidx(i)].y);
+      const double2 no =
+          conv_old ? make_double2(-conv_old[cidx(i)].x + src, -conv_old[cidx(i)].y) : make_double2(src, 0.0);
       rv[i] = cadd(cadd(make_double2(ax, ay), cscale(nn, dt_gamma)), cscale(no, dt_xi));
     }
   }
@@ -684,21 +695,23 @@ __global__ void __launch_bounds__(kMeanFlowThreads) k_mean_flow(
 
 // u, w from continuity and omega_y (rk_not_00, navier_stokes.py:1506-1527);
 // the (0,0) mode from the mean-flow solve; walls zeroed (domain.py:630-647).
+// (g.ny = Chebyshev points, g.nb runs; uw00 holds 2 Ny entries per run)
 __global__ void k_reconstruct(Geo g, const double2* __restrict__ dvn, const double2* __restrict__ omn,
                               const double2* __restrict__ uw00, double2* __restrict__ u, double2* __restrict__ v,
                               double2* __restrict__ w) {
-  const size_t total = (size_t)g.ny * g.nk;
+  const size_t total = (size_t)g.ny * g.nb * g.nk;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
-    const int y = (int)(t / g.nk);
-    const int r = (int)(t - (size_t)y * g.nk);
+    const int plane = (int)(t / g.nk);
+    const int r = (int)(t - (size_t)plane * g.nk);
+    const int y = plane / g.nb, run = plane - y * g.nb;
     const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
     if (y == 0 || y == g.ny - 1) {
       u[t] = v[t] = w[t] = make_double2(0.0, 0.0);
       continue;
     }
     if (ix == 0 && iz == 0) {
-      u[t] = uw00[y];
-      w[t] = uw00[g.ny + y];
+      u[t] = uw00[(size_t)run * 2 * g.ny + y];
+      w[t] = uw00[(size_t)run * 2 * g.ny + g.ny + y];
       continue;
     }
     const double kx = kx_of(g, ix), kz = kz_of(g, iz);
@@ -751,6 +764,17 @@ __global__ void k_weighted_total(int ny, const double* __restrict__ weights, con
     for (int y = 0; y < ny; ++y) acc += weights[y] * partial[y];
     out[0] = scale * acc;
   }
+}
+
+// Per-run totals of a batch: out[run] = scale * sum_y w_y partial[y * nb + run]
+// (partial per plane from k_plane_sums).
+__global__ void k_weighted_total_runs(int ny, int nb, const double* __restrict__ weights,
+                                      const double* __restrict__ partial, double scale, double* __restrict__ out) {
+  const int run = blockIdx.x * blockDim.x + threadIdx.x;
+  if (run >= nb) return;
+  double acc = 0.0;
+  for (int y = 0; y < ny; ++y) acc += weights[y] * partial[(size_t)y * nb + run];
+  out[run] = scale * acc;
 }
 
 // Constant mass flux (navier_stokes.py:724-805, 1205-1214): with the flow rate

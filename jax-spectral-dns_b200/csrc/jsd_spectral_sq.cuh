@@ -330,8 +330,8 @@ __global__ void __launch_bounds__(kSqWarps * 32, xsq_min_blocks<C>()) k_xmid_sq(
   C* xb = otile + 3 * K1 * ZC + (ln.warp * G + ln.gi) * XB;
   const int z0 = blockIdx.x * ZC, y = blockIdx.y;
   const int zl = ln.warp * G + ln.gi;
-  const Rl ub = ubase ? (Rl)ubase[y] : (Rl)0;
-  const Rl dub = dubase ? (Rl)dubase[y] : (Rl)0;
+  const Rl ub = ubase ? (Rl)ubase[y / g.nb] : (Rl)0;
+  const Rl dub = dubase ? (Rl)dubase[y / g.nb] : (Rl)0;
   const Rl c = (Rl)g.c_inv, lam = (Rl)lam_d, half = (Rl)0.5;
   xsq_stage_tile<C, ZC>(g, inter, tile, kZinvLines, y, z0);
   // twiddle table w_N^e in shared memory (read by stage 1 of every transform)
@@ -424,8 +424,8 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_xmid_dual_sq(Geo g, const C* 
   C* xb = otile + 3 * K1 * ZC + (ln.warp * G + ln.gi) * XB;
   const int z0 = blockIdx.x * ZC, y = blockIdx.y;
   const int zl = ln.warp * G + ln.gi;
-  const Rl ub = (Rl)ubase[y];
-  const Rl dub = (Rl)dubase[y];
+  const Rl ub = (Rl)ubase[y / g.nb];
+  const Rl dub = (Rl)dubase[y / g.nb];
   const Rl c = (Rl)g.c_inv, q4 = (Rl)0.25;
   xsq_stage_tile<C, ZC>(g, inter, tile, 2 * kZinvLines, y, z0);
   // twiddle table w_N^e in shared memory (read by stage 1 of every transform)
@@ -563,8 +563,8 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_xmid_h2(Geo g, const C* __res
   C* stab = otile + 3 * K1 * ZC + kSqWarps * G * XB;
   const int z0 = blockIdx.x * ZC, y = blockIdx.y;
   const int zl = ln.warp * G + ln.gi;
-  const Rl ub = ubase ? (Rl)ubase[y] : (Rl)0;
-  const Rl dub = dubase ? (Rl)dubase[y] : (Rl)0;
+  const Rl ub = ubase ? (Rl)ubase[y / g.nb] : (Rl)0;
+  const Rl dub = dubase ? (Rl)dubase[y / g.nb] : (Rl)0;
   const Rl c = (Rl)g.c_inv, lam = (Rl)lam_d, half = (Rl)0.5;
   xsq_stage_tile<C, ZC>(g, inter, tile, kZinvLines, y, z0);
   for (int e = threadIdx.x; e < N; e += blockDim.x) stab[e] = twtab[e];

@@ -35,6 +35,7 @@ class JsdDesc(ctypes.Structure):
         ("c0", _dp), ("cN", _dp), ("w0", _dp), ("wN", _dp), ("y_weights", _dp),
         ("rhs_ns", _dp), ("lhs_inv_ns", _dp),
         ("precision", ctypes.c_int),
+        ("n_batch", ctypes.c_int), ("re_tau_batch", _dp),
     ]
 
 
@@ -49,7 +50,10 @@ EXPORTED = (
     "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc", "jsd_step_trajectory",
     "jsd_launches_first_step_extra", "jsd_autotune", "jsd_gemm_config",
     "jsd_set_gemm_config", "jsd_xmid_variant", "jsd_set_xmid_variant",
+    "jsd_energy_runs", "jsd_set_batch_active", "jsd_batch_active",
 )
+
+ABI_VERSION = 2  # JSD_ABI_VERSION of include/jsd.h this binding is written for
 
 # GEMM call sites of a plan (jsd_gemm_config) and the number of DMMA tile configurations
 GEMM_SITES = {"dfield": 0, "eig_in": 1, "eig_out": 2}
@@ -96,12 +100,18 @@ def load(path: str = LIB_PATH):
     lib.jsd_gemm_config.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_set_gemm_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.jsd_xmid_variant.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    lib.jsd_energy_runs.argtypes = [vp, vp, vp, vp]
+    lib.jsd_set_batch_active.argtypes = [vp, ctypes.c_int]
+    lib.jsd_batch_active.argtypes = [vp]
     lib.jsd_set_xmid_variant.argtypes = [vp, ctypes.c_int]
     lib.jsd_profile_read.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                      ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double)]
     for name in EXPORTED:
         if name not in ("jsd_workspace_bytes", "jsd_last_error"):
             getattr(lib, name).restype = ctypes.c_int
+    if lib.jsd_abi_version() != ABI_VERSION:
+        raise NativeError(f"{path} has ABI version {lib.jsd_abi_version()}, this binding needs {ABI_VERSION}; "
+                          "rebuild it")
     if path == LIB_PATH:
         _lib = lib
     return lib

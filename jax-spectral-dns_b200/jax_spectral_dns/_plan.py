@@ -33,6 +33,18 @@ def to_reference_layout(x: torch.Tensor) -> torch.Tensor:
     return x.transpose(-3, -2).contiguous()
 
 
+def pack_runs(states, device="cuda") -> torch.Tensor:
+    """Reference-layout states (3, Mx, Ny, Mz) of several runs -> the batch
+    layout (3, Ny, runs, Mx, Mz) on the device."""
+    dev = torch.stack([to_device_layout(x, device=device) for x in states])  # (runs, 3, Ny, Mx, Mz)
+    return dev.permute(1, 2, 0, 3, 4).contiguous()
+
+
+def unpack_runs(state: torch.Tensor) -> list:
+    """Batch layout (3, Ny, runs, Mx, Mz) -> list of reference-layout states."""
+    return [to_reference_layout(state[:, :, r]) for r in range(state.shape[2])]
+
+
 def _stream_ptr() -> ctypes.c_void_p:
     return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
 
@@ -50,7 +62,12 @@ class StepPlan:
         self.modes = (mx, ny, mz)
         self.device = torch.device(device)
         t = operator_tables(ny)
-        rhs_ns, lhs_inv_ns = mean_flow_matrices(ny, re_tau, dt)
+        batch = np.ndim(re_tau) > 0
+        re_runs = np.atleast_1d(np.asarray(re_tau, dtype=np.float64))
+        self.n_batch = len(re_runs) if batch else 1
+        mats = [mean_flow_matrices(ny, float(r), dt) for r in re_runs]
+        rhs_ns = np.concatenate([m[0] for m in mats])
+        lhs_inv_ns = np.concatenate([m[1] for m in mats])
         self._keep = []
 
         def arr(a):
@@ -68,7 +85,10 @@ class StepPlan:
         d.kind = int(kind)
         d.linearise = int(bool(linearise))
         d.constant_mass_flux = int(bool(constant_mass_flux))
-        d.re_tau = float(re_tau)
+        d.re_tau = float(re_runs[0])
+        if batch:
+            d.n_batch = self.n_batch
+            d.re_tau_batch = arr(re_runs)
         d.dt = float(dt)
         d.dt_explicit = float(dt if dt_explicit is None else dt_explicit)
         d.flow_rate_target = float(flow_rate_target)
@@ -182,6 +202,19 @@ class StepPlan:
         _native.check(self.lib.jsd_energy(self.handle, ctypes.c_void_p(state.data_ptr()),
                                           ctypes.c_void_p(out.data_ptr()), _stream_ptr()), "jsd_energy")
         return out
+
+    def energy_runs(self, state: torch.Tensor) -> torch.Tensor:
+        """Energies of the active runs of a batch plan (device tensor)."""
+        out = torch.empty(self.batch_active(), dtype=torch.float64, device=state.device)
+        _native.check(self.lib.jsd_energy_runs(self.handle, ctypes.c_void_p(state.data_ptr()),
+                                               ctypes.c_void_p(out.data_ptr()), _stream_ptr()), "jsd_energy_runs")
+        return out
+
+    def set_batch_active(self, n_runs: int) -> None:
+        _native.check(self.lib.jsd_set_batch_active(self.handle, int(n_runs)), "jsd_set_batch_active")
+
+    def batch_active(self) -> int:
+        return int(self.lib.jsd_batch_active(self.handle))
 
     def flow_rate(self, u_field: torch.Tensor) -> torch.Tensor:
         out = torch.empty(1, dtype=torch.float64, device=u_field.device)

@@ -134,3 +134,121 @@ class Ensemble:
 
     def energies(self) -> np.ndarray:
         return np.array([p.energy(st).item() for p, st in zip(self.plans, self.states)])
+
+
+class BatchedEnsemble:
+    """The same ensemble with every group of runs that share a box stepped as
+    one batch plan: one set of launches per RK stage advances all runs of the
+    group (each y-operator is a single product over the group, the transform
+    kernels see one plane per (y, run), Re enters per run).
+
+    Runs of a group are ordered by horizon, longest first. The group steps in
+    phases between successive horizons; at the end of a phase the runs that
+    reached their horizon (the tail of the order) are copied out and the batch
+    shrinks (jsd_set_batch_active), so no run steps past its horizon. Each
+    phase replays CUDA graphs of up to `chunk` steps; groups are spread over a
+    pool of streams.
+    """
+
+    def __init__(self, specs: List[RunSpec], streams: int = 4, chunk: int = 100, precision: str = "fp64",
+                 device: str = "cuda"):
+        from ._plan import pack_runs
+
+        self.specs = specs
+        self.device = torch.device(device)
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(max(1, streams))]
+        keys = {}
+        for i, s in enumerate(specs):
+            keys.setdefault((s.n, s.ny, s.lx, s.lz, s.dt, s.linearise), []).append(i)
+        self.groups = []
+        for (n, ny, lx, lz, dt, lin), idx in keys.items():
+            idx = sorted(idx, key=lambda i: (-specs[i].steps, i))
+            shape = (n, ny, n)
+            modes, phys = mode_counts(shape)
+            kmax = (min(8, modes[0] // 2), min(8, modes[2] // 2))
+            plan = StepPlan(modes, phys, lx, lz, _native.JSD_KIND_PERTURBATION, [specs[i].re for i in idx], dt,
+                            linearise=lin, base_u=1 - cheb_points(modes[1]) ** 2, precision=precision,
+                            device=device)
+            init = pack_runs([seeded_velocity_hat(shape, (lx, lz), kmax, specs[i].e0, specs[i].seed) for i in idx],
+                             device=self.device)
+            buf = init.clone().reshape(-1)
+            dp = torch.zeros(1, dtype=torch.float64, device=self.device)
+            mx, _, mz = modes
+            # phases: (active runs, steps in the phase, graphs)
+            steps = [specs[i].steps for i in idx]
+            phases, done = [], 0
+            bounds = sorted(set(steps))
+            for b in bounds:
+                active = sum(1 for st in steps if st >= b)
+                phases.append([active, b - done, []])
+                done = b
+            for ph in phases:
+                active, n_steps, graphs = ph
+                if n_steps <= 0:
+                    continue
+                plan.set_batch_active(active)
+                view = buf[: 3 * ny * active * mx * mz].view(3, ny, active, mx, mz)
+                full, rem = divmod(n_steps, chunk)
+                if full:
+                    graphs.append((GraphedSteps(plan, view, dp, 0, chunk), full))
+                if rem:
+                    graphs.append((GraphedSteps(plan, view, dp, 0, rem), 1))
+            self.groups.append({"idx": idx, "plan": plan, "init": init, "buf": buf, "dp": dp, "phases": phases,
+                                "dims": (ny, mx, mz), "final": torch.zeros_like(init)})
+        torch.cuda.synchronize(self.device)
+
+    @property
+    def total_steps(self) -> int:
+        return sum(s.steps for s in self.specs)
+
+    def reset(self) -> None:
+        for g in self.groups:
+            g["buf"].copy_(g["init"].reshape(-1))
+            g["dp"].zero_()
+            g["final"].zero_()
+        torch.cuda.synchronize(self.device)
+
+    def _run_group(self, g) -> None:
+        ny, mx, mz = g["dims"]
+        buf, phases = g["buf"], g["phases"]
+        for k, (active, n_steps, graphs) in enumerate(phases):
+            for graph, reps in graphs:
+                for _ in range(reps):
+                    graph.replay()
+            view = buf[: 3 * ny * active * mx * mz].view(3, ny, active, mx, mz)
+            nxt = phases[k + 1][0] if k + 1 < len(phases) else 0
+            # runs nxt .. active-1 reached their horizon: keep their states
+            g["final"][:, :, nxt:active].copy_(view[:, :, nxt:active])
+            if nxt:
+                keep = view[:, :, :nxt].clone()
+                buf[: 3 * ny * nxt * mx * mz].view(3, ny, nxt, mx, mz).copy_(keep)
+
+    def run(self) -> float:
+        """All runs to their horizons; returns the elapsed device time in ms."""
+        main = torch.cuda.current_stream(self.device)
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(main)
+        for s in self.streams:
+            s.wait_event(start)
+        order = sorted(range(len(self.groups)),
+                       key=lambda k: -sum(self.specs[i].steps for i in self.groups[k]["idx"]) *
+                       self.groups[k]["dims"][0] * self.groups[k]["dims"][1] ** 2)
+        for j, k in enumerate(order):
+            with torch.cuda.stream(self.streams[j % len(self.streams)]):
+                self._run_group(self.groups[k])
+        for s in self.streams:
+            main.wait_stream(s)
+        stop.record(main)
+        torch.cuda.synchronize(self.device)
+        return start.elapsed_time(stop)
+
+    def energies(self) -> np.ndarray:
+        """Kinetic energy of every run at its horizon, in the order of `specs`."""
+        out = np.zeros(len(self.specs))
+        for g in self.groups:
+            plan = g["plan"]
+            plan.set_batch_active(len(g["idx"]))
+            e = plan.energy_runs(g["final"]).cpu().numpy()
+            for pos, i in enumerate(g["idx"]):
+                out[i] = e[pos]
+        return out

@@ -44,7 +44,7 @@ def test_binding_covers_header(lib):
 
 
 def test_abi_version_and_error_strings(lib):
-    assert lib.jsd_abi_version() == 1
+    assert lib.jsd_abi_version() == 2
     assert isinstance(lib.jsd_last_error(), bytes)
 
 
