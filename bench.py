@@ -51,7 +51,8 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-KERNEL_NAMES = {"gemm": "k_dgemm", "sgemm": "k_sgemm3", "zinv": "k_zinv", "xmid": "k_xmid", "zfwd": "k_zfwd",
+# kernel class -> summary file stem under profiles/ (<stem>_channel_128x129x128.md)
+KERNEL_NAMES = {"gemm": "k_dgemm", "sgemm": "k_sgemm3", "zinv": "k_zinv_sq", "xmid": "k_xmid", "zfwd": "k_zfwd_sq",
                 "eigen": "k_eigen_update"}
 
 

@@ -1038,6 +1038,12 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   p->sqx = square_side(g.px);
   p->sqz = square_side(g.pz);
   p->xmid_variant = default_xmid_variant(p);
+  // default tiles before any autotuning: the two-stage 48- or 64-row tile that
+  // pads the call site's row count least (configurations 0 and 1)
+  for (int site = 0; site < kGemmSites; ++site) {
+    const int m = site == kSiteEigIn ? ny - 2 : ny;
+    p->gemm_cfg[site] = ((m + 47) / 48 * 48 < (m + 63) / 64 * 64) ? 0 : 1;
+  }
   for (int axis = 0; axis < 2; ++axis) {
     const int n = axis == 0 ? g.px : g.pz;
     if (!(axis == 0 ? p->sqx : p->sqz)) continue;
