@@ -330,6 +330,8 @@ def run_ours(args):
         forms_out = {pr: {"steps_per_s": world * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
                           "energy_after": r["energy"],
                           "gemm_configs": {site: cfg for site, (cfg, _) in plans[pr].gemm_configs().items()},
+                          "split_kernel": plans[pr].split_kernel()[0],
+                          "split_kernel_ms": plans[pr].split_kernel()[1],
                           "xmid_variant": plans[pr].xmid_variant()[0],
                           "xmid_variant_ms": plans[pr].xmid_variant()[1]}
                      for pr, r in results.items()}

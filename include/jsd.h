@@ -207,6 +207,18 @@ int jsd_xmid_variant(const jsd_plan* plan, float* times_ms);
  * plan's FFT length, precision or equation). No counterpart in the reference. */
 int jsd_set_xmid_variant(jsd_plan* plan, int variant);
 
+/* Split-TF32 y-derivative kernel of a mixed-precision plan: 0 mma.sync
+ * (k_sgemm3), 1 tcgen05 with the accumulator in tensor memory
+ * (k_tc05_dfield, Ny <= 129); -1 for FP64 plans. times_ms (2 floats, may be
+ * null) receives the autotuner's timings. No counterpart in the reference. */
+int jsd_split_kernel(const jsd_plan* plan, float* times_ms);
+int jsd_set_split_kernel(jsd_plan* plan, int kernel);
+
+/* JSD_ERR_CUDA (and clears the flag) when a kernel of the plan gave up a
+ * bounded wait since the last check (its results are then invalid);
+ * synchronises the stream. No counterpart in the reference. */
+int jsd_device_error(jsd_plan* plan, void* stream);
+
 /* Number of kernel launches one call of jsd_step issues per time step after
  * its first; the first step of each call issues jsd_launches_first_step_extra
  * more (it derives omega_y, and dv/dy for linearised plans, from the caller's

@@ -29,6 +29,7 @@
 #include "jsd_gemm.cuh"
 #include "jsd_spectral.cuh"
 #include "jsd_spectral_sq.cuh"
+#include "jsd_tc05.cuh"
 
 using namespace jsd;
 
@@ -159,6 +160,15 @@ struct jsd_plan {
   double2 *twx = nullptr, *twz = nullptr;
   float2 *twx32 = nullptr, *twz32 = nullptr;
   int nb_max = 1;               // runs the workspace is sized for (g.nb = runs stepped now)
+  // tcgen05 split-TF32 y-derivatives (mixed form, Ny <= 129): rows computed
+  // (min(Ny, 128); for Ny = 129 the y = -1 wall row is left out, which only
+  // steady-state stages may do), packed D parts, kernel choice, error flag
+  int tc_rows = 0;
+  float *tc_ahi = nullptr, *tc_alo = nullptr;
+  int split_kernel = 0;         // 0: k_sgemm3 (mma.sync), 1: k_tc05_dfield (tcgen05)
+  int* errflag = nullptr;       // set by kernels whose bounded waits expired
+  int num_sms = 148;
+  float split_ms[2] = {};       // autotuner timings of the two split kernels
   double* re_run = nullptr;     // Reynolds number per run of a batch (device)
   int gemm_cfg[3] = {2, 2, 2};  // DMMA tile configuration per call site (GemmSite)
   int xmid_variant = 2;         // x-pass kernel (launch_xmid), set at creation, autotuned on request
@@ -281,13 +291,39 @@ void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M,
 
 // y-derivatives D * f of up to kGemmMaxBatch fields: FP64 DMMA, or 3xTF32 in
 // the mixed-precision mode
-int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
+// Split-TF32 y-derivatives on tcgen05 (rows 0 .. tc_rows-1 of D).
+int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
+  Tc05Batch b;
+  memset(&b, 0, sizeof(b));
+  b.N = 2 * p->g.nk * p->g.nb;
+  b.M = p->tc_rows;
+  b.K = p->g.ny;
+  b.ldb = b.ldc = b.N;
+  for (int i = 0; i < count; ++i) {
+    b.B[b.count] = src[i];
+    b.C[b.count++] = dst[i];
+  }
+  const int tiles = (b.N + kTcN - 1) / kTcN * b.count;
+  ProfScope ps(p, JSD_PROF_SGEMM, 2.0 * b.M * (double)b.K * b.N * count, s);
+  k_tc05_dfield<<<tiles < p->num_sms ? tiles : p->num_sms, 128, kTcSmem, s>>>(p->tc_ahi, p->tc_alo, b, p->errflag);
+  JSD_LAUNCHED("k_tc05_dfield");
+  return 0;
+}
+
+// y-derivatives D * f of up to kGemmMaxBatch fields: FP64 DMMA, or 3xTF32 in
+// the mixed-precision mode (mma.sync, or tcgen05 when the plan chose it and
+// the call allows its rows: all rows for Ny <= 128; for Ny = 129 only calls
+// whose wall-row derivatives are never used, `walls_free`)
+int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s,
+                  bool walls_free = false, int force_split = -1) {
   const int ny = p->g.ny;
   if (!p->mixed) {
     GemmBatch b = gemm_batch(p);
     for (int i = 0; i < count; ++i) add_entry(b, p->Dm, src[i], dst[i], ny, ny, 1.0);
     return launch_gemm(p, b, ny, kSiteDfield, s);
   }
+  const int kernel = force_split >= 0 ? force_split : p->split_kernel;
+  if (kernel == 1 && p->tc_rows && (p->tc_rows == ny || walls_free)) return launch_tc05(p, src, dst, count, s);
   SplitGemmBatch b;
   memset(&b, 0, sizeof(b));
   b.N = 2 * p->g.nk * p->g.nb;
@@ -412,7 +448,10 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
         src[cnt] = (const double*)(uhist + c * fs);
         dst[cnt++] = (double*)(p->Dfld + (3 + c) * fs);
       }
-    int rc = launch_dfield(p, src, dst, cnt, s);
+    // after the first stage of a call the state comes out of k_reconstruct,
+    // which zeroes u, v, w on the wall rows: every product that multiplies a
+    // wall-row derivative of u or w then vanishes (dv/dy is carried in dvn)
+    int rc = launch_dfield(p, src, dst, cnt, s, p->dv_valid && !dual);
     if (rc) return rc;
   }
   return p->mixed ? transforms<float2>(p, state, uhist, conv, s) : transforms<double2>(p, state, uhist, conv, s);
@@ -665,6 +704,7 @@ int set_smem_limits() {
     JSD_CUDA(e);
   }
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_tc05_dfield, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
   cudaError_t err = cudaSuccess;
   for (int sd : kSquareSides)
     with_square_side(sd, [&](auto side) {
@@ -858,6 +898,30 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
       }
     }
   }
+  // split-TF32 y-derivative kernels (mixed plans): the steady-state call on u and w
+  if (rc == 0 && plan->mixed && plan->tc_rows) {
+    const double* src[2] = {(const double*)plan->q, (const double*)plan->H1};
+    double* dst[2] = {(double*)plan->Dfld, (double*)(plan->Dfld + 2 * fs)};
+    float best = 3.0e38f;
+    for (int k = 0; k < 2 && rc == 0; ++k) {
+      rc = launch_dfield(plan, src, dst, 2, s, true, k);  // warm-up
+      if (rc) break;
+      if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(JSD_ERR_CUDA, "cudaEventRecord");
+      for (int r = 0; r < 5 && rc == 0; ++r) rc = launch_dfield(plan, src, dst, 2, s, true, k);
+      if (rc) break;
+      float ms = 0.f;
+      if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+          cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        rc = fail(JSD_ERR_CUDA, "autotune timing");
+        break;
+      }
+      plan->split_ms[k] = ms / 5.f;
+      if (ms < best) {
+        best = ms;
+        plan->split_kernel = k;
+      }
+    }
+  }
   // x-pass kernel variants (nonlinear plans)
   const bool linear = plan->desc.linearise && plan->desc.kind != JSD_KIND_NS;
   if (rc == 0 && !linear) {
@@ -889,6 +953,34 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   return rc;
+}
+
+int jsd_split_kernel(const jsd_plan* plan, float* times_ms) {
+  if (!plan) return -1;
+  if (times_ms)
+    for (int k = 0; k < 2; ++k) times_ms[k] = plan->split_ms[k];
+  return plan->mixed ? plan->split_kernel : -1;
+}
+
+int jsd_set_split_kernel(jsd_plan* plan, int kernel) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  if (!plan->mixed || kernel < 0 || kernel > 1 || (kernel == 1 && !plan->tc_rows))
+    return fail(JSD_ERR_ARG, "split-TF32 kernel not available for this plan");
+  plan->split_kernel = kernel;
+  return 0;
+}
+
+int jsd_device_error(jsd_plan* plan, void* stream) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  int h = 0;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  JSD_CUDA(cudaMemcpyAsync(&h, plan->errflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+  JSD_CUDA(cudaStreamSynchronize(s));
+  if (h) {
+    JSD_CUDA(cudaMemsetAsync(plan->errflag, 0, sizeof(int), s));
+    return fail(JSD_ERR_CUDA, "a kernel's bounded wait expired (tcgen05 accumulator or bulk copy did not complete)");
+  }
+  return 0;
 }
 
 int jsd_xmid_variant(const jsd_plan* plan, float* times_ms) {
@@ -1074,6 +1166,22 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
       }
     JSD_TRY(upload(p, &p->Dhi, hi.data(), hi.size()));
     JSD_TRY(upload(p, &p->Dlo, lo.data(), lo.size()));
+    if (ny <= kTcM + 1) {
+      p->tc_rows = ny < kTcM ? ny : kTcM;
+      std::vector<float> ahi, alo;
+      tc05_pack_a(d->D, p->tc_rows, ny, ny, tf32_round, ahi, alo);
+      JSD_TRY(upload(p, &p->tc_ahi, ahi.data(), ahi.size()));
+      JSD_TRY(upload(p, &p->tc_alo, alo.data(), alo.size()));
+      p->split_kernel = 1;
+    }
+  }
+  JSD_TRY(dev_alloc(p, (void**)&p->errflag, sizeof(int)));
+  JSD_CUDA(cudaMemset(p->errflag, 0, sizeof(int)));
+  {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+      p->num_sms = sms;
   }
   JSD_TRY(upload_padded(p, &p->Dm, d->D, ny, ny, p->lda));
   JSD_TRY(upload_padded(p, &p->VinvD, VinvD.data(), ni, ny, p->lda));

@@ -51,6 +51,7 @@ EXPORTED = (
     "jsd_launches_first_step_extra", "jsd_autotune", "jsd_gemm_config",
     "jsd_set_gemm_config", "jsd_xmid_variant", "jsd_set_xmid_variant",
     "jsd_energy_runs", "jsd_set_batch_active", "jsd_batch_active",
+    "jsd_split_kernel", "jsd_set_split_kernel", "jsd_device_error",
 )
 
 ABI_VERSION = 2  # JSD_ABI_VERSION of include/jsd.h this binding is written for
@@ -101,6 +102,9 @@ def load(path: str = LIB_PATH):
     lib.jsd_set_gemm_config.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.jsd_xmid_variant.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_energy_runs.argtypes = [vp, vp, vp, vp]
+    lib.jsd_split_kernel.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    lib.jsd_set_split_kernel.argtypes = [vp, ctypes.c_int]
+    lib.jsd_device_error.argtypes = [vp, vp]
     lib.jsd_set_batch_active.argtypes = [vp, ctypes.c_int]
     lib.jsd_batch_active.argtypes = [vp]
     lib.jsd_set_xmid_variant.argtypes = [vp, ctypes.c_int]

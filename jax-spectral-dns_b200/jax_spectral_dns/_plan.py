@@ -149,6 +149,20 @@ class StepPlan:
     def set_xmid_variant(self, variant: int) -> None:
         _native.check(self.lib.jsd_set_xmid_variant(self.handle, int(variant)), "jsd_set_xmid_variant")
 
+    def split_kernel(self):
+        """(split-TF32 y-derivative kernel in use: 0 mma.sync, 1 tcgen05, -1 FP64 plan;
+        [autotune ms of both])."""
+        times = (ctypes.c_float * 2)()
+        k = int(self.lib.jsd_split_kernel(self.handle, times))
+        return k, [float(t) for t in times]
+
+    def set_split_kernel(self, kernel: int) -> None:
+        _native.check(self.lib.jsd_set_split_kernel(self.handle, int(kernel)), "jsd_set_split_kernel")
+
+    def check_device_errors(self) -> None:
+        """Raise when a kernel of this plan gave up a bounded wait."""
+        _native.check(self.lib.jsd_device_error(self.handle, _stream_ptr()), "jsd_device_error")
+
     def gemm_configs(self) -> dict:
         """{site: (configuration id, [per-configuration autotune ms])}."""
         out = {}
