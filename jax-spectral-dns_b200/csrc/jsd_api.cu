@@ -13,6 +13,7 @@
 // and, with constant mass flux, 3 more launches and one copy per step.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -170,6 +171,7 @@ struct jsd_plan {
   int num_sms = 148;
   float split_ms[2] = {};       // autotuner timings of the two split kernels
   double* re_run = nullptr;     // Reynolds number per run of a batch (device)
+  double* lr_ns = nullptr;      // Linv_ns R_ns per run and stage (row-parallel mean-flow update)
   int gemm_cfg[3] = {2, 2, 2};  // DMMA tile configuration per call site (GemmSite)
   int xmid_variant = 2;         // x-pass kernel (launch_xmid), set at creation, autotuned on request
   float xmid_ms[3] = {};        // autotuner timings of the x-pass variants (0: not timed)
@@ -647,10 +649,13 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     const double2* conv = p->conv + (size_t)st * 2 * gp.ny;
     const double2* conv_old = st == 0 ? nullptr : p->conv + (size_t)(st - 1) * 2 * gp.ny;
     const double dte = p->desc.dt_explicit;
-    // per-run matrices: rns / lns point at run 0's stage-st matrices, the kernel offsets by run
-    k_mean_flow<<<g.nb, kMeanFlowThreads, sizeof(double2) * 2 * n2, s>>>(g, rns, lns, u, w, conv, conv_old, dpdx, p->dpdx_scale,
-                                                        dte * kGamma[st], dte * kXi[st], p->uw00);
-    JSD_LAUNCHED("k_mean_flow");
+    // per-run matrices: lr / lns point at run 0's stage-st matrices, the kernel offsets by run
+    (void)rns;
+    const double* lr = p->lr_ns + (size_t)st * n2 * n2;
+    const dim3 grid((unsigned)((n2 + kMeanFlowRows - 1) / kMeanFlowRows), (unsigned)g.nb);
+    k_mean_flow_rows<<<grid, 32 * kMeanFlowRows, sizeof(double2) * 2 * n2, s>>>(
+        g, lr, lns, u, w, conv, conv_old, dpdx, p->dpdx_scale, dte * kGamma[st], dte * kXi[st], p->uw00);
+    JSD_LAUNCHED("k_mean_flow_rows");
   }
   {
     GemmBatch b = gemm_batch(p);
@@ -670,11 +675,11 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
 int mass_flux(jsd_plan* p, double2* state, double* dpdx, cudaStream_t s) {
   const Geo& g = p->g;
   const size_t fs = (size_t)g.ny * g.nk;
-  k_plane_sums<<<g.ny, 256, 0, s>>>(g, state, 1, 1, p->partial);
-  JSD_LAUNCHED("k_plane_sums");
-  k_mass_flux_scalar<<<1, 32, 0, s>>>(g.ny, p->yw, p->partial, g.c_inv, p->desc.flow_rate_target,
-                                      p->desc.dt_explicit, dpdx, p->scal);
-  JSD_LAUNCHED("k_mass_flux_scalar");
+  k_plane_sums_sliced<<<dim3(g.ny, kSumSlices), 256, 0, s>>>(g, state, 1, 1, p->partial);
+  JSD_LAUNCHED("k_plane_sums_sliced");
+  k_mass_flux_scalar_sliced<<<1, 32, 0, s>>>(g.ny, p->yw, p->partial, g.c_inv, p->desc.flow_rate_target,
+                                             p->desc.dt_explicit, dpdx, p->scal);
+  JSD_LAUNCHED("k_mass_flux_scalar_sliced");
   k_roundtrip_shift<<<grid_for(fs, 256), 256, 0, s>>>(g, state, p->scal, p->tmp);
   JSD_LAUNCHED("k_roundtrip_shift");
   JSD_CUDA(cudaMemcpyAsync(state, p->tmp, fs * sizeof(double2), cudaMemcpyDeviceToDevice, s));
@@ -704,6 +709,7 @@ int set_smem_limits() {
     JSD_CUDA(e);
   }
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_mean_flow_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_tc05_dfield, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
   cudaError_t err = cudaSuccess;
   for (int sd : kSquareSides)
@@ -1198,6 +1204,27 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(upload(p, &p->rhs_ns, d->rhs_ns, (size_t)nb * 3 * n2 * n2));
   JSD_TRY(upload(p, &p->lhs_inv_ns, d->lhs_inv_ns, (size_t)nb * 3 * n2 * n2));
   if (nb > 1) JSD_TRY(upload(p, &p->re_run, d->re_tau_batch, (size_t)nb));
+  {
+    // LR = Linv_ns R_ns for every run and stage (the matrices are block
+    // structured, so zero entries of Linv are skipped)
+    std::vector<double> lr((size_t)nb * 3 * n2 * n2);
+    for (size_t m = 0; m < (size_t)nb * 3; ++m) {
+      const double* L = d->lhs_inv_ns + m * n2 * n2;
+      const double* R = d->rhs_ns + m * n2 * n2;
+      double* O = lr.data() + m * n2 * n2;
+      for (size_t i = 0; i < n2; ++i) {
+        double* row = O + i * n2;
+        std::fill(row, row + n2, 0.0);
+        for (size_t k = 0; k < n2; ++k) {
+          const double lik = L[i * n2 + k];
+          if (lik == 0.0) continue;
+          const double* rk = R + k * n2;
+          for (size_t j = 0; j < n2; ++j) row[j] += lik * rk[j];
+        }
+      }
+    }
+    JSD_TRY(upload(p, &p->lr_ns, lr.data(), lr.size()));
+  }
   if (d->base_u) JSD_TRY(upload(p, &p->ub, d->base_u, ny));
   if (d->base_du) JSD_TRY(upload(p, &p->dub, d->base_du, ny));
 
@@ -1218,7 +1245,7 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(dev_alloc(p, (void**)&p->T, 4 * p->edoubles * sizeof(double)));
   for (double** f : {&p->hv_old, &p->hg_old, &p->vnt, &p->omnt, &p->vnt_alt, &p->omnt_alt})
     JSD_TRY(dev_alloc(p, (void**)f, p->edoubles * sizeof(double)));
-  JSD_TRY(dev_alloc(p, (void**)&p->partial, (size_t)ny * nb * sizeof(double)));
+  JSD_TRY(dev_alloc(p, (void**)&p->partial, (size_t)ny * nb * kSumSlices * sizeof(double)));
   JSD_TRY(dev_alloc(p, (void**)&p->scal, 8 * sizeof(double)));
   // conv entries are only written at (0,0); clear once so every read is defined
   JSD_CUDA(cudaMemset(p->conv, 0, 3 * n2 * nb * sizeof(double2)));
@@ -1290,10 +1317,11 @@ int jsd_energy(jsd_plan* plan, const void* state, double* out, void* stream) {
   if (plan->g.nb > 1) return fail(JSD_ERR_ARG, "single-run entry point called on a batch plan (see jsd_energy_runs)");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Geo& g = plan->g;
-  k_plane_sums<<<g.ny, 256, 0, s>>>(g, static_cast<const double2*>(state), 3, 0, plan->partial);
-  JSD_LAUNCHED("k_plane_sums");
-  k_weighted_total<<<1, 32, 0, s>>>(g.ny, plan->yw, plan->partial, 0.25 * g.c_inv * g.c_inv, out);
-  JSD_LAUNCHED("k_weighted_total");
+  k_plane_sums_sliced<<<dim3(g.ny, kSumSlices), 256, 0, s>>>(g, static_cast<const double2*>(state), 3, 0,
+                                                              plan->partial);
+  JSD_LAUNCHED("k_plane_sums_sliced");
+  k_weighted_total_sliced<<<1, 32, 0, s>>>(g.ny, plan->yw, plan->partial, 0.25 * g.c_inv * g.c_inv, out);
+  JSD_LAUNCHED("k_weighted_total_sliced");
   return 0;
 }
 
@@ -1302,11 +1330,12 @@ int jsd_energy_runs(jsd_plan* plan, const void* state, double* out, void* stream
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Geo& g = plan->g;
   const Geo gp = planes_of(g);
-  k_plane_sums<<<gp.ny, 256, 0, s>>>(gp, static_cast<const double2*>(state), 3, 0, plan->partial);
-  JSD_LAUNCHED("k_plane_sums");
-  k_weighted_total_runs<<<(g.nb + 127) / 128, 128, 0, s>>>(g.ny, g.nb, plan->yw, plan->partial,
-                                                           0.25 * g.c_inv * g.c_inv, out);
-  JSD_LAUNCHED("k_weighted_total_runs");
+  k_plane_sums_sliced<<<dim3(gp.ny, kSumSlices), 256, 0, s>>>(gp, static_cast<const double2*>(state), 3, 0,
+                                                               plan->partial);
+  JSD_LAUNCHED("k_plane_sums_sliced");
+  k_weighted_total_runs_sliced<<<g.nb, 32, 0, s>>>(g.ny, g.nb, plan->yw, plan->partial, 0.25 * g.c_inv * g.c_inv,
+                                                    out);
+  JSD_LAUNCHED("k_weighted_total_runs_sliced");
   return 0;
 }
 
@@ -1325,10 +1354,11 @@ int jsd_flow_rate(jsd_plan* plan, const void* u_field, double* out, void* stream
   if (plan->g.nb > 1) return fail(JSD_ERR_ARG, "single-run entry point called on a batch plan (see jsd_energy_runs)");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const Geo& g = plan->g;
-  k_plane_sums<<<g.ny, 256, 0, s>>>(g, static_cast<const double2*>(u_field), 1, 1, plan->partial);
-  JSD_LAUNCHED("k_plane_sums");
-  k_weighted_total<<<1, 32, 0, s>>>(g.ny, plan->yw, plan->partial, g.c_inv, out);
-  JSD_LAUNCHED("k_weighted_total");
+  k_plane_sums_sliced<<<dim3(g.ny, kSumSlices), 256, 0, s>>>(g, static_cast<const double2*>(u_field), 1, 1,
+                                                              plan->partial);
+  JSD_LAUNCHED("k_plane_sums_sliced");
+  k_weighted_total_sliced<<<1, 32, 0, s>>>(g.ny, plan->yw, plan->partial, g.c_inv, out);
+  JSD_LAUNCHED("k_weighted_total_sliced");
   return 0;
 }
 

@@ -693,6 +693,51 @@ __global__ void __launch_bounds__(kMeanFlowThreads) k_mean_flow(
   }
 }
 
+// Row-parallel form of the same update with LR = Linv_ns R_ns precomputed per
+// stage: x_new = LR x + Linv_ns (dt_e gamma N + dt_e xi N_old). Grid (row
+// blocks, runs), one warp per output row; every block first builds x and the
+// forcing f = dt_e gamma N + dt_e xi N_old of its run in shared memory.
+constexpr int kMeanFlowRows = 8;  // rows (warps) per block
+
+__global__ void __launch_bounds__(32 * kMeanFlowRows) k_mean_flow_rows(
+    Geo g, const double* __restrict__ lr_ns, const double* __restrict__ lhs_inv_ns, const double2* __restrict__ u,
+    const double2* __restrict__ w, const double2* __restrict__ conv, const double2* __restrict__ conv_old,
+    const double* __restrict__ dpdx, double dpdx_scale, double dt_gamma, double dt_xi, double2* __restrict__ uw00) {
+  extern __shared__ __align__(16) double2 msm[];
+  const int n = g.ny, n2 = 2 * g.ny;
+  const int run = blockIdx.y, nb = g.nb;
+  lr_ns += (size_t)run * 3 * n2 * n2;
+  lhs_inv_ns += (size_t)run * 3 * n2 * n2;
+  uw00 += (size_t)run * n2;
+  double2* xv = msm;      // (U00, W00) of the run
+  double2* fv = xv + n2;  // forcing
+  const double dp = dpdx ? dpdx[0] * dpdx_scale : 0.0;
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+    const int ci = (i < n) ? i * nb + run : n * nb + (i - n) * nb + run;
+    xv[i] = (i < n) ? u[sidx(g, i * nb + run, 0, 0)] : w[sidx(g, (i - n) * nb + run, 0, 0)];
+    const double src = (i < n) ? -dp : 0.0;
+    const double2 nn = make_double2(-conv[ci].x + src, -conv[ci].y);
+    const double2 no = conv_old ? make_double2(-conv_old[ci].x + src, -conv_old[ci].y) : make_double2(src, 0.0);
+    fv[i] = cadd(cscale(nn, dt_gamma), cscale(no, dt_xi));
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int i = blockIdx.x * kMeanFlowRows + (threadIdx.x >> 5);
+  if (i >= n2) return;
+  const double* lr = lr_ns + (size_t)i * n2;
+  const double* li = lhs_inv_ns + (size_t)i * n2;
+  double ax = 0.0, ay = 0.0;
+  for (int j = lane; j < n2; j += 32) {
+    ax += lr[j] * xv[j].x + li[j] * fv[j].x;
+    ay += lr[j] * xv[j].y + li[j] * fv[j].y;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ax += __shfl_down_sync(0xffffffffu, ax, o);
+    ay += __shfl_down_sync(0xffffffffu, ay, o);
+  }
+  if (lane == 0) uw00[i] = make_double2(ax, ay);
+}
+
 // u, w from continuity and omega_y (rk_not_00, navier_stokes.py:1506-1527);
 // the (0,0) mode from the mean-flow solve; walls zeroed (domain.py:630-647).
 // (g.ny = Chebyshev points, g.nb runs; uw00 holds 2 Ny entries per run)
@@ -763,6 +808,85 @@ __global__ void k_weighted_total(int ny, const double* __restrict__ weights, con
     double acc = 0.0;
     for (int y = 0; y < ny; ++y) acc += weights[y] * partial[y];
     out[0] = scale * acc;
+  }
+}
+
+// Sliced form for the plan's reductions: block (plane, slice) sums one of
+// kSumSlices contiguous slices of the plane's modes; out[plane * kSumSlices +
+// slice]. Same terms as k_plane_sums, summed in a fixed order.
+constexpr int kSumSlices = 8;
+
+__global__ void __launch_bounds__(256) k_plane_sums_sliced(Geo g, const double2* __restrict__ f, int ncomp, int mode,
+                                                          double* __restrict__ out) {
+  const int y = blockIdx.x, slice = blockIdx.y;
+  const int chunk = (g.nk + kSumSlices - 1) / kSumSlices;
+  const int r0 = slice * chunk, r1 = min(g.nk, r0 + chunk);
+  const size_t fs = (size_t)g.ny * g.nk;
+  double acc = 0.0;
+  if (mode == 0) {
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+      const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+      for (int c = 0; c < ncomp; ++c) {
+        const double2 sv = sym_at(g, f + c * fs, y, signed_mode(ix, g.mx), signed_mode(iz, g.mz));
+        acc += sv.x * sv.x + sv.y * sv.y;
+      }
+    }
+  } else {
+    const double2* row = f + (size_t)y * g.nk;
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x) acc += row[r].x;
+  }
+  __shared__ double red[8];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double a = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (threadIdx.x == 0) out[(size_t)y * kSumSlices + slice] = a;
+  }
+}
+
+// One warp: sum_y w_y sum_s partial[(y * stride + offset) * kSumSlices + s], fixed order
+__device__ __forceinline__ double weighted_slices(int ny, int stride, int offset, const double* __restrict__ weights,
+                                                  const double* __restrict__ partial) {
+  const int lane = threadIdx.x & 31;
+  double acc = 0.0;
+  for (int y = lane; y < ny; y += 32) {
+    const double* p = partial + ((size_t)y * stride + offset) * kSumSlices;
+    double sy = 0.0;
+#pragma unroll
+    for (int sl = 0; sl < kSumSlices; ++sl) sy += p[sl];
+    acc += weights[y] * sy;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  return acc;  // valid in lane 0
+}
+
+// out = scale * sum over planes (single run), one warp
+__global__ void k_weighted_total_sliced(int ny, const double* __restrict__ weights,
+                                        const double* __restrict__ partial, double scale, double* __restrict__ out) {
+  const double a = weighted_slices(ny, 1, 0, weights, partial);
+  if (threadIdx.x == 0) out[0] = scale * a;
+}
+
+// per-run totals of a batch: one warp per run
+__global__ void k_weighted_total_runs_sliced(int ny, int nb, const double* __restrict__ weights,
+                                             const double* __restrict__ partial, double scale,
+                                             double* __restrict__ out) {
+  const int run = blockIdx.x;
+  const double a = weighted_slices(ny, nb, run, weights, partial);
+  if (threadIdx.x == 0) out[run] = scale * a;
+}
+
+// mass-flux scalar from sliced partial sums of Re u, one warp
+__global__ void k_mass_flux_scalar_sliced(int ny, const double* __restrict__ weights,
+                                          const double* __restrict__ partial, double c_inv, double q0, double dt_e,
+                                          double* __restrict__ dpdx, double* __restrict__ qdiff) {
+  const double a = weighted_slices(ny, 1, 0, weights, partial);
+  if (threadIdx.x == 0) {
+    const double d = c_inv * a - q0;
+    dpdx[0] = dpdx[0] + d / dt_e;
+    qdiff[0] = d;
   }
 }
 
