@@ -364,11 +364,12 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
-def adjoint_leg(dev, checkpoints=(10, 50, 150)):
+def adjoint_leg(dev, checkpoints=(10, 50, 150, 1500)):
     """Gain gradients per second on the 32x65x32 adjoint configuration
     (Re = 3000, Lx = 2 pi, Lz = pi, T = 15, dt = 0.01: 1500 steps), linear and
     nonlinear (E0 = 1e-4), for checkpoints every K steps; timed with CUDA events
-    against a forward-only pass of the same horizon."""
+    against a forward-only pass of the same horizon. K = 1500 (one segment)
+    records the trajectory in the forward pass and recomputes nothing."""
     import torch
     from jax_spectral_dns.adjoint import GainProblem
     from jax_spectral_dns._plan import to_device_layout

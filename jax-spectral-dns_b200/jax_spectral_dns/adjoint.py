@@ -14,7 +14,9 @@ module puts the dual-solver gradient behind ``torch.autograd.Function``:
   them), register them with the dual plan and take K dual steps.
 
 Memory is N/K + K + 1 states instead of N + 1; the cost is one forward pass,
-one recompute pass and one dual pass (about 3 forward costs).
+one recompute pass and one dual pass (about 3 forward costs). With K >= N the
+forward pass itself records the N + 1 states (there is one segment and nothing
+to recompute): N + 1 states of memory, one forward and one dual pass.
 
 Gradients. With the dual field v0 (the dual run started from -u(T)),
 dE(T) = <-v0, du> and dE(0) = <u0, du> in the energy inner product
@@ -52,7 +54,8 @@ class GainProblem:
         self.dt = float(dt)
         self.n_steps = max(0, int(end_time / dt))
         self.linearise = bool(linearise)
-        self.K = max(1, int(checkpoint_every))
+        self.K = max(1, min(int(checkpoint_every), max(1, self.n_steps)))
+        self.full_trajectory = self.K >= self.n_steps  # one segment: record it in the forward pass
         ny = self.modes[1]
         base = u_max * (1 - cheb_points(ny) ** 2)
         self.fwd = StepPlan(modes, phys, lx, lz, _native.JSD_KIND_PERTURBATION, self.re_tau, self.dt,
@@ -74,6 +77,7 @@ class GainProblem:
         self.w_ddp = torch.zeros(1, dtype=torch.float64, device=device)
         self.w_traj = torch.zeros((self.K + 1,) + shape, dtype=torch.complex128, device=device)
         self._graphs = {}
+        self._traj_owner = None  # checkpoint list of the forward pass whose trajectory w_traj holds
 
     def _run(self, key, make):
         """Replay the captured graph for `key` (capture on first use)."""
@@ -114,10 +118,17 @@ class GainProblem:
         return self.fwd.energy(state)
 
     def forward_checkpoints(self, u0_dev: torch.Tensor):
-        """Run all steps; return the final state and the states at steps 0, K, 2K, ..."""
+        """Run all steps; return the final state and the states at steps 0, K, 2K, ...
+        (with one segment and a nonlinear dual, the whole trajectory is kept in
+        the working buffer instead)."""
         self.w_fwd.copy_(u0_dev)
         self.w_dp.zero_()
         cps = [u0_dev.clone()]
+        if self.full_trajectory and not self.linearise and self.n_steps > 0:
+            self._fwd_traj(self.n_steps)
+            self._traj_owner = cps  # the recorded trajectory belongs to this forward pass
+            return self.w_fwd.clone(), cps
+        self._traj_owner = None
         t = 0
         while t < self.n_steps:
             n = min(self.K, self.n_steps - t)
@@ -136,10 +147,13 @@ class GainProblem:
         for seg in range(len(bounds) - 2, -1, -1):
             s0, s1 = bounds[seg], bounds[seg + 1]
             n = s1 - s0
-            if not self.linearise:
+            # (a later forward pass may have overwritten the recorded trajectory:
+            # then the single segment is recomputed like any other)
+            if not self.linearise and not (self._traj_owner is cps and len(bounds) == 2):
                 self.w_fwd.copy_(cps[seg])
                 self.w_dp.zero_()
                 self._fwd_traj(n)
+                self._traj_owner = None  # w_traj now holds this recomputed segment
             # dual step t of this segment uses the segment state n - t
             self._dual_steps(n)
         return self.w_dual.clone()

@@ -26,10 +26,11 @@ def test_linear_dual_gradient_matches_reference(cuda, K):
     assert abs(g / float(d["gain"]) - 1) < 1e-10
 
 
-@pytest.mark.parametrize("K", [1, 2, 5])
+@pytest.mark.parametrize("K", [1, 2, 5, 10**6])
 def test_nonlinear_dual_gradient_with_checkpoints(cuda, K):
     """Checkpoints every K steps and segment recompute give the reference
-    gradient (the forward states the dual reads are recomputed exactly)."""
+    gradient (the forward states the dual reads are recomputed exactly); K >= N
+    records the trajectory in the forward pass and recomputes nothing."""
     d = golden("dual_nonlin_9x33x9")
     g, grad = dual_gradient(torch.as_tensor(d["u0"]), _problem(d, False, K))
     assert rel(grad.cpu().numpy(), d["grad"]) < 1e-10
@@ -92,3 +93,23 @@ def test_autograd_gain_vs_central_differences(cuda, linearise, tol):
         fd = (gain(u0 + h * dvec, p) - gain(u0 - h * dvec, p)).item() / (2 * h)
         ad = torch.sum((x.grad.conj() * dvec).real).item()
         assert abs(ad / fd - 1) < tol, (ad, fd)
+
+
+def test_recorded_trajectory_is_not_reused_after_another_forward(cuda):
+    """With one segment the forward pass records the trajectory; a later
+    forward pass on another field overwrites it, and the backward of the first
+    must then recompute instead of reading the wrong states."""
+    d = golden("dual_nonlin_9x33x9")
+    p = _problem(d, False, 10**6)
+    assert p.full_trajectory
+    ua = torch.as_tensor(d["u0"]).clone().requires_grad_(True)
+    ub = (0.5 * torch.as_tensor(d["u0"])).clone().requires_grad_(True)
+    ga = gain(ua, p)
+    gb = gain(ub, p)
+    ga.backward()
+    gb.backward()
+    ref = _problem(d, False, 1)
+    for u, g in ((ua, ua.grad), (ub, ub.grad)):
+        uu = u.detach().clone().requires_grad_(True)
+        gain(uu, ref).backward()
+        assert rel(g.cpu().numpy(), uu.grad.cpu().numpy()) < 1e-10
