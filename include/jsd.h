@@ -143,6 +143,18 @@ int jsd_energy_runs(jsd_plan* plan, const void* state, double* out, void* stream
  * finished runs from the end of the run order. Runs keep their Reynolds
  * numbers. No counterpart in the reference. */
 int jsd_set_batch_active(jsd_plan* plan, int n_runs);
+
+/* coupling_term of the perturbation and dual equations
+ * (navier_stokes_perturbation.py:401-415; the extra terms of
+ * navier_stokes_perturbation.py:217-237 and ..._dual.py:270-292 when off).
+ * Default on. */
+int jsd_set_coupling_term(jsd_plan* plan, int on);
+
+/* Replace the base profile U(y) and dU/dy (device arrays of Ny doubles,
+ * copied on `stream`) for the following steps: the time-dependent base of
+ * NavierStokesVelVortPerturbationInstationary.vel_base_fn
+ * (navier_stokes_perturbation_instationary.py:37-83) is set once per step. */
+int jsd_set_base_flow(jsd_plan* plan, const double* base_u, const double* base_du, void* stream);
 int jsd_batch_active(const jsd_plan* plan);
 
 /* Kinetic energy of a state without a plan and without allocating anything.

@@ -161,6 +161,7 @@ struct jsd_plan {
   double2 *twx = nullptr, *twz = nullptr;
   float2 *twx32 = nullptr, *twz32 = nullptr;
   int nb_max = 1;               // runs the workspace is sized for (g.nb = runs stepped now)
+  bool coupling = true;         // false: coupling_term = False terms (perturbation and dual)
   // tcgen05 split-TF32 y-derivatives (mixed form, Ny <= 129): rows computed
   // (min(Ny, 128); for Ny = 129 the y = -1 wall row is left out, which only
   // steady-state stages may do), packed D parts, kernel choice, error flag
@@ -607,6 +608,13 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
   int rc = nonlinear(p, state, uhist, st, s);
   if (rc) return rc;
   const int blk = 256;
+  if (!p->coupling && p->desc.kind != JSD_KIND_NS) {
+    if (p->desc.kind == JSD_KIND_PERTURBATION)
+      k_coupling_off<kPerturbation><<<grid_for(fs, blk), blk, 0, s>>>(gp, v, p->dub, p->H1, p->hg);
+    else
+      k_coupling_off<kDual><<<grid_for(fs, blk), blk, 0, s>>>(gp, u, p->dub, p->H1, p->hg);
+    JSD_LAUNCHED("k_coupling_off");
+  }
   if (!p->om_valid) {
     k_omega<<<grid_for(fs, blk), blk, 0, s>>>(gp, u, w, p->om);
     JSD_LAUNCHED("k_omega");
@@ -1034,7 +1042,8 @@ int jsd_launches_per_step(const jsd_plan* plan) {
   // dv/dy carried from the last stage), nonlinear terms (3 transforms or 1 linear
   // kernel), 2 GEMMs, eigen update, mean flow and reconstruct; omega_y is carried
   // too, except after the mass-flux correction (3 launches) changed u
-  const int per_stage = linear ? 6 : 9;
+  const bool coupling_off = !plan->coupling && plan->desc.kind != JSD_KIND_NS;
+  const int per_stage = (linear ? 6 : 9) + (coupling_off ? 1 : 0);
   const bool cmf = plan->desc.constant_mass_flux != 0;
   return 3 * per_stage + (cmf ? 3 + 1 : 0);
 }
@@ -1336,6 +1345,23 @@ int jsd_energy_runs(jsd_plan* plan, const void* state, double* out, void* stream
   k_weighted_total_runs_sliced<<<g.nb, 32, 0, s>>>(g.ny, g.nb, plan->yw, plan->partial, 0.25 * g.c_inv * g.c_inv,
                                                     out);
   JSD_LAUNCHED("k_weighted_total_runs_sliced");
+  return 0;
+}
+
+int jsd_set_coupling_term(jsd_plan* plan, int on) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  if (plan->desc.kind == JSD_KIND_NS && !on) return fail(JSD_ERR_ARG, "coupling_term applies to perturbation equations");
+  plan->coupling = on != 0;
+  return 0;
+}
+
+int jsd_set_base_flow(jsd_plan* plan, const double* base_u, const double* base_du, void* stream) {
+  if (!plan || !base_u || !base_du) return fail(JSD_ERR_ARG, "null argument");
+  if (!plan->ub || !plan->dub) return fail(JSD_ERR_STATE, "the plan has no base flow");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t bytes = (size_t)plan->g.ny * sizeof(double);
+  JSD_CUDA(cudaMemcpyAsync(plan->ub, base_u, bytes, cudaMemcpyDeviceToDevice, s));
+  JSD_CUDA(cudaMemcpyAsync(plan->dub, base_du, bytes, cudaMemcpyDeviceToDevice, s));
   return 0;
 }
 

@@ -469,6 +469,35 @@ __global__ void k_linear_terms(Geo g, const double2* __restrict__ u, const doubl
   }
 }
 
+// coupling_term = False (navier_stokes_perturbation.py:217-237,
+// navier_stokes_perturbation_dual.py:270-292): with C = hat(U'(y) f) =
+// U'(y) RT(f) (RT = Hermitian part, then the reference truncation)
+//   perturbation: h_g += i kz C  with f = v (wall-normal velocity);
+//   dual:         h_v += d_x^2 C + d_z^2 C = -k^2 C, i.e. H1 += C, with f = the
+//                 streamwise component of the dual field.
+// g.ny = planes (batch runs included); dubase indexed by Chebyshev row.
+template <int KIND>
+__global__ void k_coupling_off(Geo g, const double2* __restrict__ f, const double* __restrict__ dubase,
+                               double2* __restrict__ H1, double2* __restrict__ hg) {
+  const size_t total = (size_t)g.ny * g.nk;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+    const int y = (int)(t / g.nk);
+    const int r = (int)(t - (size_t)y * g.nk);
+    const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+    int sx, sz;
+    bool cj;
+    truncation_source(g, ix, iz, sx, sz, cj);
+    double2 c = sym_at(g, f, y, sx, sz);
+    if (cj) c = cconj(c);
+    c = cscale(c, dubase[y / g.nb]);
+    if (KIND == kPerturbation) {
+      hg[t] = cadd(hg[t], cmul_ik(c, kz_of(g, iz)));
+    } else {
+      H1[t] = cadd(H1[t], c);
+    }
+  }
+}
+
 // omega_y = i kz u - i kx w (the y component of curl u, domain.py:920-933)
 __global__ void k_omega(Geo g, const double2* __restrict__ u, const double2* __restrict__ w,
                         double2* __restrict__ om) {

@@ -52,6 +52,7 @@ EXPORTED = (
     "jsd_set_gemm_config", "jsd_xmid_variant", "jsd_set_xmid_variant",
     "jsd_energy_runs", "jsd_set_batch_active", "jsd_batch_active",
     "jsd_split_kernel", "jsd_set_split_kernel", "jsd_device_error",
+    "jsd_set_coupling_term", "jsd_set_base_flow",
 )
 
 ABI_VERSION = 2  # JSD_ABI_VERSION of include/jsd.h this binding is written for
@@ -105,6 +106,8 @@ def load(path: str = LIB_PATH):
     lib.jsd_split_kernel.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_set_split_kernel.argtypes = [vp, ctypes.c_int]
     lib.jsd_device_error.argtypes = [vp, vp]
+    lib.jsd_set_coupling_term.argtypes = [vp, ctypes.c_int]
+    lib.jsd_set_base_flow.argtypes = [vp, vp, vp, vp]
     lib.jsd_set_batch_active.argtypes = [vp, ctypes.c_int]
     lib.jsd_batch_active.argtypes = [vp]
     lib.jsd_set_xmid_variant.argtypes = [vp, ctypes.c_int]

@@ -224,6 +224,17 @@ class StepPlan:
                                                ctypes.c_void_p(out.data_ptr()), _stream_ptr()), "jsd_energy_runs")
         return out
 
+    def set_coupling_term(self, on: bool) -> None:
+        _native.check(self.lib.jsd_set_coupling_term(self.handle, int(bool(on))), "jsd_set_coupling_term")
+
+    def set_base_flow(self, base_u: torch.Tensor, base_du: torch.Tensor) -> None:
+        """U(y) and dU/dy as float64 device tensors of Ny entries (copied on the current stream)."""
+        assert base_u.dtype == torch.float64 and base_du.dtype == torch.float64
+        assert base_u.is_contiguous() and base_du.is_contiguous()
+        _native.check(self.lib.jsd_set_base_flow(self.handle, ctypes.c_void_p(base_u.data_ptr()),
+                                                 ctypes.c_void_p(base_du.data_ptr()), _stream_ptr()),
+                      "jsd_set_base_flow")
+
     def set_batch_active(self, n_runs: int) -> None:
         _native.check(self.lib.jsd_set_batch_active(self.handle, int(n_runs)), "jsd_set_batch_active")
 

@@ -42,6 +42,7 @@ class NavierStokesVelVort(Equation):
         super().__init__(domain, velocity_field, **params)
         self._plan: Optional[StepPlan] = None
         self._plan_key = None
+        self._plans = {}  # plans by specification (linearise / coupling may change with the step)
         self.enforce_base = False
         self.constant_mass_flux = bool(params.get("constant_mass_flux", False))
         self.flow_rate = self.get_flow_rate()
@@ -94,9 +95,10 @@ class NavierStokesVelVort(Equation):
     def update_dt(self, new_dt: float) -> None:
         self._dt = float(new_dt)
         self._plan = None
+        self._plans = {}
 
     # ---- native plan ------------------------------------------------------
-    def _plan_spec(self) -> dict:
+    def _plan_spec(self, time_step: int = 0) -> dict:
         dom = self.get_physical_domain()
         return dict(kind=self._kind, re_tau=self.get_Re_tau(), dt=self.get_dt(), dt_explicit=None,
                     linearise=False, constant_mass_flux=self.constant_mass_flux,
@@ -104,16 +106,30 @@ class NavierStokesVelVort(Equation):
                     base_u=None, modes=dom.get_shape(), phys=dom.get_shape_aliasing(),
                     lx=dom.scale_factors[0], lz=dom.scale_factors[2])
 
-    def get_plan(self) -> StepPlan:
-        spec = self._plan_spec()
+    def get_plan(self, time_step: int = 0) -> StepPlan:
+        """The native plan for time step `time_step` (one per distinct set of
+        operators and term switches, created on first use)."""
+        spec = self._plan_spec(time_step)
         key = tuple((k, (tuple(v) if isinstance(v, (tuple, list, np.ndarray)) else v)) for k, v in spec.items())
-        if self._plan is None or self._plan_key != key:
-            self._plan = StepPlan(spec["modes"], spec["phys"], spec["lx"], spec["lz"], spec["kind"], spec["re_tau"],
-                                  spec["dt"], dt_explicit=spec["dt_explicit"], linearise=spec["linearise"],
-                                  constant_mass_flux=spec["constant_mass_flux"],
-                                  flow_rate_target=spec["flow_rate_target"], base_u=spec["base_u"])
-            self._plan_key = key
-        return self._plan
+        plan = self._plans.get(key)
+        if plan is None:
+            plan = StepPlan(spec["modes"], spec["phys"], spec["lx"], spec["lz"], spec["kind"], spec["re_tau"],
+                            spec["dt"], dt_explicit=spec["dt_explicit"], linearise=spec["linearise"],
+                            constant_mass_flux=spec["constant_mass_flux"],
+                            flow_rate_target=spec["flow_rate_target"], base_u=spec["base_u"])
+            if not spec.get("coupling", True):
+                plan.set_coupling_term(False)
+            self._plans[key] = plan
+        self._plan, self._plan_key = plan, key
+        return plan
+
+    def _time_dependent(self) -> bool:
+        """True when the step depends on the step index beyond the dual
+        history (term switches, a time-dependent base flow)."""
+        return False
+
+    def _prepare_step(self, plan: StepPlan, time_step: int) -> None:
+        """Hook run before each step (time-dependent base flows)."""
 
     def _prepare_plan_history(self, plan: StepPlan) -> None:
         """Hook for the dual equations (forward trajectory)."""
@@ -153,8 +169,9 @@ class NavierStokesVelVort(Equation):
         return vf
 
     def perform_runge_kutta_step(self, vel_hat_data, dPdx, time_step: int):
-        plan = self.get_plan()
+        plan = self.get_plan(time_step)
         self._prepare_plan_history(plan)
+        self._prepare_step(plan, time_step)
         st = to_device_layout(vel_hat_data)
         dp = torch.tensor([float(dPdx)], dtype=torch.float64, device=st.device)
         plan.step(st, dp, int(time_step), 1)
@@ -183,8 +200,24 @@ class NavierStokesVelVort(Equation):
                    keep_trajectory: bool = False):
         """Advance a device-layout state; optionally return all states
         (n_steps + 1, 3, Ny, Mx, Mz) including the initial one."""
-        plan = self.get_plan()
+        plan = self.get_plan(first_step)
         self._prepare_plan_history(plan)
+        if self._time_dependent():
+            traj = dps = None
+            if keep_trajectory:
+                traj = torch.empty((n_steps + 1,) + tuple(state.shape), dtype=state.dtype, device=state.device)
+                dps = torch.empty(n_steps + 1, dtype=torch.float64, device=state.device)
+                traj[0].copy_(state)
+                dps[0] = dpdx[0]
+            for t in range(n_steps):
+                plan = self.get_plan(first_step + t)
+                self._prepare_plan_history(plan)
+                self._prepare_step(plan, first_step + t)
+                plan.step(state, dpdx, first_step + t, 1)
+                if keep_trajectory:
+                    traj[t + 1].copy_(state)
+                    dps[t + 1] = dpdx[0]
+            return traj, dps
         if not keep_trajectory:
             plan.step(state, dpdx, first_step, n_steps)
             return None, None

@@ -3,8 +3,11 @@
 Drop-in for ``NavierStokesVelVortPerturbation`` of dakling/jax-spectral-dns
 (navier_stokes_perturbation.py:341-520): the default base flow is
 u_max_over_u_tau * (1 - y^2); ``velocity_base_hat`` may supply another
-streamwise profile U(y); ``linearise`` drops the quadratic term;
-``constant_mass_flux`` keeps zero perturbation flow rate.
+streamwise profile U(y); ``linearise`` drops the quadratic term and
+``coupling_term=False`` adds the reference's extra h_g term, both also
+switchable at a fraction of the run (``linearise_switch``,
+``coupling_term_switch``); ``constant_mass_flux`` keeps zero perturbation
+flow rate.
 """
 from __future__ import annotations
 
@@ -38,13 +41,25 @@ class NavierStokesVelVortPerturbation(NavierStokesVelVort):
             base_hat = VectorField([ux.hat(), zero.hat(), zero.hat()], "velocity_base_hat")
         self.add_field("velocity_base_hat", base_hat)
         self.base_profile = self._base_profile(base_hat)
-        if params.get("linearise_switch") is not None or params.get("coupling_term_switch") is not None:
-            raise NotImplementedError("time-dependent linearise/coupling switches are not supported")
-        lin = bool(params.get("linearise", False))
-        self.linearise = lambda _t: lin
-        if not bool(params.get("coupling_term", True)):
-            raise NotImplementedError("coupling_term=False is not supported")
-        self.coupling_term = lambda _t: True
+        # linearise / coupling_term, constant or switched at a fraction of the
+        # run (navier_stokes_perturbation.py:385-415)
+        n_total = len(np.arange(0, self.end_time, self.get_dt()))
+        self.linearise_switch = params.get("linearise_switch")
+        if self.linearise_switch is not None:
+            assert params.get("linearise") is None, "need to either pass linearise or linearise_switch."
+            ls = float(self.linearise_switch)
+            self.linearise = lambda t: t < n_total * ls
+        else:
+            lin = bool(params.get("linearise", False))
+            self.linearise = lambda _t: lin
+        self.coupling_term_switch = params.get("coupling_term_switch")
+        if self.coupling_term_switch is not None:
+            assert params.get("coupling_term") is None, "need to either pass coupling_term or coupling_term_switch."
+            cs = float(self.coupling_term_switch)
+            self.coupling_term = lambda t: not (t < n_total * cs)
+        else:
+            cpl = bool(params.get("coupling_term", True))
+            self.coupling_term = lambda _t: cpl
         self.enforce_base = bool(params.get("enforce_base", False))
         if self.enforce_base:
             raise NotImplementedError("enforce_base is not supported")
@@ -62,11 +77,15 @@ class NavierStokesVelVortPerturbation(NavierStokesVelVort):
         u = self.get_physical_domain().hat().field_no_hat(data[0])
         return u[0, :, 0].double().cpu().numpy().copy()
 
-    def _plan_spec(self) -> dict:
-        spec = super()._plan_spec()
-        spec["linearise"] = self.linearise(0)
+    def _plan_spec(self, time_step: int = 0) -> dict:
+        spec = super()._plan_spec(time_step)
+        spec["linearise"] = bool(self.linearise(time_step))
+        spec["coupling"] = bool(self.coupling_term(time_step))
         spec["base_u"] = self.base_profile
         return spec
+
+    def _time_dependent(self) -> bool:
+        return self.linearise_switch is not None or self.coupling_term_switch is not None
 
     def set_linearise(self) -> None:
         """Pressure-gradient / mass-flux set-up (navier_stokes_perturbation.py:468-520)."""

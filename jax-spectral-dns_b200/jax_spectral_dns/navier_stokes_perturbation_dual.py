@@ -64,10 +64,10 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
                    coupling_term=True, **stripped)
         return dual
 
-    def _plan_spec(self) -> dict:
+    def _plan_spec(self, time_step: int = 0) -> dict:
         """The dual steps with the forward equation's implicit operators
         (positive Re and dt) and -dt on the explicit terms."""
-        spec = super()._plan_spec()
+        spec = super()._plan_spec(time_step)
         spec["re_tau"] = self.forward_equation.get_Re_tau()
         spec["dt"] = self.forward_equation.get_dt()
         spec["dt_explicit"] = self.get_dt()

@@ -316,6 +316,9 @@ class Stepper:
         self.base_hat = base_hat
         self.flow_rate_target = flow_rate_target
         self.u_history = None  # dual: callable t -> forward state
+        # time-dependent base flow t -> base_hat (NavierStokesVelVortPerturbationInstationary);
+        # linearise / coupling_term may also be callables t -> bool (the *_switch parameters)
+        self.base_fn = None
         self._prepare()
 
     def _prepare(self):
@@ -401,11 +404,14 @@ class Stepper:
 
     def _nonlinear(self, vel_hat, t):
         g = self.g
+        lin = self.linearise(t) if callable(self.linearise) else self.linearise
+        cpl = self.coupling_term(t) if callable(self.coupling_term) else self.coupling_term
+        base = self.base_fn(t) if self.base_fn is not None else self.base_hat
         if self.kind == "ns":
             return nonlinear_ns(g, vel_hat)
         if self.kind == "perturbation":
-            return nonlinear_perturbation(g, vel_hat, self.base_hat, self.linearise, self.coupling_term)
-        return nonlinear_dual(g, vel_hat, self.base_hat, self.u_history(t), self.linearise, self.coupling_term)
+            return nonlinear_perturbation(g, vel_hat, base, lin, cpl)
+        return nonlinear_dual(g, vel_hat, base, self.u_history(t), lin, cpl)
 
     def rk_step(self, vel_hat: np.ndarray, dpdx: float, time_step: int):
         """perform_runge_kutta_step + enforce_constant_mass_flux
@@ -497,6 +503,31 @@ def laminar_base_hat(g: Grid, u_max: float = 1.0) -> np.ndarray:
     X = np.meshgrid(np.zeros(g.px), g.y, np.zeros(g.pz), indexing="ij")[1]
     ux = u_max * (1 - X ** 2)
     zero = 0.0 * X
+    return np.array([g.hat(ux), g.hat(zero), g.hat(zero)])
+
+
+def instationary_base_hat(g: Grid, t: float, re: float, kappa: float = 1.0, accelerate: bool = True,
+                          n_max: int = 100) -> np.ndarray:
+    """Base flow of NavierStokesVelVortPerturbationInstationary.vel_base_fn
+    (navier_stokes_perturbation_instationary.py:37-83) at time t: wall-driven
+    profile with wall speed g_w(t) = 1 - exp(-kappa t) (accelerate) or
+    exp(-kappa t) and its series correction, built on the physical grid and
+    transformed like the reference."""
+    gw = (1.0 - np.exp(-kappa * t)) if accelerate else np.exp(-kappa * t)
+    dgw = (kappa * np.exp(-kappa * t)) if accelerate else (-kappa * np.exp(-kappa * t))
+    dgw0 = kappa if accelerate else -kappa
+    y = g.y
+    prof = gw * y + re / 6 * dgw * (y ** 3 - y)
+    coeff = -1.0 if accelerate else 1.0
+    for n in range(1, n_max):
+        c1n = (-2 * re * (-1) ** n / (np.pi * n) ** 3) * dgw0
+        a_n = (np.pi * n) ** 2 / re
+        integ = kappa ** 2 * coeff / (a_n - kappa)
+        prof = prof + (np.exp(-kappa * t) - np.exp(-a_n * t)) * (
+            -(2 * re * (-1) ** n) / (np.pi * n) ** 3 * integ * np.sin(n * np.pi * y))
+        prof = prof + np.exp(-a_n * t) * c1n * np.sin(n * np.pi * y)
+    ux = np.broadcast_to(prof[None, :, None], (g.px, g.ny, g.pz)).copy()
+    zero = np.zeros_like(ux)
     return np.array([g.hat(ux), g.hat(zero), g.hat(zero)])
 
 

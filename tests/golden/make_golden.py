@@ -46,6 +46,8 @@ from jax_spectral_dns.field import FourierField, VectorField  # noqa: E402
 from jax_spectral_dns.navier_stokes import NavierStokesVelVort  # noqa: E402
 from jax_spectral_dns.navier_stokes_perturbation import NavierStokesVelVortPerturbation  # noqa: E402
 from jax_spectral_dns.navier_stokes_perturbation_dual import NavierStokesVelVortPerturbationDual  # noqa: E402
+from jax_spectral_dns.navier_stokes_perturbation_instationary import (  # noqa: E402
+    NavierStokesVelVortPerturbationInstationary)
 
 Equation.initialize()
 Equation.verbosity_level = 0
@@ -202,6 +204,39 @@ def case_dual_nonlin():
                (4, 4), 1e-4, 6, False)
 
 
+def case_instationary():
+    """Perturbation about the accelerating wall-driven base flow of
+    NavierStokesVelVortPerturbationInstationary (kappa = 1.5, n_max = 30,
+    coupling_term off, base re-evaluated every step), Re=2000, 9x33x9 modes,
+    E0=1e-3, dt=0.01, 12 steps."""
+    shape, lx, lz = (8, 33, 8), 2 * math.pi, math.pi
+    re, dt, n = 2000.0, 0.01, 12
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (4, 4), 1e-3, seed=7)
+    nse = NavierStokesVelVortPerturbationInstationary(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, kappa=1.5,
+                                                      accelerate=True, n_max=30)
+    nse.activate_jit()
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={1, n})
+    _save("instationary_9x33x9", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n,
+          kappa=1.5, n_max=30, u0=u0, u1=states[1], un=states[n], energy=en)
+
+
+def case_coupling_off():
+    """Nonlinear perturbation about Poiseuille flow with coupling_term=False
+    and linearised for the first half of the run (linearise_switch = 0.5),
+    Re=3000, 9x33x9 modes, E0=1e-3, dt=0.01, 10 steps."""
+    shape, lx, lz = (8, 33, 8), 2 * math.pi, math.pi
+    re, dt, n = 3000.0, 0.01, 10
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (4, 4), 1e-3, seed=8)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, coupling_term=False,
+                                          linearise_switch=0.5)
+    nse.activate_jit()
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={1, n})
+    _save("coupling_off_9x33x9", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n,
+          linearise_switch=0.5, u0=u0, u1=states[1], un=states[n], energy=en)
+
+
 def case_cg_opt():
     """Reference ConjugateGradientDescentSolver, 5 iterations, linearised
     pseudo-2D 5x33x5, Re=3000, T=0.2 (20 steps): gain per iteration and the
@@ -241,6 +276,8 @@ CASES = {
     "dual_lin": case_dual_lin,
     "dual_nonlin": case_dual_nonlin,
     "cg_opt": case_cg_opt,
+    "instationary": case_instationary,
+    "coupling_off": case_coupling_off,
 }
 
 if __name__ == "__main__":

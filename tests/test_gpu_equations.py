@@ -77,3 +77,39 @@ def test_dual_class_nonlinear_gradient(cuda):
     grad = dual.get_grad()
     assert rel(grad.cpu().numpy(), d["grad"]) < TOL
     assert abs(dual.gain / float(d["gain"]) - 1) < TOL
+
+
+def test_instationary_base_flow_matches_reference(cuda):
+    """NavierStokesVelVortPerturbationInstationary: base re-evaluated every
+    step, coupling term off (reference fixture)."""
+    from jax_spectral_dns.navier_stokes_perturbation_instationary import NavierStokesVelVortPerturbationInstationary
+
+    d = golden("instationary_9x33x9")
+    n, dt = int(d["n_steps"]), float(d["dt"])
+    nse = NavierStokesVelVortPerturbationInstationary(_vf(d), Re=float(d["re"]), dt=dt, end_time=n * dt,
+                                                      kappa=float(d["kappa"]), accelerate=True, n_max=int(d["n_max"]))
+    u = nse.get_initial_field("velocity_hat").get_data()
+    dpdx = 0.0
+    for t in range(n):
+        u, dpdx = nse.perform_time_step(u, dpdx, t)
+        if t == 0:
+            assert rel(u.cpu().numpy(), d["u1"]) < TOL
+    assert rel(u.cpu().numpy(), d["un"]) < TOL
+    # the same run through solve_scan (one step per launch sequence, base updated in between)
+    nse2 = NavierStokesVelVortPerturbationInstationary(_vf(d), Re=float(d["re"]), dt=dt, end_time=n * dt,
+                                                       kappa=float(d["kappa"]), accelerate=True,
+                                                       n_max=int(d["n_max"]))
+    nse2.solve_scan()
+    assert rel(nse2.get_latest_field("velocity_hat").get_data().cpu().numpy(), d["un"]) < TOL
+
+
+def test_coupling_off_and_linearise_switch_match_reference(cuda):
+    d = golden("coupling_off_9x33x9")
+    n, dt = int(d["n_steps"]), float(d["dt"])
+    nse = NavierStokesVelVortPerturbation(_vf(d), Re=float(d["re"]), dt=dt, end_time=n * dt, coupling_term=False,
+                                          linearise_switch=float(d["linearise_switch"]))
+    nse.solve_scan()
+    assert rel(nse.get_latest_field("velocity_hat").get_data().cpu().numpy(), d["un"]) < TOL
+    u = nse.get_initial_field("velocity_hat").get_data()
+    u1, _ = nse.perform_time_step(u, 0.0, 0)
+    assert rel(u1.cpu().numpy(), d["u1"]) < TOL

@@ -66,3 +66,27 @@ def test_transient_growth_energy_history():
     assert e.shape == (101,)
     assert np.all(np.isfinite(e)) and e[0] > 0
     assert abs(e[0] / 1e-6 - 1) < 1e-10  # seeded at E0 = 1e-6
+
+
+def test_instationary_base_flow():
+    """Wall-driven accelerating base re-evaluated every step, coupling_term
+    off (NavierStokesVelVortPerturbationInstationary)."""
+    d = golden("instationary_9x33x9")
+    n, dt, re = int(d["n_steps"]), float(d["dt"]), float(d["re"])
+    st = _pert(d, False)
+    st.coupling_term = False
+    st.base_fn = lambda t: O.instationary_base_hat(st.g, t * dt, re, float(d["kappa"]), True, int(d["n_max"]))
+    u, _, _ = O.run(st, d["u0"], n)
+    assert rel(u, d["un"]) < 1e-12
+
+
+def test_coupling_off_with_linearise_switch():
+    d = golden("coupling_off_9x33x9")
+    n = int(d["n_steps"])
+    st = _pert(d, False)
+    st.coupling_term = False
+    st.linearise = lambda t: t < n * float(d["linearise_switch"])
+    u1, _, _ = O.run(st, d["u0"], 1)
+    assert rel(u1, d["u1"]) < 1e-12
+    u, _, _ = O.run(st, d["u0"], n)
+    assert rel(u, d["un"]) < 1e-12
