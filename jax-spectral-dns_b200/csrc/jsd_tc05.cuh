@@ -39,6 +39,7 @@ constexpr int kTcKp = 136;                     // padded K (17 MMA steps of 8)
 constexpr int kTcASize = kTcM * kTcKp * 4;     // bytes of one A part (69632)
 constexpr int kTcBSize = kTcN * kTcKp * 4;     // bytes of one B part (34816)
 constexpr int kTcStageLd = kTcN + 1;           // padded row of the FP64 output stage
+constexpr int kTcBatch = 17;                   // tile loads in flight per thread during the conversion
 constexpr size_t kTcSmem = 2 * (size_t)kTcASize + 2 * (size_t)kTcBSize + 64;
 static_assert((size_t)kTcM * kTcStageLd * 8 <= 2 * (size_t)kTcBSize, "output stage must fit in the B tiles");
 
@@ -181,17 +182,32 @@ __global__ void __launch_bounds__(128, 1) k_tc05_dfield(const float* __restrict_
     const double* B;
     double* C;
     tc05_entry(b, e, B, C);
-    // B tile -> TF32 hi / lo core matrices; a warp fills one core matrix (8 columns x 4 K) per pass
-    for (int cm = warp; cm < (kTcN / 8) * (2 * ksteps); cm += 4) {
-      const int g = cm % (kTcN / 8), c = cm / (kTcN / 8);
-      const int n = g * 8 + (lane >> 2), k = c * 4 + (lane & 3);
-      double v = 0.0;
-      if (k < b.K && n0 + n < b.N) v = B[(size_t)k * b.ldb + n0 + n];
-      const float h = tf32_round_dev((float)v);
-      const float l = tf32_round_dev((float)(v - (double)h));
-      const int off = tc05_offset(kTcN, n, k) >> 2;
-      sBh[off] = h;
-      sBl[off] = l;
+    // B tile -> TF32 hi / lo core matrices. A warp fills one core matrix
+    // (8 columns x 4 K, lane = (column, K) pair) per pass; each thread first
+    // issues the loads of kTcBatch passes, then converts and stores them, so
+    // that many loads are in flight.
+    const int ncm = (kTcN / 8) * (2 * ksteps);
+    for (int cm0 = warp; cm0 < ncm; cm0 += 4 * kTcBatch) {
+      double v[kTcBatch];
+#pragma unroll
+      for (int q = 0; q < kTcBatch; ++q) {
+        const int cm = cm0 + 4 * q;
+        const int g = cm % (kTcN / 8), c = cm / (kTcN / 8);
+        const int n = g * 8 + (lane >> 2), k = c * 4 + (lane & 3);
+        v[q] = (cm < ncm && k < b.K && n0 + n < b.N) ? B[(size_t)k * b.ldb + n0 + n] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < kTcBatch; ++q) {
+        const int cm = cm0 + 4 * q;
+        if (cm >= ncm) break;
+        const int g = cm % (kTcN / 8), c = cm / (kTcN / 8);
+        const int n = g * 8 + (lane >> 2), k = c * 4 + (lane & 3);
+        const float h = tf32_round_dev((float)v[q]);
+        const float l = tf32_round_dev((float)(v[q] - (double)h));
+        const int off = tc05_offset(kTcN, n, k) >> 2;
+        sBh[off] = h;
+        sBl[off] = l;
+      }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();

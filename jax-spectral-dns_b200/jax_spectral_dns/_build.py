@@ -9,7 +9,6 @@ import sys
 _HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(os.path.dirname(_HERE), "csrc")
 SOURCES = ["jsd_api.cu"]
-HEADERS = ["jsd_common.cuh", "jsd_fft.cuh", "jsd_gemm.cuh", "jsd_spectral.cuh"]
 OUT = os.path.join(_HERE, "libjsd.so")
 
 NVCC_FLAGS = [
@@ -30,7 +29,8 @@ def _stale() -> bool:
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
+    headers = sorted(f for f in os.listdir(CSRC) if f.endswith(".cuh"))  # every header the library includes
+    deps = [os.path.join(CSRC, f) for f in SOURCES + headers]
     deps.append(os.path.join(os.path.dirname(os.path.dirname(_HERE)), "include", "jsd.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
