@@ -266,7 +266,43 @@ def case_cg_opt():
           u0=u0, gains=np.array(gains), final_guess=final, final_value=float(solver.value))
 
 
+def case_lsc():
+    """Reference LinearStabilityCalculation (n = 50): eigenvalues, leading
+    eigenvectors, optimal gains and coefficients for three (Re, alpha, beta,
+    T) cases, and the optimal initial field on the 5x50x5-mode box of the
+    reference's run_transient_growth (examples.py:1274-1324)."""
+    from jax_spectral_dns.linear_stability_calculation import LinearStabilityCalculation
+
+    out = {}
+    for tag, re, alpha, beta, t, modes in (("re3000", 3000.0, 1.0, 0.0, 15.0, 60),
+                                           ("re600", 600.0, 1.0, 0.0, 2.0, 60),
+                                           ("re1000b", 1000.0, 1.0, 1.0, 10.0, 40)):
+        lsc = LinearStabilityCalculation(Re=re, alpha=alpha, beta=beta, n=50)
+        evs, evecs = lsc.calculate_eigenvalues()
+        s, coeffs = lsc.calculate_transient_growth_svd(t, modes, save=False)
+        out[tag + "_params"] = np.array([re, alpha, beta, t, modes])
+        out[tag + "_evs"] = np.asarray(evs)
+        out[tag + "_evecs3"] = np.array(evecs[:3])
+        out[tag + "_S"] = np.asarray(s)
+        out[tag + "_coeffs"] = np.asarray(coeffs)
+        if tag == "re3000":
+            out[tag + "_gains_T"] = np.array([2.0, 5.0, 10.0])
+            out[tag + "_gains"] = np.array([float(lsc.calculate_transient_growth_svd(tt, modes)[0][0] ** 2)
+                                            for tt in (2.0, 5.0, 10.0)])
+            dom = PhysicalDomain.create((4, 50, 4), (True, False, True),
+                                        scale_factors=(2 * math.pi / alpha, 1.0, 1.0e-3), aliasing=3 / 2)
+            u = lsc.calculate_transient_growth_initial_condition(dom, t, modes, recompute_full=True,
+                                                                 save_final=False)
+            out[tag + "_ic"] = np.array([np.asarray(u[i].data) for i in range(3)])
+            out[tag + "_ic_energy"] = float(u.energy())
+            out[tag + "_mode0_energy"] = float(lsc.velocity_field_single_mode(dom, 0, recompute_partial=True).energy())
+    lsc = LinearStabilityCalculation(Re=5772.22, alpha=1.02056, n=50)
+    out["neutral_evs"] = np.asarray(lsc.calculate_eigenvalues()[0][:5])
+    _save("lsc_n50", **out)
+
+
 CASES = {
+    "lsc": case_lsc,
     "lin_pert": case_lin_pert,
     "lin_pert_gain": case_lin_pert_gain,
     "nonlin_pert": case_nonlin_pert,
