@@ -333,7 +333,9 @@ def run_ours(args):
                           "split_kernel": plans[pr].split_kernel()[0],
                           "split_kernel_ms": plans[pr].split_kernel()[1],
                           "xmid_variant": plans[pr].xmid_variant()[0],
-                          "xmid_variant_ms": plans[pr].xmid_variant()[1]}
+                          "xmid_variant_ms": plans[pr].xmid_variant()[1],
+                          "eig_kernels": {site: plans[pr].eig_kernel(i)[0] for i, site in ((1, "eig_in"), (2, "eig_out"))},
+                          "eig_kernel_ms": {site: plans[pr].eig_kernel(i)[1] for i, site in ((1, "eig_in"), (2, "eig_out"))}}
                      for pr, r in results.items()}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,

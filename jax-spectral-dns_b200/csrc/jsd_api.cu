@@ -31,6 +31,7 @@
 #include "jsd_spectral.cuh"
 #include "jsd_spectral_sq.cuh"
 #include "jsd_tc05.cuh"
+#include "jsd_ozaki.cuh"
 
 using namespace jsd;
 
@@ -171,6 +172,15 @@ struct jsd_plan {
   int* errflag = nullptr;       // set by kernels whose bounded waits expired
   int num_sms = 148;
   float split_ms[2] = {};       // autotuner timings of the two split kernels
+  // FP64-accurate eigenbasis products on the int8 tensor cores (mixed plans,
+  // Ny <= 129): slice packs of V^-1 D, V^-1, V and D V (index kOzVinvD ..),
+  // the FP64 operator each replaces, and the kernel choice per call site
+  int8_t* oz_a[4] = {};
+  double *oz_rs[4] = {}, *oz_xr[4] = {}, *oz_xc[4] = {};
+  const double* oz_src[4] = {};
+  bool oz_ready = false;
+  int eig_kernel[3] = {0, 0, 0};  // per GemmSite (eigen sites): 0 DMMA, 1 Ozaki int8
+  float eig_ms[3][2] = {};        // autotuner timings per eigen site: DMMA (best tile), Ozaki
   double* re_run = nullptr;     // Reynolds number per run of a batch (device)
   double* lr_ns = nullptr;      // Linv_ns R_ns per run and stage (row-parallel mean-flow update)
   int gemm_cfg[3] = {2, 2, 2};  // DMMA tile configuration per call site (GemmSite)
@@ -372,6 +382,44 @@ void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M,
 int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, GemmSite site, cudaStream_t s) {
   ProfScope ps(const_cast<jsd_plan*>(p), JSD_PROF_GEMM, gemm_flops(b), s);
   return launch_gemm_cfg(p, b, max_m, p->gemm_cfg[site], s);
+}
+
+// The eigenbasis products of a batch on the int8 tensor cores (k_oz8_gemm);
+// every entry's operator must be one of the packed ones.
+int launch_ozaki(const jsd_plan* p, const GemmBatch& b, cudaStream_t s) {
+  OzBatch o;
+  memset(&o, 0, sizeof(o));
+  o.N = b.N;
+  o.ldb = b.ldb;
+  o.ldc = b.ldc;
+  for (int i = 0; i < b.count; ++i) {
+    const GemmEntry& g = b.e[i];
+    int k = 0;
+    while (k < 4 && p->oz_src[k] != g.A) ++k;
+    if (k == 4 || g.alpha != 1.0) return fail(JSD_ERR_STATE, "operator has no int8 slice pack");
+    OzEntry& e = o.e[o.count++];
+    e.a = p->oz_a[k];
+    e.row_scale = p->oz_rs[k];
+    e.xrow = p->oz_xr[k];
+    e.xcol = p->oz_xc[k];
+    e.B = g.B;
+    e.C = g.C;
+    e.M = g.M;
+    e.K = g.K;
+  }
+  const long long tiles = (long long)((o.N + kOzN - 1) / kOzN) * o.count;
+  ProfScope ps(const_cast<jsd_plan*>(p), JSD_PROF_GEMM, gemm_flops(b), s);
+  k_oz8_gemm<<<(int)std::min<long long>(tiles, p->num_sms), kOzThreads, kOzSmem, s>>>(o, p->errflag);
+  JSD_LAUNCHED("k_oz8_gemm");
+  return 0;
+}
+
+// eigenbasis in / out products: DMMA, or the Ozaki int8 kernel where the plan
+// chose it for the site (force: -1 the plan's choice, 0 DMMA, 1 Ozaki)
+int launch_eig(const jsd_plan* p, const GemmBatch& b, int max_m, GemmSite site, cudaStream_t s, int force = -1) {
+  const int k = force >= 0 ? force : p->eig_kernel[site];
+  if (k == 1 && p->oz_ready) return launch_ozaki(p, b, s);
+  return launch_gemm(p, b, max_m, site, s);
 }
 
 int grid_for(size_t total, int block) {
@@ -629,7 +677,7 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     add_entry(b, p->Vinv, (const double*)p->hg + rowd, p->T + 1 * E, ni, ni);
     if (!p->ev_valid) add_entry(b, p->Vinv, (const double*)v + rowd, p->T + 2 * E, ni, ni);
     if (!p->om_valid) add_entry(b, p->Vinv, (const double*)p->om + rowd, p->T + 3 * E, ni, ni);
-    rc = launch_gemm(p, b, ni, kSiteEigIn, s);
+    rc = launch_eig(p, b, ni, kSiteEigIn, s);
     if (rc) return rc;
   }
   {
@@ -670,7 +718,7 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     add_entry(b, p->Vfull, p->vnt, (double*)v, ny, ni);
     add_entry(b, p->DVfull, p->vnt, (double*)p->dvn, ny, ni);
     add_entry(b, p->Vfull, p->omnt, (double*)p->om, ny, ni);
-    rc = launch_gemm(p, b, ny, kSiteEigOut, s);
+    rc = launch_eig(p, b, ny, kSiteEigOut, s);
     if (rc) return rc;
   }
   k_reconstruct<<<grid_for(fs, blk), blk, 0, s>>>(g, p->dvn, p->om, p->uw00, u, v, w);
@@ -719,6 +767,7 @@ int set_smem_limits() {
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_tc05_dfield, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  JSD_CUDA(cudaFuncSetAttribute(k_oz8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOzSmem));
   cudaError_t err = cudaSuccess;
   for (int sd : kSquareSides)
     with_square_side(sd, [&](auto side) {
@@ -911,6 +960,21 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
         plan->gemm_cfg[site] = c;
       }
     }
+    // eigenbasis sites of mixed plans: the Ozaki int8 kernel against the best DMMA tile
+    if (rc == 0 && site != kSiteDfield && plan->oz_ready) {
+      plan->eig_ms[site][0] = best / 5.f;
+      rc = launch_ozaki(plan, b, s);  // warm-up
+      if (rc == 0 && cudaEventRecord(e0, s) != cudaSuccess) rc = fail(JSD_ERR_CUDA, "cudaEventRecord");
+      for (int r = 0; r < 5 && rc == 0; ++r) rc = launch_ozaki(plan, b, s);
+      float ms = 0.f;
+      if (rc == 0 && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                      cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+        rc = fail(JSD_ERR_CUDA, "autotune timing");
+      if (rc == 0) {
+        plan->eig_ms[site][1] = ms / 5.f;
+        plan->eig_kernel[site] = ms < best ? 1 : 0;
+      }
+    }
   }
   // split-TF32 y-derivative kernels (mixed plans): the steady-state call on u and w
   if (rc == 0 && plan->mixed && plan->tc_rows) {
@@ -981,6 +1045,21 @@ int jsd_set_split_kernel(jsd_plan* plan, int kernel) {
   if (!plan->mixed || kernel < 0 || kernel > 1 || (kernel == 1 && !plan->tc_rows))
     return fail(JSD_ERR_ARG, "split-TF32 kernel not available for this plan");
   plan->split_kernel = kernel;
+  return 0;
+}
+
+int jsd_eig_kernel(const jsd_plan* plan, int site, float* times_ms) {
+  if (!plan || (site != kSiteEigIn && site != kSiteEigOut)) return -1;
+  if (times_ms)
+    for (int k = 0; k < 2; ++k) times_ms[k] = plan->eig_ms[site][k];
+  return plan->oz_ready ? plan->eig_kernel[site] : 0;
+}
+
+int jsd_set_eig_kernel(jsd_plan* plan, int site, int kernel) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  if ((site != kSiteEigIn && site != kSiteEigOut) || kernel < 0 || kernel > 1 || (kernel == 1 && !plan->oz_ready))
+    return fail(JSD_ERR_ARG, "eigenbasis kernel not available for this plan and site");
+  plan->eig_kernel[site] = kernel;
   return 0;
 }
 
@@ -1203,6 +1282,25 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(upload_padded(p, &p->Vinv, d->Vinv, ni, ni, p->lda));
   JSD_TRY(upload_padded(p, &p->Vfull, Vfull.data(), ny, ni, p->lda));
   JSD_TRY(upload_padded(p, &p->DVfull, DVfull.data(), ny, ni, p->lda));
+  if (p->mixed && ny <= kOzM + 1) {
+    // int8 slice packs of the four eigenbasis operators (V^-1 D: K = Ny; V and
+    // D V: M = Ny; at most one of M, K above 128)
+    const double* hostA[4] = {VinvD.data(), d->Vinv, Vfull.data(), DVfull.data()};
+    const int Ms[4] = {ni, ni, ny, ny}, Ks[4] = {ny, ni, ni, ni};
+    const double* devA[4] = {p->VinvD, p->Vinv, p->Vfull, p->DVfull};
+    for (int k = 0; k < 4; ++k) {
+      OzPackA pk;
+      oz_pack_a(hostA[k], Ms[k], Ks[k], Ks[k], pk);
+      JSD_TRY(upload(p, &p->oz_a[k], pk.slices.data(), pk.slices.size()));
+      JSD_TRY(upload(p, &p->oz_rs[k], pk.row_scale.data(), pk.row_scale.size()));
+      JSD_TRY(upload(p, &p->oz_xr[k], pk.xrow.data(), pk.xrow.size()));
+      JSD_TRY(upload(p, &p->oz_xc[k], pk.xcol.data(), pk.xcol.size()));
+      p->oz_src[k] = devA[k];
+    }
+    // (the epilogue's pair stores need 16-byte aligned rows: every output is a
+    // double2 field or an even offset into one, with an even row stride 2 nk nb)
+    p->oz_ready = true;
+  }
   JSD_TRY(upload(p, &p->lam, d->lam, ni));
   JSD_TRY(upload(p, &p->sgn, d->sgn, ni));
   JSD_TRY(upload(p, &p->c0, d->c0, ni));

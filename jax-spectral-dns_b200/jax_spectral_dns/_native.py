@@ -52,7 +52,7 @@ EXPORTED = (
     "jsd_set_gemm_config", "jsd_xmid_variant", "jsd_set_xmid_variant",
     "jsd_energy_runs", "jsd_set_batch_active", "jsd_batch_active",
     "jsd_split_kernel", "jsd_set_split_kernel", "jsd_device_error",
-    "jsd_set_coupling_term", "jsd_set_base_flow",
+    "jsd_set_coupling_term", "jsd_set_base_flow", "jsd_eig_kernel", "jsd_set_eig_kernel",
 )
 
 ABI_VERSION = 2  # JSD_ABI_VERSION of include/jsd.h this binding is written for
@@ -105,6 +105,8 @@ def load(path: str = LIB_PATH):
     lib.jsd_energy_runs.argtypes = [vp, vp, vp, vp]
     lib.jsd_split_kernel.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_set_split_kernel.argtypes = [vp, ctypes.c_int]
+    lib.jsd_eig_kernel.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
+    lib.jsd_set_eig_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.jsd_device_error.argtypes = [vp, vp]
     lib.jsd_set_coupling_term.argtypes = [vp, ctypes.c_int]
     lib.jsd_set_base_flow.argtypes = [vp, vp, vp, vp]

@@ -159,6 +159,16 @@ class StepPlan:
     def set_split_kernel(self, kernel: int) -> None:
         _native.check(self.lib.jsd_set_split_kernel(self.handle, int(kernel)), "jsd_set_split_kernel")
 
+    def eig_kernel(self, site: int):
+        """(eigenbasis product kernel at GEMM site 1 or 2: 0 FP64 DMMA, 1 Ozaki
+        int8 tensor cores; [autotune ms of the best DMMA tile and of Ozaki])."""
+        times = (ctypes.c_float * 2)()
+        k = int(self.lib.jsd_eig_kernel(self.handle, int(site), times))
+        return k, [float(t) for t in times]
+
+    def set_eig_kernel(self, site: int, kernel: int) -> None:
+        _native.check(self.lib.jsd_set_eig_kernel(self.handle, int(site), int(kernel)), "jsd_set_eig_kernel")
+
     def check_device_errors(self) -> None:
         """Raise when a kernel of this plan gave up a bounded wait."""
         _native.check(self.lib.jsd_device_error(self.handle, _stream_ptr()), "jsd_device_error")
