@@ -172,8 +172,8 @@ struct jsd_plan {
   int* errflag = nullptr;       // set by kernels whose bounded waits expired
   int num_sms = 148;
   float split_ms[2] = {};       // autotuner timings of the two split kernels
-  // FP64-accurate eigenbasis products on the int8 tensor cores (mixed plans,
-  // Ny <= 129): slice packs of V^-1 D, V^-1, V and D V (index kOzVinvD ..),
+  // FP64-accurate eigenbasis products on the int8 tensor cores (Ny <= 129;
+  // chosen by the mixed form's autotuner, selectable in any plan): slice packs of V^-1 D, V^-1, V and D V (index kOzVinvD ..),
   // the FP64 operator each replaces, and the kernel choice per call site
   int8_t* oz_a[4] = {};
   double *oz_rs[4] = {}, *oz_xr[4] = {}, *oz_xc[4] = {};
@@ -961,7 +961,7 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
       }
     }
     // eigenbasis sites of mixed plans: the Ozaki int8 kernel against the best DMMA tile
-    if (rc == 0 && site != kSiteDfield && plan->oz_ready) {
+    if (rc == 0 && site != kSiteDfield && plan->oz_ready && plan->mixed) {
       plan->eig_ms[site][0] = best / 5.f;
       rc = launch_ozaki(plan, b, s);  // warm-up
       if (rc == 0 && cudaEventRecord(e0, s) != cudaSuccess) rc = fail(JSD_ERR_CUDA, "cudaEventRecord");
@@ -1282,9 +1282,10 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
   JSD_TRY(upload_padded(p, &p->Vinv, d->Vinv, ni, ni, p->lda));
   JSD_TRY(upload_padded(p, &p->Vfull, Vfull.data(), ny, ni, p->lda));
   JSD_TRY(upload_padded(p, &p->DVfull, DVfull.data(), ny, ni, p->lda));
-  if (p->mixed && ny <= kOzM + 1) {
+  if (ny <= kOzM + 1) {
     // int8 slice packs of the four eigenbasis operators (V^-1 D: K = Ny; V and
-    // D V: M = Ny; at most one of M, K above 128)
+    // D V: M = Ny; at most one of M, K above 128). FP64 plans may select the
+    // kernel too (jsd_set_eig_kernel); only the mixed form's autotuning does.
     const double* hostA[4] = {VinvD.data(), d->Vinv, Vfull.data(), DVfull.data()};
     const int Ms[4] = {ni, ni, ny, ny}, Ks[4] = {ny, ni, ni, ni};
     const double* devA[4] = {p->VinvD, p->Vinv, p->Vfull, p->DVfull};
