@@ -1,5 +1,5 @@
 // FP64-accurate products on the int8 tensor cores (Ozaki splitting), for the
-// eigenbasis transforms of the mixed-precision form.
+// eigenbasis transforms.
 //
 // C (M x N) = A (M x K) B (K x N), A a constant operator (M, K <= 129), B a
 // batch of FP64 fields. Each row i of A and each column j of B is scaled by a
@@ -8,31 +8,37 @@
 //   a_ik = 2^ea_i sum_p alpha_ikp 2^(-7p),  b_kj = 2^eb_j sum_q beta_kjq 2^(-7q),
 //   alpha, beta in [-127, 127], p, q = 1..8.
 // The products alpha_p beta_q are exact int8 tensor-core GEMMs with exact
-// int32 accumulation; the pairs with p + q <= 9 (36 GEMMs) are kept and summed
-// per diagonal d = p + q into 8 int32 accumulators in tensor memory (at most
-// 8 pairs x K=128 x 127^2 < 2^31), which the epilogue combines in FP64:
+// int32 accumulation; the pairs with p + q <= 9 (36 products) are kept and
+// summed per diagonal d = p + q into 8 int32 accumulators in tensor memory (at
+// most 8 pairs x K=128 x 127^2 < 2^31), which the epilogue combines in FP64:
 //   c_ij = 2^(ea_i + eb_j - 14) sum_d acc_d 2^(-7 (d - 2)).
 // The error bound is of the order of an FP64 GEMM's (the dropped terms and the
 // slice remainders are below 2^-56 of |a_i|max |b_j|max per product), so the
-// solves stay FP64-accurate while the arithmetic runs at int8 tensor rate.
+// products stay FP64-accurate while the arithmetic runs at int8 tensor rate.
 // Tensor rows and K are 128; a 129th row of A (M = 129) or a 129th column
-// (K = 129) is applied in FP64 beside the tensor part: the converter warps
-// form the extra row's dot products from the B values they already hold, and
-// the epilogue adds a_i,128 b_128,j.
+// (K = 129) is applied in FP64 beside the tensor part.
 //
-// One persistent CTA of 9 warps per SM, each CTA a contiguous range of
+// The 8 B slices of a 32-column tile are stacked into one 256-row operand
+// (row 32 (q - 1) + column). One MMA per A slice p and K step, with
+// N = 32 (9 - p) stacked rows (slices q = 1..9-p) and its accumulator placed
+// (p - 1) x 32 TMEM columns on, lands every product (p, q) in the columns of
+// diagonal p + q: 32 MMAs of N = 32..256 per tile instead of 36 x 4 narrow
+// ones, so the operands are read from shared memory once per wide product.
+//
+// One persistent CTA of 18 warps per SM, each CTA a contiguous range of
 // 32-column tiles:
-//   * warps 0-3 (converters): load the 128 x 32 FP64 tile of B (warp w columns
-//     8w..8w+7, 4 lanes per column of 32 rows each), find the column scales by
-//     shuffles, cut the slices and store them in the canonical K-major
-//     core-matrix layout (int8, 16 K per 16-byte row), double-buffered;
-//   * warp 8 (issuer): keeps A's 8 slices resident (bulk copy, reloaded when
-//     the operator changes), issues 36 x 4 tcgen05.mma.kind::i8 (M = 128,
-//     N = 32, K = 32) per tile into one of two accumulator sets of 8 x 32 TMEM
-//     columns and commits to an mbarrier;
-//   * warps 4-7 (epilogue, TMEM lane quadrant = warp % 4 = row block): read the
-//     8 accumulators (tcgen05.ld), combine, scale, add the FP64 extras and
-//     store the rows.
+//   * warp 17 (producer): bulk-copies (cp.async.bulk, mbarrier completion) the
+//     next tile's FP64 rows of B into a staging buffer;
+//   * warps 0-7 (converters, warp w = rows 16w..16w+15, lane = column): read
+//     the staged tile, release the staging buffer, exchange partial column
+//     maxima through an mbarrier, cut the 16-row chunk into the 8 slices and
+//     store them in the canonical K-major core-matrix layout;
+//   * warp 16 (issuer): keeps A's 8 slices resident (bulk copy, reloaded when
+//     the operator changes), issues the 32 MMAs (kind::i8, M = 128) into one of
+//     two accumulator sets of 8 x 32 TMEM columns and commits to an mbarrier;
+//   * warps 8-15 (epilogue, TMEM lane quadrant = warp % 4 = row block, half of
+//     the columns each): read the 8 accumulators (tcgen05.ld, two per wait),
+//     combine, scale, add the FP64 extras and store.
 // Every mbarrier wait has an iteration limit; on expiry the kernel raises the
 // error flag, every role stops at its next tile, the issuer waits (bounded) for
 // its last MMAs, and the CTA frees its TMEM and returns.
@@ -52,16 +58,22 @@ constexpr int kOzSlices = 8;                         // 7-bit slices per operand
 constexpr int kOzDiags = kOzSlices;                  // diagonals d = p + q = 2..9
 constexpr int kOzM = 128, kOzK = 128, kOzN = 32;     // tensor rows, tensor K, tile columns
 constexpr int kOzASlice = kOzM * kOzK;               // bytes per A slice (16384)
-constexpr int kOzBSlice = kOzN * kOzK;               // bytes per B slice (4096)
 constexpr int kOzABytes = kOzSlices * kOzASlice;     // 131072
-constexpr int kOzBBytes = kOzSlices * kOzBSlice;     // 32768 per buffer
+constexpr int kOzBRows = kOzSlices * kOzN;           // stacked B operand rows (256)
+constexpr int kOzBBytes = kOzBRows * kOzK;           // 32768
+constexpr int kOzStageRows = kOzK + 1;               // staged FP64 rows (row 128: the K = 129 extra)
+constexpr int kOzStageBytes = kOzStageRows * kOzN * 8;  // 33024
 constexpr int kOzTmemCols = 2 * kOzDiags * kOzN;     // 512: two accumulator sets
-constexpr int kOzConvWarps = 4, kOzEpiWarps = 4;
-constexpr int kOzThreads = 32 * (kOzConvWarps + kOzEpiWarps + 1);
-// side data per buffer (doubles): column scales, B row 128, extra-row dot products
-constexpr int kOzSideScale = 0, kOzSideBx = kOzN, kOzSideDot = 2 * kOzN;
-constexpr int kOzSideDoubles = 3 * kOzN;
-constexpr size_t kOzSmem = (size_t)kOzABytes + 2 * (size_t)kOzBBytes + 2 * sizeof(double) * kOzSideDoubles + 128;
+constexpr int kOzConvWarps = 8, kOzEpiWarps = 8;
+constexpr int kOzIssuerWarp = kOzConvWarps + kOzEpiWarps, kOzProducerWarp = kOzIssuerWarp + 1;
+constexpr int kOzThreads = 32 * (kOzProducerWarp + 1);  // 576
+// side data per tile buffer (doubles): column scales, B row 128, extra-row
+// dot products (read by the epilogue), partial maxima and partial dots per
+// converter warp (exchanged among the converters)
+constexpr int kOzSideScale = 0, kOzSideBx = kOzN, kOzSideDot = 2 * kOzN, kOzSidePMax = 3 * kOzN,
+              kOzSidePDot = kOzSidePMax + kOzConvWarps * kOzN;
+constexpr int kOzSideDoubles = kOzSidePDot + kOzConvWarps * kOzN;
+constexpr size_t kOzSmem = (size_t)kOzABytes + kOzBBytes + kOzStageBytes + 2 * sizeof(double) * kOzSideDoubles + 128;
 
 // byte offset of element (row r, k) of an R-row int8 operand in the canonical
 // K-major layout: core matrix (row group r/8, K chunk k/16) of 8 rows x 16
@@ -141,45 +153,55 @@ __device__ __forceinline__ OzEntry oz_entry(const OzBatch& b, int e) {
 }
 
 #if defined(__CUDA_ARCH__)
-// S32 accumulator, signed int8 A and B, both K-major, N = 32, M = 128
-constexpr uint32_t kOzIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kOzN >> 3) << 17) |
-                              ((uint32_t)(kOzM >> 4) << 24);
+// S32 accumulator, signed int8 A and B, both K-major, M = 128, N as given
+__host__ __device__ constexpr uint32_t oz_idesc(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kOzM >> 4) << 24);
+}
 
-__device__ __forceinline__ void oz_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void oz_mma(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(tmem),
-      "l"(a), "l"(b), "r"(kOzIdesc), "r"(acc), "r"(0u));
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u));
 }
 
-__device__ __forceinline__ void oz_ld32(uint32_t taddr, int* v) {
-  uint32_t r[32];
+__device__ __forceinline__ void oz_ld16(uint32_t taddr, uint32_t* r) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-#pragma unroll
-  for (int j = 0; j < 32; ++j) v[j] = (int)r[j];
 }
 
 __device__ __forceinline__ void oz_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void oz_bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   tc_smem(dst)),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void oz_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
 }
 #endif
 
 __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(OzBatch b, int* __restrict__ err) {
 #if defined(__CUDA_ARCH__)
   extern __shared__ __align__(1024) unsigned char osm[];
-  unsigned char* sA = osm;
-  unsigned char* sB = osm + kOzABytes;
-  double* side = reinterpret_cast<double*>(osm + kOzABytes + 2 * kOzBBytes);
+  unsigned char* sA = osm;                                     // 8 A slices
+  unsigned char* sB = osm + kOzABytes;                         // stacked B slices
+  double* stage = reinterpret_cast<double*>(sB + kOzBBytes);   // staged FP64 tile, row k at 32 k
+  double* side = stage + kOzStageRows * kOzN;                  // two tile buffers
   uint64_t* bars = reinterpret_cast<uint64_t*>(side + 2 * kOzSideDoubles);
-  // bars: 0,1 full (B slices ready); 2,3 mma done; 4,5 epilogue done; 6 A loaded
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 8);
+  // bars: 0,1 full (B slices + side data of tile parity); 2,3 mma done; 4,5
+  // epilogue done; 6 A loaded; 7 staged tile ready; 8 staging released;
+  // 9 partial maxima exchanged
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 10);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto bar = [&](int i) { return tc_smem(&bars[i]); };
@@ -191,6 +213,9 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(OzBatch b, int* __re
     mbar_init(bar(4), 32 * kOzEpiWarps);
     mbar_init(bar(5), 32 * kOzEpiWarps);
     mbar_init(bar(6), 1);
+    mbar_init(bar(7), 1);
+    mbar_init(bar(8), 32 * kOzConvWarps);
+    mbar_init(bar(9), 32 * kOzConvWarps);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -216,68 +241,81 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(OzBatch b, int* __re
 
   if (warp < kOzConvWarps) {
     // ---------------------------------------------------------------- converters
-    // warp w: tile columns 8w..8w+7, lane = (column c = lane % 8, K quarter
-    // kq = lane / 8 holding rows 32 kq..32 kq+31); column maxima and the
-    // extra row's dot products reduce over the 4 lanes of a column by shuffles
-    const int c = lane & 7, kq = lane >> 3, k0 = 32 * kq, n = 8 * warp + c;
+    const int n = lane, k0 = 16 * warp;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
-      bool ok = i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1);
+      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
+      const OzEntry E = oz_entry(b, e);
+      const int kt = E.K < kOzK ? E.K : kOzK;
+      const bool cv = n0 + n < b.N;
+      bool ok = mbar_wait(bar(7), i & 1);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
       }
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
-      const OzEntry E = oz_entry(b, e);
-      const int kt = E.K < kOzK ? E.K : kOzK;
-      const int col = n0 + n;
-      const bool cv = col < b.N;
-      double v[32];
+      double v[16];
 #pragma unroll
-      for (int j = 0; j < 32; ++j)
-        v[j] = (cv && k0 + j < kt) ? __ldg(E.B + (size_t)(k0 + j) * b.ldb + col) : 0.0;
+      for (int j = 0; j < 16; ++j) v[j] = (cv && k0 + j < kt) ? stage[(k0 + j) * kOzN + n] : 0.0;
+      const double bx = (E.K > kOzK && cv) ? stage[kOzK * kOzN + n] : 0.0;
+      oz_arrive(bar(8));  // staging may be refilled
       double* sd = side + buf * kOzSideDoubles;
-      if (kq == 0) sd[kOzSideBx + n] = (E.K > kOzK && cv) ? __ldg(E.B + (size_t)kOzK * b.ldb + col) : 0.0;
+      double mx = 0.0, dot = 0.0;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) mx = fmax(mx, fabs(v[j]));
       if (E.M > kOzM) {
-        double dot = 0.0;
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
+        for (int j = 0; j < 16; ++j)
           if (k0 + j < kt) dot = fma(__ldg(E.xrow + k0 + j), v[j], dot);
-        dot += __shfl_xor_sync(0xffffffffu, dot, 8);
-        dot += __shfl_xor_sync(0xffffffffu, dot, 16);
-        if (kq == 0) sd[kOzSideDot + n] = dot;
       }
-      double mx = 0.0;
+      sd[kOzSidePMax + warp * kOzN + n] = mx;
+      sd[kOzSidePDot + warp * kOzN + n] = dot;
+      oz_arrive(bar(9));
+      ok = mbar_wait(bar(9), i & 1);
+      if (!__all_sync(0xffffffffu, ok)) {
+        fail_now();
+        break;
+      }
+      double cm = sd[kOzSidePMax + n];
 #pragma unroll
-      for (int j = 0; j < 32; ++j) mx = fmax(mx, fabs(v[j]));
-      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 8));
-      mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, 16));
-      const int eb = oz_exponent(mx);
-      if (kq == 0) sd[kOzSideScale + n] = oz_pow2(eb);
+      for (int w = 1; w < kOzConvWarps; ++w) cm = fmax(cm, sd[kOzSidePMax + w * kOzN + n]);
+      const int eb = oz_exponent(cm);
       const double sc = oz_pow2(56 - eb);
-      unsigned char* dst = sB + buf * kOzBBytes;
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
+      uint32_t wd[kOzSlices][4];
+      {
         double xs[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) xs[j] = v[16 * h + j] * sc;
-        uint32_t w[kOzSlices][4];
-        oz_pack16(xs, w);
-        const int off = oz_offset(kOzN, n, k0 + 16 * h);
+        for (int j = 0; j < 16; ++j) xs[j] = v[j] * sc;
+        oz_pack16(xs, wd);
+      }
+      // the B slices are free once the previous tile's MMAs completed; the
+      // side buffer once the epilogue of the tile two back is done
+      ok = (i < 1 || mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1)) &&
+           (i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1));
+      if (!__all_sync(0xffffffffu, ok)) {
+        fail_now();
+        break;
+      }
 #pragma unroll
-        for (int q = 0; q < kOzSlices; ++q)
-          *reinterpret_cast<uint4*>(dst + q * kOzBSlice + off) = make_uint4(w[q][0], w[q][1], w[q][2], w[q][3]);
+      for (int q = 0; q < kOzSlices; ++q)
+        *reinterpret_cast<uint4*>(sB + oz_offset(kOzBRows, q * kOzN + n, k0)) =
+            make_uint4(wd[q][0], wd[q][1], wd[q][2], wd[q][3]);
+      if (warp == 0) {
+        double x = sd[kOzSidePDot + n];
+#pragma unroll
+        for (int w = 1; w < kOzConvWarps; ++w) x += sd[kOzSidePDot + w * kOzN + n];
+        sd[kOzSideDot + n] = x;
+        sd[kOzSideScale + n] = oz_pow2(eb);
+        sd[kOzSideBx + n] = bx;
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       oz_arrive(bar(buf));
     }
   } else if (warp < kOzConvWarps + kOzEpiWarps) {
     // ----------------------------------------------------------------- epilogue
-    const int quad = warp & 3, row = 32 * quad + lane;
+    const int ew = warp - kOzConvWarps, quad = warp & 3, half = ew >> 2;
+    const int row = 32 * quad + lane, c0 = 16 * half;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
-      // the full wait is already complete (it only orders the converters'
-      // side data before the reads below)
       const bool ok = mbar_wait(bar(2 + buf), (i >> 1) & 1) && mbar_wait(bar(buf), (i >> 1) & 1);
       if (!__all_sync(0xffffffffu, ok)) {  // tcgen05.ld below needs the whole warp
         fail_now();
@@ -286,21 +324,22 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(OzBatch b, int* __re
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
       const OzEntry E = oz_entry(b, e);
-      const uint32_t tbase = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * kOzDiags * kOzN);
-      double r[32];
-      {
-        int acc[32];
-        oz_ld32(tbase + (uint32_t)((kOzDiags - 1) * kOzN), acc);
+      const uint32_t tbase =
+          tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * kOzDiags * kOzN) + (uint32_t)c0;
+      double r[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) r[j] = 0.0;
+#pragma unroll
+      for (int d = kOzDiags - 1; d >= 1; d -= 2) {  // two loads per wait, highest diagonal first
+        uint32_t hi[16], lo[16];
+        oz_ld16(tbase + (uint32_t)(d * kOzN), hi);
+        oz_ld16(tbase + (uint32_t)((d - 1) * kOzN), lo);
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < 32; ++j) r[j] = (double)acc[j];
-      }
-      for (int d = kOzDiags - 2; d >= 0; --d) {
-        int acc[32];
-        oz_ld32(tbase + (uint32_t)(d * kOzN), acc);
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 32; ++j) r[j] = fma(r[j], 0.0078125, (double)acc[j]);
+        for (int j = 0; j < 16; ++j) {
+          r[j] = fma(r[j], 0.0078125, (double)(int)hi[j]);
+          r[j] = fma(r[j], 0.0078125, (double)(int)lo[j]);
+        }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       const double* sd = side + buf * kOzSideDoubles;
@@ -308,84 +347,96 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(OzBatch b, int* __re
       if (row < mt) {
         const double sa = __ldg(E.row_scale + row);
         const double xc = E.K > kOzK ? __ldg(E.xcol + row) : 0.0;
-        double* out = E.C + (size_t)row * b.ldc + n0;
-        if (n0 + kOzN <= b.N) {
+        double* out = E.C + (size_t)row * b.ldc + n0 + c0;
+        if (n0 + c0 + 16 <= b.N) {
 #pragma unroll
-          for (int j = 0; j < 32; j += 2) {
-            const double o0 = fma(xc, sd[kOzSideBx + j], r[j] * sa * sd[kOzSideScale + j]);
-            const double o1 = fma(xc, sd[kOzSideBx + j + 1], r[j + 1] * sa * sd[kOzSideScale + j + 1]);
+          for (int j = 0; j < 16; j += 2) {
+            const double o0 = fma(xc, sd[kOzSideBx + c0 + j], r[j] * sa * sd[kOzSideScale + c0 + j]);
+            const double o1 = fma(xc, sd[kOzSideBx + c0 + j + 1], r[j + 1] * sa * sd[kOzSideScale + c0 + j + 1]);
             *reinterpret_cast<double2*>(out + j) = make_double2(o0, o1);
           }
         } else {
 #pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (n0 + j < b.N) out[j] = fma(xc, sd[kOzSideBx + j], r[j] * sa * sd[kOzSideScale + j]);
+          for (int j = 0; j < 16; ++j)
+            if (n0 + c0 + j < b.N) out[j] = fma(xc, sd[kOzSideBx + c0 + j], r[j] * sa * sd[kOzSideScale + c0 + j]);
         }
       }
-      if (E.M > kOzM && quad == 0 && n0 + lane < b.N) {
-        E.C[(size_t)kOzM * b.ldc + n0 + lane] = sd[kOzSideDot + lane];
-      }
+      if (E.M > kOzM && ew == 0 && n0 + lane < b.N) E.C[(size_t)kOzM * b.ldc + n0 + lane] = sd[kOzSideDot + lane];
       oz_arrive(bar(4 + buf));
     }
-  } else if (lane == 0) {
+  } else if (warp == kOzIssuerWarp) {
     // ------------------------------------------------------------------- issuer
-    const int8_t* cur = nullptr;
-    int a_loads = 0, issued = 0;
-    for (int i = 0; i < nt && !*abort_flag; ++i) {
-      const int buf = i & 1;
-      const int t = t_begin + i, e = t / tiles_n;
-      const OzEntry E = oz_entry(b, e);
-      if (E.a != cur) {
-        // the MMAs of the previous tile read the resident slices: let them finish
-        if (i > 0 && !mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1)) {
+    if (lane == 0) {
+      const int8_t* cur = nullptr;
+      int a_loads = 0, issued = 0;
+      for (int i = 0; i < nt && !*abort_flag; ++i) {
+        const int buf = i & 1;
+        const int t = t_begin + i, e = t / tiles_n;
+        const OzEntry E = oz_entry(b, e);
+        if (E.a != cur) {
+          // the MMAs of the previous tile read the resident slices: let them finish
+          if (i > 0 && !mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1)) {
+            fail_now();
+            break;
+          }
+          oz_expect_tx(bar(6), (uint32_t)kOzABytes);
+          for (int h = 0; h < 4; ++h)
+            oz_bulk_g2s(sA + h * (kOzABytes / 4), E.a + h * (kOzABytes / 4), (uint32_t)(kOzABytes / 4), bar(6));
+          if (!mbar_wait(bar(6), a_loads & 1)) {
+            fail_now();
+            break;
+          }
+          ++a_loads;
+          cur = E.a;
+        }
+        if (!mbar_wait(bar(buf), (i >> 1) & 1)) {
           fail_now();
           break;
         }
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar(6)),
-                     "r"((uint32_t)kOzABytes)
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        // descriptors at slice 1 / K step 0; the start-address field (bits
+        // 0-13, address / 16) of every other operand tile is a constant away
+        constexpr uint32_t lbo_a = kOzM * 16, lbo_b = kOzBRows * 16;
+        const uint64_t da0 = tc05_desc(tc_smem(sA), lbo_a, 128);
+        const uint64_t db0 = tc05_desc(tc_smem(sB), lbo_b, 128);
+        const uint32_t acc0 = tmem + (uint32_t)(buf * kOzDiags * kOzN);
+#pragma unroll
+        for (int ks = 0; ks < kOzK / 32; ++ks)
+#pragma unroll
+          for (int p = 1; p <= kOzSlices; ++p)
+            oz_mma(acc0 + (uint32_t)((p - 1) * kOzN),
+                   da0 + (uint64_t)((uint32_t)((p - 1) * kOzASlice + 2 * ks * lbo_a) >> 4),
+                   db0 + (uint64_t)((uint32_t)(2 * ks * lbo_b) >> 4), oz_idesc(kOzN * (kOzSlices + 1 - p)),
+                   (p == 1 && ks == 0) ? 0u : 1u);
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         bar(2 + buf))
                      : "memory");
-        for (int h = 0; h < 4; ++h)
-          asm volatile(
-              "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                  tc_smem(sA + h * (kOzABytes / 4))),
-              "l"(E.a + h * (kOzABytes / 4)), "r"((uint32_t)(kOzABytes / 4)), "r"(bar(6))
-              : "memory");
-        if (!mbar_wait(bar(6), a_loads & 1)) {
-          fail_now();
-          break;
-        }
-        ++a_loads;
-        cur = E.a;
+        issued = i + 1;
       }
-      if (!mbar_wait(bar(buf), (i >> 1) & 1)) {
+      // no MMA may still run when the CTA frees its tensor memory
+      if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1)) fail_now();
+    }
+  } else {
+    // ----------------------------------------------------------------- producer
+    for (int i = 0; i < nt && !*abort_flag; ++i) {
+      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
+      const OzEntry E = oz_entry(b, e);
+      const int kt = E.K < kOzK ? E.K : kOzK;
+      const int rows = kt + (E.K > kOzK ? 1 : 0);
+      const int ncols = b.N - n0 < kOzN ? b.N - n0 : kOzN;  // even: N is even
+      const bool ok = i < 1 || mbar_wait(bar(8), (i - 1) & 1);
+      if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
       }
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t a0 = tc_smem(sA), b0 = tc_smem(sB + buf * kOzBBytes);
-      const uint32_t acc0 = tmem + (uint32_t)(buf * kOzDiags * kOzN);
-      constexpr uint32_t lbo_a = kOzM * 16, lbo_b = kOzN * 16;
-      for (int d = 0; d < kOzDiags; ++d) {  // diagonal p + q = d + 2
-        uint32_t accumulate = 0u;
-        for (int p = 1; p <= kOzSlices; ++p) {
-          const int q = d + 2 - p;
-          if (q < 1 || q > kOzSlices) continue;
-#pragma unroll
-          for (int ks = 0; ks < kOzK / 32; ++ks) {
-            const uint64_t da = tc05_desc(a0 + (p - 1) * kOzASlice + 2 * ks * lbo_a, lbo_a, 128);
-            const uint64_t db = tc05_desc(b0 + (q - 1) * kOzBSlice + 2 * ks * lbo_b, lbo_b, 128);
-            oz_mma(acc0 + (uint32_t)(d * kOzN), da, db, accumulate);
-            accumulate = 1u;
-          }
-        }
+      if (lane == 0) oz_expect_tx(bar(7), (uint32_t)(rows * ncols * 8));
+      __syncwarp();
+      for (int k = lane; k < rows; k += 32) {
+        const int srow = k < kt ? k : kOzK;  // the K = 129 extra row lands in staging row 128
+        oz_bulk_g2s(stage + srow * kOzN, E.B + (size_t)(k < kt ? k : kOzK) * b.ldb + n0, (uint32_t)(ncols * 8),
+                    bar(7));
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                       bar(2 + buf))
-                   : "memory");
-      issued = i + 1;
     }
-    // no MMA may still run when the CTA frees its tensor memory
-    if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1)) fail_now();
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();

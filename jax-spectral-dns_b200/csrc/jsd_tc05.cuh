@@ -213,15 +213,16 @@ __global__ void __launch_bounds__(128, 1) k_tc05_dfield(const float* __restrict_
     __syncthreads();
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const uint32_t ah = tc_smem(sAh), al = tc_smem(sAl), bh = tc_smem(sBh), bl = tc_smem(sBl);
-      for (int s = 0; s < ksteps; ++s) {
-        const uint64_t dah = tc05_desc(ah + 2 * s * lbo_a, lbo_a, 128);
-        const uint64_t dal = tc05_desc(al + 2 * s * lbo_a, lbo_a, 128);
-        const uint64_t dbh = tc05_desc(bh + 2 * s * lbo_b, lbo_b, 128);
-        const uint64_t dbl = tc05_desc(bl + 2 * s * lbo_b, lbo_b, 128);
-        tc_mma(tmem, dah, dbh, s > 0 ? 1u : 0u);
-        tc_mma(tmem, dah, dbl, 1u);
-        tc_mma(tmem, dal, dbh, 1u);
+      // K step s moves the start-address field (address / 16) by a constant
+      const uint64_t dah = tc05_desc(tc_smem(sAh), lbo_a, 128), dal = tc05_desc(tc_smem(sAl), lbo_a, 128);
+      const uint64_t dbh = tc05_desc(tc_smem(sBh), lbo_b, 128), dbl = tc05_desc(tc_smem(sBl), lbo_b, 128);
+#pragma unroll
+      for (int s = 0; s < kTcKp / 8; ++s) {
+        if (s >= ksteps) break;
+        const uint64_t oa = (2u * s * lbo_a) >> 4, ob = (2u * s * lbo_b) >> 4;
+        tc_mma(tmem, dah + oa, dbh + ob, s > 0 ? 1u : 0u);
+        tc_mma(tmem, dah + oa, dbl + ob, 1u);
+        tc_mma(tmem, dal + oa, dbh + ob, 1u);
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_m)
                    : "memory");

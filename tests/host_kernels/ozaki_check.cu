@@ -1,7 +1,8 @@
 // Host-side check of the Ozaki int8 product (jsd_ozaki.cuh): packs A with
-// oz_pack_a and 32-column tiles of B the way the converter warps do, emulates
-// the tensor-core products by reading both operands back through their
-// canonical-layout offsets (int32 accumulation per diagonal), combines like
+// oz_pack_a and 32-column tiles of B the way the converter warps do (slices
+// stacked into one 256-row operand), emulates the tensor-core products by
+// reading both operands back through their canonical-layout offsets (int32
+// accumulation per diagonal), combines like
 // the epilogue (FP64 extras for row 128 / column 128 included) and compares
 // with a long-double product. Prints per case: M K error/(|A||B|) max,
 // relative Frobenius error, and the same two for a plain FP64 product.
@@ -43,14 +44,13 @@ static void run_case(int M, int K, int N, unsigned long long seed) {
       }
       bx[lane] = (K > kOzK && col < N) ? B[(size_t)kOzK * N + col] : 0.0;
       double dot = 0.0;
-      if (M > kOzM) {  // 4 lanes of 32 rows each, then the shuffle butterfly (xor 8, xor 16)
-        double part[4];
-        for (int w = 0; w < 4; ++w) {
-          part[w] = 0.0;
-          for (int j = 0; j < 32; ++j)
-            if (32 * w + j < kt) part[w] = std::fma(pa.xrow[32 * w + j], v[32 * w + j], part[w]);
+      if (M > kOzM) {  // 8 converter warps of 16 rows each, partials summed in warp order
+        for (int w = 0; w < kOzConvWarps; ++w) {
+          double part = 0.0;
+          for (int j = 0; j < 16; ++j)
+            if (16 * w + j < kt) part = std::fma(pa.xrow[16 * w + j], v[16 * w + j], part);
+          dot = w == 0 ? part : dot + part;
         }
-        dot = (part[0] + part[1]) + (part[2] + part[3]);
       }
       xdot[lane] = dot;
       const int eb = oz_exponent(mx);
@@ -61,9 +61,9 @@ static void run_case(int M, int K, int N, unsigned long long seed) {
         for (int j = 0; j < 16; ++j) xs[j] = v[k0 + j] * sc;
         uint32_t w[kOzSlices][4];
         oz_pack16(xs, w);
-        const int off = oz_offset(kOzN, lane, k0);
         for (int q = 0; q < kOzSlices; ++q)
-          for (int j = 0; j < 16; ++j) bs[(size_t)q * kOzBSlice + off + j] = (unsigned char)((w[q][j >> 2] >> (8 * (j & 3))) & 0xFFu);
+          for (int j = 0; j < 16; ++j)
+            bs[oz_offset(kOzBRows, q * kOzN + lane, k0) + j] = (unsigned char)((w[q][j >> 2] >> (8 * (j & 3))) & 0xFFu);
       }
     }
     for (int r = 0; r < mt; ++r)
@@ -76,7 +76,7 @@ static void run_case(int M, int K, int N, unsigned long long seed) {
             long long s = 0;
             for (int k = 0; k < kOzK; ++k)
               s += (long long)pa.slices[(size_t)(p - 1) * kOzASlice + oz_offset(kOzM, r, k)] *
-                   (long long)(signed char)bs[(size_t)(q - 1) * kOzBSlice + oz_offset(kOzN, lane, k)];
+                   (long long)(signed char)bs[oz_offset(kOzBRows, (q - 1) * kOzN + lane, k)];
             acc[d] += s;
           }
         for (int d = 0; d < kOzDiags; ++d)
