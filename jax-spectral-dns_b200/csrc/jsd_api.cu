@@ -180,6 +180,13 @@ struct jsd_plan {
   const double* oz_src[4] = {};
   bool oz_ready = false;
   int eig_kernel[3] = {0, 0, 0};  // per GemmSite (eigen sites): 0 DMMA, 1 Ozaki int8
+  struct OzMap {
+    const double* B = nullptr;
+    int N = 0, K = 0, ldb = 0;
+    CUtensorMap map;
+  };
+  OzMap oz_maps[16];  // tensor maps of the B operands seen so far (round robin)
+  int oz_map_next = 0;
   float eig_ms[3][2] = {};        // autotuner timings per eigen site: DMMA (best tile), Ozaki
   double* re_run = nullptr;     // Reynolds number per run of a batch (device)
   double* lr_ns = nullptr;      // Linv_ns R_ns per run and stage (row-parallel mean-flow update)
@@ -384,9 +391,57 @@ int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, GemmSite site,
   return launch_gemm_cfg(p, b, max_m, p->gemm_cfg[site], s);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (null when
+// the driver does not provide it)
+using EncodeTiledFn = decltype(&cuTensorMapEncodeTiled);
+EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+  });
+  return fn;
+}
+
+// 2-D tensor map of B (N doubles per row, min(K, 128) rows, row stride ldb),
+// box 32 x 128, zero fill outside; cached per plan
+int oz_tensor_map(jsd_plan* p, const double* B, int N, int K, int ldb, CUtensorMap* out) {
+  for (const auto& m : p->oz_maps)
+    if (m.B == B && m.N == N && m.K == K && m.ldb == ldb) {
+      *out = m.map;
+      return 0;
+    }
+  EncodeTiledFn enc = tensor_map_encoder();
+  if (!enc) return fail(JSD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
+  auto& slot = p->oz_maps[p->oz_map_next];
+  p->oz_map_next = (p->oz_map_next + 1) % 16;
+  const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)(K < kOzK ? K : kOzK)};
+  const cuuint64_t strides[1] = {(cuuint64_t)ldb * sizeof(double)};
+  const cuuint32_t box[2] = {(cuuint32_t)kOzN, (cuuint32_t)kOzK};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(&slot.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(B), dims, strides, box,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    slot.B = nullptr;
+    return fail(JSD_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+  }
+  slot.B = B;
+  slot.N = N;
+  slot.K = K;
+  slot.ldb = ldb;
+  *out = slot.map;
+  return 0;
+}
+
 // The eigenbasis products of a batch on the int8 tensor cores (k_oz8_gemm);
 // every entry's operator must be one of the packed ones.
-int launch_ozaki(const jsd_plan* p, const GemmBatch& b, cudaStream_t s) {
+int launch_ozaki(const jsd_plan* pc, const GemmBatch& b, cudaStream_t s) {
+  jsd_plan* p = const_cast<jsd_plan*>(pc);  // the tensor-map cache
   OzBatch o;
   memset(&o, 0, sizeof(o));
   o.N = b.N;
@@ -397,6 +452,10 @@ int launch_ozaki(const jsd_plan* p, const GemmBatch& b, cudaStream_t s) {
     int k = 0;
     while (k < 4 && p->oz_src[k] != g.A) ++k;
     if (k == 4 || g.alpha != 1.0) return fail(JSD_ERR_STATE, "operator has no int8 slice pack");
+    if (reinterpret_cast<uintptr_t>(g.B) % 16 || b.ldb % 2 || b.N % 2)
+      return fail(JSD_ERR_STATE, "int8 eigenbasis product needs 16-byte aligned rows");
+    int rc = oz_tensor_map(p, g.B, b.N, g.K, b.ldb, &o.map[o.count]);
+    if (rc) return rc;
     OzEntry& e = o.e[o.count++];
     e.a = p->oz_a[k];
     e.row_scale = p->oz_rs[k];
@@ -1300,7 +1359,7 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
     }
     // (the epilogue's pair stores need 16-byte aligned rows: every output is a
     // double2 field or an even offset into one, with an even row stride 2 nk nb)
-    p->oz_ready = true;
+    p->oz_ready = tensor_map_encoder() != nullptr;
   }
   JSD_TRY(upload(p, &p->lam, d->lam, ni));
   JSD_TRY(upload(p, &p->sgn, d->sgn, ni));

@@ -27,8 +27,9 @@
 //
 // One persistent CTA of 18 warps per SM, each CTA a contiguous range of
 // 32-column tiles:
-//   * warp 17 (producer): bulk-copies (cp.async.bulk, mbarrier completion) the
-//     next tile's FP64 rows of B into a staging buffer;
+//   * warp 17 (producer): loads the next tile's 128 x 32 FP64 block of B into
+//     a staging buffer with one 2-D TMA copy (cp.async.bulk.tensor, mbarrier
+//     completion; rows past K and columns past N arrive as zeros);
 //   * warps 0-7 (converters, warp w = rows 16w..16w+15, lane = column): read
 //     the staged tile, release the staging buffer, exchange partial column
 //     maxima through an mbarrier, cut the 16-row chunk into the 8 slices and
@@ -43,6 +44,8 @@
 // error flag, every role stops at its next tile, the issuer waits (bounded) for
 // its last MMAs, and the CTA frees its TMEM and returns.
 #pragma once
+
+#include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime's driver entry point)
 
 #include <cmath>
 #include <cstdint>
@@ -105,23 +108,31 @@ __host__ __device__ __forceinline__ int oz_exponent(double m) {
 
 // Slices of 16 values already scaled by 2^(56 - e) (|xs| < 2^56), packed
 // little-endian: byte j of w[q] (4 words = 16 bytes) is slice q + 1 of xs[j].
+// Sign-magnitude digits (a small value has small digits, so the dropped
+// low-order products stay small): the 7-bit fields of trunc(|xs|), negated
+// for negative xs. Four elements share a word: their magnitude bytes are
+// packed first and the bytes of the negative ones negated together,
+// (0x80808080 - W) ^ 0x80808080 being the byte-wise two's complement of bytes
+// <= 127 without carries between bytes.
 __host__ __device__ __forceinline__ void oz_pack16(const double* xs, uint32_t (*w)[4]) {
 #pragma unroll
-  for (int q = 0; q < kOzSlices; ++q)
+  for (int g = 0; g < 4; ++g) {
+    unsigned long long a[4];
+    uint32_t neg = 0u;
 #pragma unroll
-    for (int t = 0; t < 4; ++t) w[q][t] = 0u;
-#pragma unroll
-  for (int j = 0; j < 16; ++j) {
-    const long long m = (long long)xs[j];  // truncation toward zero, exact below 2^56
-    const unsigned long long a = m < 0 ? (unsigned long long)(-m) : (unsigned long long)m;
-    const uint32_t hi = (uint32_t)(a >> 28), lo = (uint32_t)(a & 0xFFFFFFFull);
-    const uint32_t neg = m < 0 ? 0xFFu : 0u;
+    for (int k = 0; k < 4; ++k) {
+      const double x = xs[4 * g + k];
+      a[k] = (unsigned long long)(x < 0.0 ? -x : x);  // truncation toward zero, exact below 2^56
+      neg |= (x < 0.0 ? 0xFFu : 0u) << (8 * k);
+    }
 #pragma unroll
     for (int q = 0; q < kOzSlices; ++q) {
-      const uint32_t src = q < 4 ? hi : lo;
-      const uint32_t v = (src >> (21 - 7 * (q & 3))) & 127u;
-      const uint32_t byte = ((v ^ neg) + (neg & 1u)) & 0xFFu;  // two's complement of -v when negative
-      w[q][j >> 2] |= byte << (8 * (j & 3));
+      const int sh = 49 - 7 * q;  // lowest bit of slice q + 1
+      uint32_t W = 0u;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) W |= (uint32_t)((a[k] >> sh) & 127u) << (8 * k);
+      const uint32_t nW = (0x80808080u - W) ^ 0x80808080u;
+      w[q][g] = W ^ ((W ^ nW) & neg);
     }
   }
 }
@@ -136,7 +147,10 @@ struct OzEntry {
   int M, K;
 };
 
+// map[i]: 2-D tensor map of entry i's B (inner N doubles, outer min(K, 128)
+// rows, row stride ldb), box 32 x 128: one TMA load per tile
 struct OzBatch {
+  CUtensorMap map[kGemmMaxBatch];
   OzEntry e[kGemmMaxBatch];
   int count;
   int N, ldb, ldc;
@@ -190,7 +204,8 @@ __device__ __forceinline__ void oz_expect_tx(uint32_t bar, uint32_t bytes) {
 }
 #endif
 
-__global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(OzBatch b, int* __restrict__ err) {
+__global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constant__ OzBatch b,
+                                                             int* __restrict__ err) {
 #if defined(__CUDA_ARCH__)
   extern __shared__ __align__(1024) unsigned char osm[];
   unsigned char* sA = osm;                                     // 8 A slices
@@ -421,20 +436,23 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(OzBatch b, int* __re
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
       const OzEntry E = oz_entry(b, e);
-      const int kt = E.K < kOzK ? E.K : kOzK;
-      const int rows = kt + (E.K > kOzK ? 1 : 0);
       const int ncols = b.N - n0 < kOzN ? b.N - n0 : kOzN;  // even: N is even
       const bool ok = i < 1 || mbar_wait(bar(8), (i - 1) & 1);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
       }
-      if (lane == 0) oz_expect_tx(bar(7), (uint32_t)(rows * ncols * 8));
-      __syncwarp();
-      for (int k = lane; k < rows; k += 32) {
-        const int srow = k < kt ? k : kOzK;  // the K = 129 extra row lands in staging row 128
-        oz_bulk_g2s(stage + srow * kOzN, E.B + (size_t)(k < kt ? k : kOzK) * b.ldb + n0, (uint32_t)(ncols * 8),
-                    bar(7));
+      if (lane == 0) {
+        // rows >= min(K, 128) and columns >= N lie outside the tensor map and arrive as zeros
+        const bool extra = E.K > kOzK;
+        oz_expect_tx(bar(7), (uint32_t)(kOzK * kOzN * 8 + (extra ? ncols * 8 : 0)));
+        asm volatile(
+            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+            "[%4];\n" ::"r"(tc_smem(stage)),
+            "l"(&b.map[e]), "r"(n0), "r"(0), "r"(bar(7))
+            : "memory");
+        if (extra)  // the K = 129 row, staged as row 128
+          oz_bulk_g2s(stage + kOzK * kOzN, E.B + (size_t)kOzK * b.ldb + n0, (uint32_t)(ncols * 8), bar(7));
       }
     }
   }
