@@ -25,19 +25,19 @@
 // diagonal p + q: 32 MMAs of N = 32..256 per tile instead of 36 x 4 narrow
 // ones, so the operands are read from shared memory once per wide product.
 //
-// One persistent CTA of 18 warps per SM, each CTA a contiguous range of
+// One persistent CTA of 26 warps per SM, each CTA a contiguous range of
 // 32-column tiles:
-//   * warp 17 (producer): loads the next tile's 128 x 32 FP64 block of B into
+//   * warp 25 (producer): loads the next tile's 128 x 32 FP64 block of B into
 //     a staging buffer with one 2-D TMA copy (cp.async.bulk.tensor, mbarrier
 //     completion; rows past K and columns past N arrive as zeros);
-//   * warps 0-7 (converters, warp w = rows 16w..16w+15, lane = column): read
+//   * warps 0-15 (converters, warp w = rows 8w..8w+7, lane = column): read
 //     the staged tile, release the staging buffer, exchange partial column
-//     maxima through an mbarrier, cut the 16-row chunk into the 8 slices and
+//     maxima through an mbarrier, cut the 8-row chunk into the 8 slices and
 //     store them in the canonical K-major core-matrix layout;
-//   * warp 16 (issuer): keeps A's 8 slices resident (bulk copy, reloaded when
+//   * warp 24 (issuer): keeps A's 8 slices resident (bulk copy, reloaded when
 //     the operator changes), issues the 32 MMAs (kind::i8, M = 128) into one of
 //     two accumulator sets of 8 x 32 TMEM columns and commits to an mbarrier;
-//   * warps 8-15 (epilogue, TMEM lane quadrant = warp % 4 = row block, half of
+//   * warps 16-23 (epilogue, TMEM lane quadrant = warp % 4 = row block, half of
 //     the columns each): read the 8 accumulators (tcgen05.ld, two per wait),
 //     combine, scale, add the FP64 extras and store.
 // Every mbarrier wait has an iteration limit; on expiry the kernel raises the
@@ -67,9 +67,10 @@ constexpr int kOzBBytes = kOzBRows * kOzK;           // 32768
 constexpr int kOzStageRows = kOzK + 1;               // staged FP64 rows (row 128: the K = 129 extra)
 constexpr int kOzStageBytes = kOzStageRows * kOzN * 8;  // 33024
 constexpr int kOzTmemCols = 2 * kOzDiags * kOzN;     // 512: two accumulator sets
-constexpr int kOzConvWarps = 8, kOzEpiWarps = 8;
+constexpr int kOzConvWarps = 16, kOzEpiWarps = 8;
+constexpr int kOzConvRows = kOzK / kOzConvWarps;  // B rows per converter lane (8)
 constexpr int kOzIssuerWarp = kOzConvWarps + kOzEpiWarps, kOzProducerWarp = kOzIssuerWarp + 1;
-constexpr int kOzThreads = 32 * (kOzProducerWarp + 1);  // 576
+constexpr int kOzThreads = 32 * (kOzProducerWarp + 1);  // 832
 // side data per tile buffer (doubles): column scales, B row 128, extra-row
 // dot products (read by the epilogue), partial maxima and partial dots per
 // converter warp (exchanged among the converters)
@@ -106,17 +107,18 @@ __host__ __device__ __forceinline__ int oz_exponent(double m) {
   return e < -900 ? -900 : e;
 }
 
-// Slices of 16 values already scaled by 2^(56 - e) (|xs| < 2^56), packed
-// little-endian: byte j of w[q] (4 words = 16 bytes) is slice q + 1 of xs[j].
+// Slices of 4 G values already scaled by 2^(56 - e) (|xs| < 2^56), packed
+// little-endian: byte j of w[q] (G words) is slice q + 1 of xs[j].
 // Sign-magnitude digits (a small value has small digits, so the dropped
 // low-order products stay small): the 7-bit fields of trunc(|xs|), negated
 // for negative xs. Four elements share a word: their magnitude bytes are
 // packed first and the bytes of the negative ones negated together,
 // (0x80808080 - W) ^ 0x80808080 being the byte-wise two's complement of bytes
 // <= 127 without carries between bytes.
-__host__ __device__ __forceinline__ void oz_pack16(const double* xs, uint32_t (*w)[4]) {
+template <int G>
+__host__ __device__ __forceinline__ void oz_pack(const double* xs, uint32_t (*w)[G]) {
 #pragma unroll
-  for (int g = 0; g < 4; ++g) {
+  for (int g = 0; g < G; ++g) {
     unsigned long long a[4];
     uint32_t neg = 0u;
 #pragma unroll
@@ -256,7 +258,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
 
   if (warp < kOzConvWarps) {
     // ---------------------------------------------------------------- converters
-    const int n = lane, k0 = 16 * warp;
+    const int n = lane, k0 = kOzConvRows * warp;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
@@ -268,18 +270,18 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         fail_now();
         break;
       }
-      double v[16];
+      double v[kOzConvRows];
 #pragma unroll
-      for (int j = 0; j < 16; ++j) v[j] = (cv && k0 + j < kt) ? stage[(k0 + j) * kOzN + n] : 0.0;
+      for (int j = 0; j < kOzConvRows; ++j) v[j] = (cv && k0 + j < kt) ? stage[(k0 + j) * kOzN + n] : 0.0;
       const double bx = (E.K > kOzK && cv) ? stage[kOzK * kOzN + n] : 0.0;
       oz_arrive(bar(8));  // staging may be refilled
       double* sd = side + buf * kOzSideDoubles;
       double mx = 0.0, dot = 0.0;
 #pragma unroll
-      for (int j = 0; j < 16; ++j) mx = fmax(mx, fabs(v[j]));
+      for (int j = 0; j < kOzConvRows; ++j) mx = fmax(mx, fabs(v[j]));
       if (E.M > kOzM) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j)
+        for (int j = 0; j < kOzConvRows; ++j)
           if (k0 + j < kt) dot = fma(__ldg(E.xrow + k0 + j), v[j], dot);
       }
       sd[kOzSidePMax + warp * kOzN + n] = mx;
@@ -295,12 +297,12 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
       for (int w = 1; w < kOzConvWarps; ++w) cm = fmax(cm, sd[kOzSidePMax + w * kOzN + n]);
       const int eb = oz_exponent(cm);
       const double sc = oz_pow2(56 - eb);
-      uint32_t wd[kOzSlices][4];
+      uint32_t wd[kOzSlices][kOzConvRows / 4];
       {
-        double xs[16];
+        double xs[kOzConvRows];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) xs[j] = v[j] * sc;
-        oz_pack16(xs, wd);
+        for (int j = 0; j < kOzConvRows; ++j) xs[j] = v[j] * sc;
+        oz_pack<kOzConvRows / 4>(xs, wd);
       }
       // the B slices are free once the previous tile's MMAs completed; the
       // side buffer once the epilogue of the tile two back is done
@@ -310,10 +312,10 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         fail_now();
         break;
       }
+      static_assert(kOzConvRows == 8, "converter lanes store 8-byte halves of 16-byte core-matrix rows");
 #pragma unroll
       for (int q = 0; q < kOzSlices; ++q)
-        *reinterpret_cast<uint4*>(sB + oz_offset(kOzBRows, q * kOzN + n, k0)) =
-            make_uint4(wd[q][0], wd[q][1], wd[q][2], wd[q][3]);
+        *reinterpret_cast<uint2*>(sB + oz_offset(kOzBRows, q * kOzN + n, k0)) = make_uint2(wd[q][0], wd[q][1]);
       if (warp == 0) {
         double x = sd[kOzSidePDot + n];
 #pragma unroll
@@ -491,7 +493,7 @@ inline void oz_pack_a(const double* A, int M, int K, int lda, OzPackA& out) {
       double xs[16];
       for (int j = 0; j < 16; ++j) xs[j] = (k0 + j < kt) ? A[(size_t)r * lda + k0 + j] * sc : 0.0;
       uint32_t w[kOzSlices][4];
-      oz_pack16(xs, w);
+      oz_pack<4>(xs, w);
       for (int q = 0; q < kOzSlices; ++q)
         for (int j = 0; j < 16; ++j)
           out.slices[(size_t)q * kOzASlice + oz_offset(kOzM, r, k0 + j)] =

@@ -44,11 +44,11 @@ static void run_case(int M, int K, int N, unsigned long long seed) {
       }
       bx[lane] = (K > kOzK && col < N) ? B[(size_t)kOzK * N + col] : 0.0;
       double dot = 0.0;
-      if (M > kOzM) {  // 8 converter warps of 16 rows each, partials summed in warp order
+      if (M > kOzM) {  // converter warps of kOzConvRows rows each, partials summed in warp order
         for (int w = 0; w < kOzConvWarps; ++w) {
           double part = 0.0;
-          for (int j = 0; j < 16; ++j)
-            if (16 * w + j < kt) part = std::fma(pa.xrow[16 * w + j], v[16 * w + j], part);
+          for (int j = 0; j < kOzConvRows; ++j)
+            if (kOzConvRows * w + j < kt) part = std::fma(pa.xrow[kOzConvRows * w + j], v[kOzConvRows * w + j], part);
           dot = w == 0 ? part : dot + part;
         }
       }
@@ -60,7 +60,7 @@ static void run_case(int M, int K, int N, unsigned long long seed) {
         double xs[16];
         for (int j = 0; j < 16; ++j) xs[j] = v[k0 + j] * sc;
         uint32_t w[kOzSlices][4];
-        oz_pack16(xs, w);
+        oz_pack<4>(xs, w);
         for (int q = 0; q < kOzSlices; ++q)
           for (int j = 0; j < 16; ++j)
             bs[oz_offset(kOzBRows, q * kOzN + lane, k0) + j] = (unsigned char)((w[q][j >> 2] >> (8 * (j & 3))) & 0xFFu);
