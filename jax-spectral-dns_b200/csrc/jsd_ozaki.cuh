@@ -190,6 +190,12 @@ __device__ __forceinline__ void oz_ld16(uint32_t taddr, uint32_t* r) {
       : "r"(taddr));
 }
 
+// int32 -> double with one FP64 add instead of a conversion: the bit pattern
+// 0x43300000:(x ^ 2^31) is the double 2^52 + 2^31 + x (exact below 2^53)
+__device__ __forceinline__ double oz_i2d(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 __device__ __forceinline__ void oz_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
 }
@@ -354,8 +360,8 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          r[j] = fma(r[j], 0.0078125, (double)(int)hi[j]);
-          r[j] = fma(r[j], 0.0078125, (double)(int)lo[j]);
+          r[j] = fma(r[j], 0.0078125, oz_i2d(hi[j]));
+          r[j] = fma(r[j], 0.0078125, oz_i2d(lo[j]));
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
