@@ -293,7 +293,29 @@ def run_ours(args):
         roofline = None
         if dom is not None:
             k = kernels[dom]
-            if dom == "gemm":
+            ozaki = head == "mixed" and all(plans[head].eig_kernel(i)[0] == 1 for i in (1, 2))
+            if dom == "gemm" and ozaki:
+                # the mixed form's only GEMM-class launches are the eigenbasis
+                # products, here on the int8 tensor cores: FP64-equivalent
+                # throughput against the FP64 GEMM peak they replace, and the
+                # int8 pipe's own use (36 slice products of 128 x 128 tensor
+                # tiles per FP64-equivalent (Ny-2) x Ny product)
+                fp64_peak = measure_fp64_peak(dev)
+                achieved = k["work"] / (k["ms"] / 1e3) / 1e12
+                ny = modes[1]
+                int8_tops = achieved * 36 * 128 * 128 / ((ny - 2) * ny)
+                int8_peak = 2 * peaks["bf16_tflops"]
+                roofline = {"kernel": "k_oz8_gemm (FP64-accurate eigenbasis products, Ozaki int8 on tcgen05)",
+                            "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
+                            "unit": "TFLOP/s (FP64-equivalent)", "frac": achieved / fp64_peak,
+                            "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 has no "
+                                           "entry in MEASURED_PEAKS.json)",
+                            "int8_pipe": {"achieved_tops": int8_tops, "peak_tops": int8_peak,
+                                          "frac": int8_tops / int8_peak,
+                                          "peak_source": "2 x bf16_tflops of MEASURED_PEAKS.json (dense int8 "
+                                                         "issues at twice the bf16 rate)"},
+                            "traffic": _ncu_traffic("k_oz8_gemm", head), "share_of_kernel_time": k["ms"] / total_k}
+            elif dom == "gemm":
                 fp64_peak = measure_fp64_peak(dev)
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e12
                 roofline = {"kernel": "k_dgemm (FP64 DMMA y-contractions)", "bound": "tensor",
