@@ -227,9 +227,10 @@ int jsd_split_kernel(const jsd_plan* plan, float* times_ms);
 int jsd_set_split_kernel(jsd_plan* plan, int kernel);
 
 /* Eigenbasis product kernel of a plan at GEMM site 1 (eigenbasis in) or 2
- * (eigenbasis out): 0 FP64 DMMA (the default), 1 FP64-accurate Ozaki
- * products on the int8 tensor cores (k_oz8_gemm, Ny <= 129; jsd_autotune
- * considers it for mixed-precision plans only); -1 for a bad site.
+ * (eigenbasis out): 0 FP64 DMMA (the default of FP64 plans), 1
+ * FP64-accurate Ozaki products on the int8 tensor cores (k_oz8_gemm,
+ * Ny <= 129; the default of mixed-precision plans, whose autotuning keeps the
+ * faster kernel per site); -1 for a bad site.
  * times_ms (2 floats, may be null) receives the autotuner's timings (best
  * DMMA tile, Ozaki). No counterpart in the reference. */
 int jsd_eig_kernel(const jsd_plan* plan, int site, float* times_ms);

@@ -1360,6 +1360,9 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
     // (the epilogue's pair stores need 16-byte aligned rows: every output is a
     // double2 field or an even offset into one, with an even row stride 2 nk nb)
     p->oz_ready = tensor_map_encoder() != nullptr;
+    // the mixed form starts on the int8 kernel at both eigenbasis sites (the
+    // autotuner keeps whichever is faster per site); FP64 plans on DMMA
+    if (p->oz_ready && p->mixed) p->eig_kernel[kSiteEigIn] = p->eig_kernel[kSiteEigOut] = 1;
   }
   JSD_TRY(upload(p, &p->lam, d->lam, ni));
   JSD_TRY(upload(p, &p->sgn, d->sgn, ni));

@@ -93,6 +93,10 @@ def test_ozaki_autotune_and_availability(cuda):
     p.check_device_errors()
     q = _plan((16, 65, 16), "fp64")
     assert all(q.eig_kernel(site)[0] == 0 for site in SITES)  # FP64 plans default to DMMA
+    modes, phys = mode_counts((16, 65, 16))
+    m = StepPlan(modes, phys, LX, LZ, _native.JSD_KIND_PERTURBATION, RE, DT, base_u=1 - cheb_points(65) ** 2,
+                 precision="mixed")
+    assert all(m.eig_kernel(site)[0] == 1 for site in SITES)  # mixed plans start on the int8 kernel
     with pytest.raises(_native.NativeError):
         q.set_eig_kernel(0, 1)  # the y-derivative site has no int8 form
     with pytest.raises(_native.NativeError):
