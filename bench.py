@@ -32,7 +32,7 @@ SHAPE = (128, 129, 128)
 LX, LZ = 4 * 3.141592653589793, 4 * 3.141592653589793 / 3
 RE_TAU, DT = 180.0, 0.002
 KMAX = (16, 16)
-METRIC = "steps/s at 128x129x128 (turbulent channel, FP64 RK3/CN step)"
+METRIC = "steps/s at 128x129x128 (turbulent channel RK3/CN step)"
 WORKLOAD = "turbulent channel Re_tau=180, 129x129x129 modes, constant mass flux, dt=0.002"
 
 
