@@ -92,6 +92,79 @@ class NavierStokesVelVort(Equation):
         vel = VectorField([PhysicalField.Zeros(domain) for _ in range(3)], "velocity")
         return cls.FromVelocityField(vel, **params)
 
+    # ---- seeding: (v, omega_y) -> (u, v, w) -------------------------------
+    @staticmethod
+    def _wall_projection(ny: int, m: int) -> np.ndarray:
+        """Least-squares projection, on the Ny Gauss-Lobatto points, onto the
+        span of phi_n = T_{n+4} - a_n T_{n+2} - b_n T_n (n < m), a_n =
+        2(n+2)/(n+1), b_n = -(n+3)/(n+1), the Chebyshev combinations with
+        phi(+-1) = phi'(+-1) = 0 (navier_stokes.py:1027-1060)."""
+        key = (ny, m)
+        cache = NavierStokesVelVort.__dict__.get("_projections")
+        if cache is None:
+            cache = {}
+            NavierStokesVelVort._projections = cache
+        if key not in cache:
+            from .domain import get_cheb_grid
+            ys = get_cheb_grid(ny)
+            basis = np.empty((ny, m))
+            for n in range(m):
+                coef = np.zeros(n + 5)
+                coef[n + 4] = 1.0
+                coef[n + 2] = -(2 * (n + 2)) / (n + 1)
+                coef[n] = (n + 3) / (n + 1)
+                basis[:, n] = np.polynomial.chebyshev.Chebyshev(coef)(ys)
+            cache[key] = basis @ np.linalg.lstsq(basis, np.eye(ny), rcond=None)[0]
+        return cache[key]
+
+    @classmethod
+    def smooth_and_enforce_bc_vel_y(cls, physical_domain: PhysicalDomain, vel_y_slice, M: Optional[int] = None):
+        """v projected (least squares on the collocation points) onto profiles
+        with v = dv/dy = 0 at both walls, along the first axis
+        (navier_stokes.py:1027-1060)."""
+        x = torch.as_tensor(vel_y_slice)
+        ny = x.shape[0]
+        p = torch.as_tensor(cls._wall_projection(ny, ny - 4 if M is None else int(M)), device=x.device)
+        return torch.tensordot(p.to(x.dtype), x, dims=([1], [0]))
+
+    @classmethod
+    def vort_yvel_to_vel(cls, physical_domain: PhysicalDomain, vort, vel_y, vel_x_00, vel_z_00,
+                         two_d: bool = False) -> torch.Tensor:
+        """(3, Mx, Ny, Mz) velocity from spectral omega_y and v: v smoothed onto
+        the wall-conforming profiles, u and w from continuity and the
+        definition of omega_y, u = (-i kx dv/dy + i kz omega_y) / -(kx^2 + kz^2),
+        w = (-i kz dv/dy - i kx omega_y) / -(kx^2 + kz^2); the (0,0) mode takes
+        vel_x_00, the smoothed v and vel_z_00 (navier_stokes.py:1062-1203).
+        With two_d, omega_y and w are zero and, as in the reference, every kz
+        column is treated as kz = 0: the whole kx = 0 row takes the (0,0) values
+        (u = vel_x_00, v = the smoothed (0,0) profile). All wavenumbers in one
+        batched product on the fields' device."""
+        vy = torch.as_tensor(vel_y).to(torch.complex128)
+        dev = vy.device
+        om = torch.zeros_like(vy) if two_d else torch.as_tensor(vort, device=dev).to(torch.complex128)
+        fd = physical_domain.hat()
+        ny = vy.shape[1]
+        proj = torch.as_tensor(cls._wall_projection(ny, ny - 4), device=dev).to(torch.complex128)
+        dmat = torch.as_tensor(fd.diff_mats[1], device=dev).to(torch.complex128)
+        vs = torch.einsum("lj,ijk->ilk", proj, vy)
+        dv = torch.einsum("lj,ijk->ilk", dmat, vs)
+        kx = torch.as_tensor(np.asarray(fd.grid[0]), dtype=torch.float64, device=dev)[:, None, None]
+        kz = torch.as_tensor(np.asarray(fd.grid[2]), dtype=torch.float64, device=dev)[None, None, :]
+        if two_d:
+            kz = torch.zeros_like(kz)
+        den = -(kx ** 2 + kz ** 2)
+        den = torch.where(den == 0, torch.ones_like(den), den)  # the (0,0) columns are replaced below
+        u = (-(1j * kx) * dv + (1j * kz) * om) / den
+        w = torch.zeros_like(u) if two_d else (-(1j * kz) * dv - (1j * kx) * om) / den
+        ux00 = torch.as_tensor(vel_x_00, device=dev).to(torch.complex128)
+        if two_d:
+            u[0] = ux00[:, None]
+            vs[0] = vs[0, :, 0].clone()[:, None]
+        else:
+            u[0, :, 0] = ux00
+            w[0, :, 0] = torch.as_tensor(vel_z_00, device=dev).to(torch.complex128)
+        return torch.stack([u, vs, w])
+
     def update_dt(self, new_dt: float) -> None:
         self._dt = float(new_dt)
         self._plan = None

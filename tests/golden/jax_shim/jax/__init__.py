@@ -68,7 +68,8 @@ class lax:
 
     @staticmethod
     def map(fun, xs, batch_size=None):
-        return numpy.array([fun(x) for x in xs])
+        # outputs stacked per leaf, as jax.lax.map does for tuple (pytree) results
+        return _stack_tree([fun(x) for x in xs])
 
     @staticmethod
     def scan(fun, init, xs=None, length=None, **kwargs):

@@ -301,7 +301,32 @@ def case_lsc():
     _save("lsc_n50", **out)
 
 
+def case_vort_yvel():
+    """Reference NavierStokesVelVort.vort_yvel_to_vel and
+    smooth_and_enforce_bc_vel_y (navier_stokes.py:1027-1203) on seeded
+    spectral omega_y and v (9x33x9 modes, box 2pi x 2 x pi), in 3-D and with
+    two_d=True."""
+    shape, lx, lz = (8, 33, 8), 2 * math.pi, math.pi
+    dom = _domain(shape, lx, lz)
+    rng = np.random.default_rng(12)
+    mx, ny, mz = 9, 33, 9
+    vort = rng.standard_normal((mx, ny, mz)) + 1j * rng.standard_normal((mx, ny, mz))
+    vel_y = rng.standard_normal((mx, ny, mz)) + 1j * rng.standard_normal((mx, ny, mz))
+    ux00 = rng.standard_normal(ny)
+    uz00 = rng.standard_normal(ny)
+    out3 = np.asarray(NavierStokesVelVort.vort_yvel_to_vel(dom, jnp.asarray(vort), jnp.asarray(vel_y),
+                                                           jnp.asarray(ux00), jnp.asarray(uz00)))
+    out2 = np.asarray(NavierStokesVelVort.vort_yvel_to_vel(dom, None, jnp.asarray(vel_y), jnp.asarray(ux00),
+                                                           None, two_d=True))
+    vs = rng.standard_normal(ny)
+    sm = np.asarray(NavierStokesVelVort.smooth_and_enforce_bc_vel_y(dom, jnp.asarray(vs)))
+    sm10 = np.asarray(NavierStokesVelVort.smooth_and_enforce_bc_vel_y(dom, jnp.asarray(vs), M=10))
+    _save("vort_yvel_9x33x9", shape=np.array(shape), lengths=np.array([lx, lz]), vort=vort, vel_y=vel_y,
+          ux00=ux00, uz00=uz00, out3=out3, out2=out2, slice_in=vs, slice_out=sm, slice_out_m10=sm10)
+
+
 CASES = {
+    "vort_yvel": case_vort_yvel,
     "lsc": case_lsc,
     "lin_pert": case_lin_pert,
     "lin_pert_gain": case_lin_pert_gain,

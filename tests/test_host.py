@@ -117,3 +117,27 @@ def test_reichardt_channel_seed():
     mean = g.no_hat(u[0]).mean(axis=(0, 2))
     prof = seeds.reichardt_profile(g.y, 180.0)
     assert np.abs(mean - prof).max() < 1e-10 * prof.max()
+
+
+def test_vort_yvel_to_vel_matches_reference():
+    """NavierStokesVelVort.vort_yvel_to_vel / smooth_and_enforce_bc_vel_y against
+    the reference's own outputs (tests/golden/vort_yvel_9x33x9.npz)."""
+    from jax_spectral_dns.navier_stokes import NavierStokesVelVort as NS
+
+    d = golden("vort_yvel_9x33x9")
+    dom = PhysicalDomain.create(tuple(int(x) for x in d["shape"]), (True, False, True),
+                                scale_factors=(d["lengths"][0], 1.0, d["lengths"][1]))
+    out3 = NS.vort_yvel_to_vel(dom, d["vort"], d["vel_y"], d["ux00"], d["uz00"]).cpu().numpy()
+    assert np.linalg.norm(out3 - d["out3"]) < 1e-12 * np.linalg.norm(d["out3"])
+    out2 = NS.vort_yvel_to_vel(dom, None, d["vel_y"], d["ux00"], None, two_d=True).cpu().numpy()
+    assert np.linalg.norm(out2 - d["out2"]) < 1e-12 * np.linalg.norm(d["out2"])
+    sm = NS.smooth_and_enforce_bc_vel_y(dom, d["slice_in"]).cpu().numpy()
+    assert np.linalg.norm(sm - d["slice_out"]) < 1e-12 * np.linalg.norm(d["slice_out"])
+    sm10 = NS.smooth_and_enforce_bc_vel_y(dom, d["slice_in"], M=10).cpu().numpy()
+    assert np.linalg.norm(sm10 - d["slice_out_m10"]) < 1e-12 * np.linalg.norm(d["slice_out_m10"])
+    # the smoothed profiles satisfy v = dv/dy = 0 at both walls
+    from jax_spectral_dns.domain import assemble_cheb_diff_mat, get_cheb_grid
+    dm = assemble_cheb_diff_mat(get_cheb_grid(33))
+    v = out3[1]
+    assert np.abs(v[:, [0, -1], :]).max() < 1e-12 * np.abs(v).max()
+    assert np.abs(np.einsum("lj,ijk->ilk", dm, v)[:, [0, -1], :]).max() < 1e-9 * np.abs(v).max()
