@@ -168,6 +168,7 @@ struct jsd_plan {
   // steady-state stages may do), packed D parts, kernel choice, error flag
   int tc_rows = 0;
   float *tc_ahi = nullptr, *tc_alo = nullptr;
+  double* tc_xrow = nullptr;  // Ny = 129: the last row of D (FP64, applied beside the tensor part)
   int split_kernel = 0;         // 0: k_sgemm3 (mma.sync), 1: k_tc05_dfield (tcgen05)
   int* errflag = nullptr;       // set by kernels whose bounded waits expired
   int num_sms = 148;
@@ -182,7 +183,7 @@ struct jsd_plan {
   int eig_kernel[3] = {0, 0, 0};  // per GemmSite (eigen sites): 0 DMMA, 1 Ozaki int8
   struct OzMap {
     const double* B = nullptr;
-    int N = 0, K = 0, ldb = 0;
+    int N = 0, K = 0, ldb = 0, box = 0;
     CUtensorMap map;
   };
   OzMap oz_maps[16];  // tensor maps of the B operands seen so far (round robin)
@@ -312,6 +313,9 @@ void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M,
 // y-derivatives D * f of up to kGemmMaxBatch fields: FP64 DMMA, or 3xTF32 in
 // the mixed-precision mode
 // Split-TF32 y-derivatives on tcgen05 (rows 0 .. tc_rows-1 of D).
+int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_rows, CUtensorMap* out);
+
+// Split-TF32 y-derivatives on tcgen05 (all Ny <= 129 rows of D; row 128 in FP64).
 int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
   Tc05Batch b;
   memset(&b, 0, sizeof(b));
@@ -319,13 +323,17 @@ int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int c
   b.M = p->tc_rows;
   b.K = p->g.ny;
   b.ldb = b.ldc = b.N;
+  b.xrow = p->tc_xrow;
   for (int i = 0; i < count; ++i) {
-    b.B[b.count] = src[i];
+    if (reinterpret_cast<uintptr_t>(src[i]) % 16) return fail(JSD_ERR_STATE, "tcgen05 y-derivative needs 16-byte aligned rows");
+    int rc = oz_tensor_map(p, src[i], b.N, b.K, b.ldb, kTcKp, &b.map[b.count]);
+    if (rc) return rc;
     b.C[b.count++] = dst[i];
   }
   const int tiles = (b.N + kTcN - 1) / kTcN * b.count;
   ProfScope ps(p, JSD_PROF_SGEMM, 2.0 * b.M * (double)b.K * b.N * count, s);
-  k_tc05_dfield<<<tiles < p->num_sms ? tiles : p->num_sms, 128, kTcSmem, s>>>(p->tc_ahi, p->tc_alo, b, p->errflag);
+  k_tc05_dfield<<<tiles < p->num_sms ? tiles : p->num_sms, kTcThreads, kTcSmem, s>>>(p->tc_ahi, p->tc_alo, b,
+                                                                                      p->errflag);
   JSD_LAUNCHED("k_tc05_dfield");
   return 0;
 }
@@ -343,7 +351,8 @@ int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int
     return launch_gemm(p, b, ny, kSiteDfield, s);
   }
   const int kernel = force_split >= 0 ? force_split : p->split_kernel;
-  if (kernel == 1 && p->tc_rows && (p->tc_rows == ny || walls_free)) return launch_tc05(p, src, dst, count, s);
+  (void)walls_free;  // the tcgen05 kernel computes every row, the y = -1 wall row in FP64
+  if (kernel == 1 && p->tc_rows) return launch_tc05(p, src, dst, count, s);
   SplitGemmBatch b;
   memset(&b, 0, sizeof(b));
   b.N = 2 * p->g.nk * p->g.nb;
@@ -407,11 +416,11 @@ EncodeTiledFn tensor_map_encoder() {
   return fn;
 }
 
-// 2-D tensor map of B (N doubles per row, min(K, 128) rows, row stride ldb),
-// box 32 x 128, zero fill outside; cached per plan
-int oz_tensor_map(jsd_plan* p, const double* B, int N, int K, int ldb, CUtensorMap* out) {
+// 2-D tensor map of B (N doubles per row, `rows` rows, row stride ldb), box
+// 32 x box_rows, zero fill outside; cached per plan
+int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_rows, CUtensorMap* out) {
   for (const auto& m : p->oz_maps)
-    if (m.B == B && m.N == N && m.K == K && m.ldb == ldb) {
+    if (m.B == B && m.N == N && m.K == rows && m.ldb == ldb && m.box == box_rows) {
       *out = m.map;
       return 0;
     }
@@ -419,9 +428,9 @@ int oz_tensor_map(jsd_plan* p, const double* B, int N, int K, int ldb, CUtensorM
   if (!enc) return fail(JSD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   auto& slot = p->oz_maps[p->oz_map_next];
   p->oz_map_next = (p->oz_map_next + 1) % 16;
-  const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)(K < kOzK ? K : kOzK)};
+  const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)ldb * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)kOzN, (cuuint32_t)kOzK};
+  const cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = enc(&slot.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(B), dims, strides, box,
                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -432,8 +441,9 @@ int oz_tensor_map(jsd_plan* p, const double* B, int N, int K, int ldb, CUtensorM
   }
   slot.B = B;
   slot.N = N;
-  slot.K = K;
+  slot.K = rows;
   slot.ldb = ldb;
+  slot.box = box_rows;
   *out = slot.map;
   return 0;
 }
@@ -454,7 +464,7 @@ int launch_ozaki(const jsd_plan* pc, const GemmBatch& b, cudaStream_t s) {
     if (k == 4 || g.alpha != 1.0) return fail(JSD_ERR_STATE, "operator has no int8 slice pack");
     if (reinterpret_cast<uintptr_t>(g.B) % 16 || b.ldb % 2 || b.N % 2)
       return fail(JSD_ERR_STATE, "int8 eigenbasis product needs 16-byte aligned rows");
-    int rc = oz_tensor_map(p, g.B, b.N, g.K, b.ldb, &o.map[o.count]);
+    int rc = oz_tensor_map(p, g.B, b.N, g.K < kOzK ? g.K : kOzK, b.ldb, kOzK, &o.map[o.count]);
     if (rc) return rc;
     OzEntry& e = o.e[o.count++];
     e.a = p->oz_a[k];
@@ -1319,12 +1329,13 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
       }
     JSD_TRY(upload(p, &p->Dhi, hi.data(), hi.size()));
     JSD_TRY(upload(p, &p->Dlo, lo.data(), lo.size()));
-    if (ny <= kTcM + 1) {
-      p->tc_rows = ny < kTcM ? ny : kTcM;
+    if (ny <= kTcM + 1 && tensor_map_encoder()) {
+      p->tc_rows = ny;
       std::vector<float> ahi, alo;
-      tc05_pack_a(d->D, p->tc_rows, ny, ny, tf32_round, ahi, alo);
+      tc05_pack_a(d->D, ny, ny, ny, tf32_round, ahi, alo);
       JSD_TRY(upload(p, &p->tc_ahi, ahi.data(), ahi.size()));
       JSD_TRY(upload(p, &p->tc_alo, alo.data(), alo.size()));
+      if (ny > kTcM) JSD_TRY(upload(p, &p->tc_xrow, d->D + (size_t)kTcM * ny, (size_t)ny));
       // k_sgemm3 stays the default: at 128 x 129 x 128 it measured 85 us per
       // call against 116 us for the tcgen05 kernel; the autotuner re-decides
       p->split_kernel = 0;

@@ -196,20 +196,6 @@ __device__ __forceinline__ double oz_i2d(uint32_t x) {
   return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
 }
 
-__device__ __forceinline__ void oz_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void oz_bulk_g2s(void* dst, const void* src, uint32_t bytes, uint32_t bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
-                   tc_smem(dst)),
-               "l"(src), "r"(bytes), "r"(bar)
-               : "memory");
-}
-
-__device__ __forceinline__ void oz_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
 #endif
 
 __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constant__ OzBatch b,
@@ -280,7 +266,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
 #pragma unroll
       for (int j = 0; j < kOzConvRows; ++j) v[j] = (cv && k0 + j < kt) ? stage[(k0 + j) * kOzN + n] : 0.0;
       const double bx = (E.K > kOzK && cv) ? stage[kOzK * kOzN + n] : 0.0;
-      oz_arrive(bar(8));  // staging may be refilled
+      tc_arrive(bar(8));  // staging may be refilled
       double* sd = side + buf * kOzSideDoubles;
       double mx = 0.0, dot = 0.0;
 #pragma unroll
@@ -292,7 +278,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
       }
       sd[kOzSidePMax + warp * kOzN + n] = mx;
       sd[kOzSidePDot + warp * kOzN + n] = dot;
-      oz_arrive(bar(9));
+      tc_arrive(bar(9));
       ok = mbar_wait(bar(9), i & 1);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
@@ -331,7 +317,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         sd[kOzSideBx + n] = bx;
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      oz_arrive(bar(buf));
+      tc_arrive(bar(buf));
     }
   } else if (warp < kOzConvWarps + kOzEpiWarps) {
     // ----------------------------------------------------------------- epilogue
@@ -385,7 +371,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         }
       }
       if (E.M > kOzM && ew == 0 && n0 + lane < b.N) E.C[(size_t)kOzM * b.ldc + n0 + lane] = sd[kOzSideDot + lane];
-      oz_arrive(bar(4 + buf));
+      tc_arrive(bar(4 + buf));
     }
   } else if (warp == kOzIssuerWarp) {
     // ------------------------------------------------------------------- issuer
@@ -402,9 +388,9 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
             fail_now();
             break;
           }
-          oz_expect_tx(bar(6), (uint32_t)kOzABytes);
+          tc_expect_tx(bar(6), (uint32_t)kOzABytes);
           for (int h = 0; h < 4; ++h)
-            oz_bulk_g2s(sA + h * (kOzABytes / 4), E.a + h * (kOzABytes / 4), (uint32_t)(kOzABytes / 4), bar(6));
+            tc_bulk_g2s(sA + h * (kOzABytes / 4), E.a + h * (kOzABytes / 4), (uint32_t)(kOzABytes / 4), bar(6));
           if (!mbar_wait(bar(6), a_loads & 1)) {
             fail_now();
             break;
@@ -453,14 +439,10 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
       if (lane == 0) {
         // rows >= min(K, 128) and columns >= N lie outside the tensor map and arrive as zeros
         const bool extra = E.K > kOzK;
-        oz_expect_tx(bar(7), (uint32_t)(kOzK * kOzN * 8 + (extra ? ncols * 8 : 0)));
-        asm volatile(
-            "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
-            "[%4];\n" ::"r"(tc_smem(stage)),
-            "l"(&b.map[e]), "r"(n0), "r"(0), "r"(bar(7))
-            : "memory");
+        tc_expect_tx(bar(7), (uint32_t)(kOzK * kOzN * 8 + (extra ? ncols * 8 : 0)));
+        tc_tma_load_2d(stage, &b.map[e], n0, 0, bar(7));
         if (extra)  // the K = 129 row, staged as row 128
-          oz_bulk_g2s(stage + kOzK * kOzN, E.B + (size_t)kOzK * b.ldb + n0, (uint32_t)(ncols * 8), bar(7));
+          tc_bulk_g2s(stage + kOzK * kOzN, E.B + (size_t)kOzK * b.ldb + n0, (uint32_t)(ncols * 8), bar(7));
       }
     }
   }
