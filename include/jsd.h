@@ -221,7 +221,7 @@ int jsd_set_xmid_variant(jsd_plan* plan, int variant);
 
 /* Split-TF32 y-derivative kernel of a mixed-precision plan: 0 mma.sync
  * (k_sgemm3), 1 tcgen05 with the accumulator in tensor memory
- * (k_tc05_dfield, Ny <= 129); -1 for FP64 plans. times_ms (2 floats, may be
+ * (k_tc05_dfield, Ny <= 129, the default); -1 for FP64 plans. times_ms (2 floats, may be
  * null) receives the autotuner's timings. No counterpart in the reference. */
 int jsd_split_kernel(const jsd_plan* plan, float* times_ms);
 int jsd_set_split_kernel(jsd_plan* plan, int kernel);

@@ -1336,9 +1336,9 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
       JSD_TRY(upload(p, &p->tc_ahi, ahi.data(), ahi.size()));
       JSD_TRY(upload(p, &p->tc_alo, alo.data(), alo.size()));
       if (ny > kTcM) JSD_TRY(upload(p, &p->tc_xrow, d->D + (size_t)kTcM * ny, (size_t)ny));
-      // k_sgemm3 stays the default: at 128 x 129 x 128 it measured 85 us per
-      // call against 116 us for the tcgen05 kernel; the autotuner re-decides
-      p->split_kernel = 0;
+      // the tcgen05 kernel is the default (58 us per call against 86 us for
+      // k_sgemm3 at 128 x 129 x 128); the autotuner re-decides per plan
+      p->split_kernel = 1;
     }
   }
   JSD_TRY(dev_alloc(p, (void**)&p->errflag, sizeof(int)));

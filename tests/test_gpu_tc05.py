@@ -2,9 +2,8 @@
 
 The tcgen05 kernel (accumulator in tensor memory) must agree with the
 mma.sync split kernel to FP32-accumulation level and with the FP64 form to the
-mixed form's own level, with all rows computed (Ny <= 128) and with the
-y = -1 wall row left out in steady-state stages (Ny = 129); its bounded waits
-must never expire.
+mixed form's own level, for Ny <= 128 and for Ny = 129 (the y = -1 wall row
+in FP64 beside the 128-row tensor part); its bounded waits must never expire.
 """
 import numpy as np
 import pytest
@@ -37,7 +36,7 @@ def _run(plan, u0, n):
 def test_tcgen05_split_kernel(cuda, shape):
     u0 = seeded_velocity_hat(shape, (LX, LZ), (6, 6), 1e-3, seed=11)
     a = _plan(shape, "mixed")
-    a.set_split_kernel(1)  # k_sgemm3 is the default; the tcgen05 kernel is selectable where it applies
+    assert a.split_kernel()[0] == 1  # the tcgen05 kernel is the default where it applies
     out_tc = _run(a, u0, 6)
     a.check_device_errors()
     b = _plan(shape, "mixed")
