@@ -58,11 +58,14 @@ def test_autotuned_plan_steps_identically(cuda, precision):
             continue  # the mixed form's y-derivatives do not use the DMMA kernel
         assert all(t > 0 for t in times)
         assert times[cfg] == min(times)
-    # the kernel choices that change round-off (x-pass variant, split-TF32 kernel)
-    # are copied, so the plans differ only in GEMM tiles, which never change a result
+    # the kernel choices that change round-off (x-pass variant, split-TF32
+    # kernel, eigenbasis kernel) are copied, so the plans differ only in GEMM
+    # tiles, which never change a result
     plain.set_xmid_variant(tuned.xmid_variant()[0])
     if precision == "mixed":
         plain.set_split_kernel(tuned.split_kernel()[0])
+        for site in (1, 2):
+            plain.set_eig_kernel(site, tuned.eig_kernel(site)[0])
     a = _steps(plain, u0, 3)
     b = _steps(tuned, u0, 3)
     assert torch.equal(a, b)
