@@ -318,7 +318,10 @@ def run_ours(args):
             elif dom == "gemm":
                 fp64_peak = measure_fp64_peak(dev)
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e12
-                roofline = {"kernel": "k_dgemm (FP64 DMMA y-contractions)", "bound": "tensor",
+                mixed_sites = head == "mixed" and any(plans[head].eig_kernel(i)[0] == 1 for i in (1, 2))
+                label = ("k_dgemm + k_oz8_gemm (eigenbasis products: FP64 DMMA at one site, FP64-accurate "
+                         "int8 Ozaki at the other)" if mixed_sites else "k_dgemm (FP64 DMMA y-contractions)")
+                roofline = {"kernel": label, "bound": "tensor",
                             "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                             "frac": achieved / fp64_peak,
                             "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 has no "
@@ -343,7 +346,7 @@ def run_ours(args):
             else:
                 per_kernel[k]["gbs"] = v["work"] / (v["ms"] / 1e3) / 1e9
         adj = None if args.no_adjoint else adjoint_leg(dev)
-        mixed_check = None if args.no_mixed_check else mixed_check_leg(dev)
+        mixed_check = None if args.no_mixed_check else mixed_check_leg(dev, args.autotune)
         ascent = None if args.no_ascent else ascent_leg(dev)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
@@ -427,7 +430,7 @@ def adjoint_leg(dev, checkpoints=(10, 50, 150, 1500)):
     return out
 
 
-def mixed_check_leg(dev, n_steps=2000, every=20):
+def mixed_check_leg(dev, autotune=True, n_steps=2000, every=20):
     """Nonlinear perturbation about the laminar base U = 1 - y^2: Re = 5000,
     48x65x48 grid (49x65x49 modes), Lx = 2 pi, Lz = pi, dt = 0.005, 2000 steps,
     seeded solenoidal field over |kx|, |kz| <= 8 with E0 = 1e-3; run in the FP64
@@ -448,7 +451,7 @@ def mixed_check_leg(dev, n_steps=2000, every=20):
     hist = {}
     for pr in ("fp64", "mixed"):
         plan = StepPlan(modes, phys, lx, lz, _native.JSD_KIND_PERTURBATION, re, dt, linearise=False,
-                        base_u=base, precision=pr, device=dev)
+                        base_u=base, precision=pr, device=dev, autotune=autotune)
         st, dp = u0.clone(), torch.zeros(1, dtype=torch.float64, device=dev)
         g = GraphedSteps(plan, st, dp, 0, every)
         energies = [plan.energy(st)]
