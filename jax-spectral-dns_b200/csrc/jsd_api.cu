@@ -1377,6 +1377,16 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
     // autotuner keeps whichever is faster per site); FP64 plans on DMMA
     if (p->oz_ready && p->mixed) p->eig_kernel[kSiteEigIn] = p->eig_kernel[kSiteEigOut] = 1;
   }
+  {
+    // small boxes: with fewer than 8 tiles of 32 columns per SM in a two-field
+    // call the persistent tcgen05 pipelines never fill (their operand loads
+    // and set-up dominate), so such plans start on k_sgemm3 and DMMA
+    const long long tiles = 2 * ((2LL * g.nk * nb + 31) / 32);
+    if (tiles < 8LL * p->num_sms) {
+      p->split_kernel = 0;
+      p->eig_kernel[kSiteEigIn] = p->eig_kernel[kSiteEigOut] = 0;
+    }
+  }
   JSD_TRY(upload(p, &p->lam, d->lam, ni));
   JSD_TRY(upload(p, &p->sgn, d->sgn, ni));
   JSD_TRY(upload(p, &p->c0, d->c0, ni));

@@ -93,10 +93,13 @@ def test_ozaki_autotune_and_availability(cuda):
     p.check_device_errors()
     q = _plan((16, 65, 16), "fp64")
     assert all(q.eig_kernel(site)[0] == 0 for site in SITES)  # FP64 plans default to DMMA
-    modes, phys = mode_counts((16, 65, 16))
-    m = StepPlan(modes, phys, LX, LZ, _native.JSD_KIND_PERTURBATION, RE, DT, base_u=1 - cheb_points(65) ** 2,
-                 precision="mixed")
-    assert all(m.eig_kernel(site)[0] == 1 for site in SITES)  # mixed plans start on the int8 kernel
+    for shape, start in (((16, 65, 16), 0), ((100, 33, 100), 1)):
+        modes, phys = mode_counts(shape)
+        m = StepPlan(modes, phys, LX, LZ, _native.JSD_KIND_PERTURBATION, RE, DT,
+                     base_u=1 - cheb_points(modes[1]) ** 2, precision="mixed")
+        # mixed plans start on the int8 kernel where each call has >= 8 tiles per SM
+        assert all(m.eig_kernel(site)[0] == start for site in SITES), shape
+        assert m.split_kernel()[0] == start, shape
     with pytest.raises(_native.NativeError):
         q.set_eig_kernel(0, 1)  # the y-derivative site has no int8 form
     with pytest.raises(_native.NativeError):
