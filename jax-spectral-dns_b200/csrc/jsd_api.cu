@@ -183,7 +183,7 @@ struct jsd_plan {
   int eig_kernel[3] = {0, 0, 0};  // per GemmSite (eigen sites): 0 DMMA, 1 Ozaki int8
   struct OzMap {
     const double* B = nullptr;
-    int N = 0, K = 0, ldb = 0, box = 0, boxc = 0;
+    int N = 0, K = 0, ldb = 0, box = 0;
     CUtensorMap map;
   };
   OzMap oz_maps[16];  // tensor maps of the B operands seen so far (round robin)
@@ -313,7 +313,7 @@ void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M,
 // y-derivatives D * f of up to kGemmMaxBatch fields: FP64 DMMA, or 3xTF32 in
 // the mixed-precision mode
 // Split-TF32 y-derivatives on tcgen05 (rows 0 .. tc_rows-1 of D).
-int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_cols, int box_rows, CUtensorMap* out);
+int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_rows, CUtensorMap* out);
 
 // Split-TF32 y-derivatives on tcgen05 (all Ny <= 129 rows of D; row 128 in FP64).
 int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
@@ -326,7 +326,7 @@ int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int c
   b.xrow = p->tc_xrow;
   for (int i = 0; i < count; ++i) {
     if (reinterpret_cast<uintptr_t>(src[i]) % 16) return fail(JSD_ERR_STATE, "tcgen05 y-derivative needs 16-byte aligned rows");
-    int rc = oz_tensor_map(p, src[i], b.N, b.K, b.ldb, kTcN, kTcKp, &b.map[b.count]);
+    int rc = oz_tensor_map(p, src[i], b.N, b.K, b.ldb, kTcKp, &b.map[b.count]);
     if (rc) return rc;
     b.C[b.count++] = dst[i];
   }
@@ -417,11 +417,10 @@ EncodeTiledFn tensor_map_encoder() {
 }
 
 // 2-D tensor map of B (N doubles per row, `rows` rows, row stride ldb), box
-// box_cols x box_rows, zero fill outside; cached per plan
-int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_cols, int box_rows,
-                  CUtensorMap* out) {
+// 32 x box_rows, zero fill outside; cached per plan
+int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_rows, CUtensorMap* out) {
   for (const auto& m : p->oz_maps)
-    if (m.B == B && m.N == N && m.K == rows && m.ldb == ldb && m.box == box_rows && m.boxc == box_cols) {
+    if (m.B == B && m.N == N && m.K == rows && m.ldb == ldb && m.box == box_rows) {
       *out = m.map;
       return 0;
     }
@@ -431,7 +430,7 @@ int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int bo
   p->oz_map_next = (p->oz_map_next + 1) % 16;
   const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)ldb * sizeof(double)};
-  const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
+  const cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = enc(&slot.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(B), dims, strides, box,
                          estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -445,7 +444,6 @@ int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int bo
   slot.K = rows;
   slot.ldb = ldb;
   slot.box = box_rows;
-  slot.boxc = box_cols;
   *out = slot.map;
   return 0;
 }
@@ -466,7 +464,7 @@ int launch_ozaki(const jsd_plan* pc, const GemmBatch& b, cudaStream_t s) {
     if (k == 4 || g.alpha != 1.0) return fail(JSD_ERR_STATE, "operator has no int8 slice pack");
     if (reinterpret_cast<uintptr_t>(g.B) % 16 || b.ldb % 2 || b.N % 2)
       return fail(JSD_ERR_STATE, "int8 eigenbasis product needs 16-byte aligned rows");
-    int rc = oz_tensor_map(p, g.B, b.N, g.K < kOzK ? g.K : kOzK, b.ldb, kOzN, kOzK, &o.map[o.count]);
+    int rc = oz_tensor_map(p, g.B, b.N, g.K < kOzK ? g.K : kOzK, b.ldb, kOzK, &o.map[o.count]);
     if (rc) return rc;
     OzEntry& e = o.e[o.count++];
     e.a = p->oz_a[k];

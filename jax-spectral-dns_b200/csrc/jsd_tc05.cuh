@@ -6,21 +6,18 @@
 // Chebyshev derivative matrix D (M = K = Ny <= 129), as three TF32 products
 // D_hi B_hi + D_lo B_hi + D_hi B_lo with FP32 accumulation in tensor memory
 // (the same 3xTF32 scheme as k_sgemm3). One persistent CTA of 27 warps per SM,
-// each CTA a contiguous range of 16-column tiles; the staged tile, the B
-// operand and the accumulators are all double-buffered, so the conversion of
-// one tile overlaps the MMAs of the previous one:
+// each CTA a contiguous range of 32-column tiles:
 //   * warp 26 (producer): one 2-D TMA load (cp.async.bulk.tensor, mbarrier
-//     completion) of the tile's 136 x 16 FP64 block of B into a staging buffer
+//     completion) of the tile's 136 x 32 FP64 block of B into a staging buffer
 //     (rows past K and columns past N arrive as zeros);
-//   * warps 0-16 (converters, warp w = rows 8w..8w+7; lane = column and half
-//     of the rows): split the staged values into TF32 hi and lo and store them
-//     as one 32-row K-major operand (hi rows 0-15, lo rows 16-31); for
-//     Ny = 129 they also form the FP64 dot products of D's last row (y = -1)
-//     with their rows;
+//   * warps 0-16 (converters, warp w = rows 8w..8w+7, lane = column): split the
+//     staged values into TF32 hi and lo and store them as one 64-row K-major
+//     operand (hi rows 0-31, lo rows 32-63); for Ny = 129 they also form the
+//     FP64 dot products of D's last row (y = -1) with their rows;
 //   * warp 25 (issuer): keeps D_hi / D_lo resident (bulk copy once), issues per
 //     K step of 8 two tcgen05.mma.kind::tf32 (M = 128): D_hi x [B_hi; B_lo]
-//     (N = 32: hi*hi into columns 0-15, hi*lo into 16-31) and D_lo x B_hi
-//     (N = 16, into columns 0-15), into one of two 32-column accumulator sets;
+//     (N = 64: hi*hi into columns 0-31, hi*lo into 32-63) and D_lo x B_hi
+//     (N = 32, into columns 0-31), into one of two 64-column accumulator sets;
 //   * warps 17-24 (epilogue, TMEM lane quadrant = warp % 4, half of the
 //     columns each): read both accumulators (tcgen05.ld), add them in FP64 and
 //     store; the last row (Ny = 129) from the converters' partial dots.
@@ -47,22 +44,21 @@ namespace jsd {
 
 constexpr int kTcM = 128;                      // accumulator rows (TMEM lanes)
 constexpr int kTcKp = 136;                     // padded K (17 MMA steps of 8)
-constexpr int kTcN = 16;                       // columns per tile
+constexpr int kTcN = 32;                       // columns per tile
 constexpr int kTcASize = kTcM * kTcKp * 4;     // bytes of one A part (69632)
 constexpr int kTcBRows = 2 * kTcN;             // stacked B operand rows (hi, lo)
-constexpr int kTcBSize = kTcBRows * kTcKp * 4;  // 17408 per buffer
-constexpr int kTcStageBytes = kTcKp * kTcN * 8;  // 17408 per buffer
+constexpr int kTcBSize = kTcBRows * kTcKp * 4;  // 34816
+constexpr int kTcStageBytes = kTcKp * kTcN * 8;  // 34816
 constexpr int kTcConvWarps = kTcKp / 8, kTcEpiWarps = 8;
 constexpr int kTcIssuerWarp = kTcConvWarps + kTcEpiWarps, kTcProducerWarp = kTcIssuerWarp + 1;
 constexpr int kTcThreads = 32 * (kTcProducerWarp + 1);  // 864
 constexpr int kTcSideDoubles = kTcConvWarps * kTcN;      // partial dots of the last row
-constexpr int kTcTmemCols = 2 * 2 * kTcN;                // two sets of (hi*hi + lo*hi, hi*lo): 64
+constexpr int kTcTmemCols = 2 * 2 * kTcN;                // two sets of (hi*hi + lo*hi, hi*lo)
 constexpr size_t kTcSmem =
-    2 * (size_t)kTcASize + 2 * (size_t)kTcBSize + 2 * (size_t)kTcStageBytes + 2 * sizeof(double) * kTcSideDoubles +
-    128;
+    2 * (size_t)kTcASize + kTcBSize + kTcStageBytes + 2 * sizeof(double) * kTcSideDoubles + 128;
 
 // map: 2-D tensor map of B[i] (inner N doubles, outer K rows, row stride
-// ldb), box 16 x 136
+// ldb), box 32 x 136
 struct Tc05Batch {
   CUtensorMap map[kGemmMaxBatch];
   double* C[kGemmMaxBatch];
@@ -153,12 +149,6 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
       : "r"(taddr));
 }
 
-__device__ __forceinline__ void tc_ld8(uint32_t taddr, uint32_t* r) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
-}
-
 __device__ __forceinline__ float tf32_round_dev(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
@@ -174,13 +164,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
   extern __shared__ __align__(1024) unsigned char tsm[];
   unsigned char* sAh = tsm;
   unsigned char* sAl = tsm + kTcASize;
-  unsigned char* sB = tsm + 2 * kTcASize;                       // two stacked hi / lo operands
-  double* stage = reinterpret_cast<double*>(sB + 2 * kTcBSize);  // two staged FP64 tiles, row k at 16 k
-  double* side = stage + 2 * kTcKp * kTcN;                      // two tile buffers of partial dots
+  unsigned char* sB = tsm + 2 * kTcASize;                       // stacked hi / lo operand
+  double* stage = reinterpret_cast<double*>(sB + kTcBSize);      // staged FP64 tile, row k at 32 k
+  double* side = stage + kTcKp * kTcN;                          // two tile buffers of partial dots
   uint64_t* bars = reinterpret_cast<uint64_t*>(side + 2 * kTcSideDoubles);
-  // bars (per tile parity): 0,1 full (B operand + partial dots); 2,3 mma done;
-  // 4,5 epilogue done; 7,8 staged tile ready; 9,10 staging released; 6 A loaded
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 11);
+  // bars: 0,1 full (B operand + partial dots of tile parity); 2,3 mma done;
+  // 4,5 epilogue done; 6 A loaded; 7 staged tile ready; 8 staging released
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 9);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto bar = [&](int i) { return tc_smem(&bars[i]); };
@@ -193,9 +183,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
     mbar_init(bar(5), 32 * kTcEpiWarps);
     mbar_init(bar(6), 1);
     mbar_init(bar(7), 1);
-    mbar_init(bar(8), 1);
-    mbar_init(bar(9), 32 * kTcConvWarps);
-    mbar_init(bar(10), 32 * kTcConvWarps);
+    mbar_init(bar(8), 32 * kTcConvWarps);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -222,53 +210,56 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
 
   if (warp < kTcConvWarps) {
     // ---------------------------------------------------------------- converters
-    const int n = lane & 15, k0 = 8 * warp + 4 * (lane >> 4);  // 4 rows of one column per lane
+    const int n = lane, k0 = 8 * warp;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
       const bool cv = n0 + n < b.N;
-      bool ok = mbar_wait(bar(7 + buf), (i >> 1) & 1);
+      bool ok = mbar_wait(bar(7), i & 1);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
       }
-      const double* st = stage + buf * kTcKp * kTcN;
-      double x[4];
+      double x[8];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) x[j] = cv ? st[(k0 + j) * kTcN + n] : 0.0;  // rows >= K arrive as zeros
-      tc_arrive(bar(9 + buf));  // this staging buffer may be refilled
+      for (int j = 0; j < 8; ++j) x[j] = cv ? stage[(k0 + j) * kTcN + n] : 0.0;  // rows >= K arrive as zeros
+      tc_arrive(bar(8));  // staging may be refilled
       double dot = 0.0;
       if (b.M > kTcM) {
 #pragma unroll
-        for (int j = 0; j < 4; ++j)
+        for (int j = 0; j < 8; ++j)
           if (k0 + j < b.K) dot = fma(__ldg(b.xrow + k0 + j), x[j], dot);
-        dot += __shfl_xor_sync(0xffffffffu, dot, 16);  // the column's other 4 rows of this warp
       }
-      uint32_t hi[4], lo[4];
+      uint32_t hi[8], lo[8];
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
+      for (int j = 0; j < 8; ++j) {
         const float h = tf32_round_dev((float)x[j]);
         hi[j] = __float_as_uint(h);
         lo[j] = __float_as_uint(tf32_round_dev((float)(x[j] - (double)h)));
       }
-      // B operand and partial dots of this parity are free once the MMAs and
-      // the epilogue of the tile two back are done
-      ok = i < 2 || (mbar_wait(bar(2 + buf), ((i - 2) >> 1) & 1) && mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1));
+      // the B operand is free once the previous tile's MMAs completed; the
+      // partial dots once the epilogue of the tile two back is done
+      ok = (i < 1 || mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1)) &&
+           (i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1));
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
       }
-      unsigned char* ob = sB + buf * kTcBSize;
-      *reinterpret_cast<uint4*>(ob + tc05_offset(kTcBRows, n, k0)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
-      *reinterpret_cast<uint4*>(ob + tc05_offset(kTcBRows, kTcN + n, k0)) = make_uint4(lo[0], lo[1], lo[2], lo[3]);
-      if (lane < 16) side[buf * kTcSideDoubles + warp * kTcN + n] = dot;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        *reinterpret_cast<uint4*>(sB + tc05_offset(kTcBRows, n, k0 + 4 * c)) =
+            make_uint4(hi[4 * c], hi[4 * c + 1], hi[4 * c + 2], hi[4 * c + 3]);
+        *reinterpret_cast<uint4*>(sB + tc05_offset(kTcBRows, kTcN + n, k0 + 4 * c)) =
+            make_uint4(lo[4 * c], lo[4 * c + 1], lo[4 * c + 2], lo[4 * c + 3]);
+      }
+      side[buf * kTcSideDoubles + warp * kTcN + n] = dot;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       tc_arrive(bar(buf));
     }
   } else if (warp < kTcConvWarps + kTcEpiWarps) {
     // ----------------------------------------------------------------- epilogue
     const int ew = warp - kTcConvWarps, quad = warp & 3, half = ew >> 2;
-    const int row = 32 * quad + lane, c0 = 8 * half;
+    const int row = 32 * quad + lane, c0 = 16 * half;
     const int mt = b.M < kTcM ? b.M : kTcM;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
@@ -284,26 +275,26 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
       for (int q = 1; q < kGemmMaxBatch; ++q)
         if (e == q) C = b.C[q];
       const uint32_t tbase = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * 2 * kTcN + c0);
-      uint32_t s0[8], s1[8];
-      tc_ld8(tbase, s0);           // hi*hi + lo*hi
-      tc_ld8(tbase + kTcN, s1);    // hi*lo
+      uint32_t s0[16], s1[16];
+      tc_ld16(tbase, s0);           // hi*hi + lo*hi
+      tc_ld16(tbase + kTcN, s1);    // hi*lo
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       if (row < mt) {
         double* out = C + (size_t)row * b.ldc + n0 + c0;
-        if (n0 + c0 + 8 <= b.N) {
+        if (n0 + c0 + 16 <= b.N) {
 #pragma unroll
-          for (int j = 0; j < 8; j += 2)
+          for (int j = 0; j < 16; j += 2)
             *reinterpret_cast<double2*>(out + j) =
                 make_double2((double)__uint_as_float(s0[j]) + (double)__uint_as_float(s1[j]),
                              (double)__uint_as_float(s0[j + 1]) + (double)__uint_as_float(s1[j + 1]));
         } else {
 #pragma unroll
-          for (int j = 0; j < 8; ++j)
+          for (int j = 0; j < 16; ++j)
             if (n0 + c0 + j < b.N) out[j] = (double)__uint_as_float(s0[j]) + (double)__uint_as_float(s1[j]);
         }
       }
-      if (b.M > kTcM && ew == 0 && lane < kTcN && n0 + lane < b.N) {
+      if (b.M > kTcM && ew == 0 && n0 + lane < b.N) {
         const double* sd = side + buf * kTcSideDoubles;
         double x = sd[lane];
 #pragma unroll
@@ -322,7 +313,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
       if (!mbar_wait(bar(6), 0)) fail_now();
       constexpr uint32_t lbo_a = kTcM * 16, lbo_b = kTcBRows * 16;
       const uint64_t dah = tc05_desc(tc_smem(sAh), lbo_a, 128), dal = tc05_desc(tc_smem(sAl), lbo_a, 128);
-      const uint64_t db0 = tc05_desc(tc_smem(sB), lbo_b, 128), db1 = tc05_desc(tc_smem(sB + kTcBSize), lbo_b, 128);
+      const uint64_t db = tc05_desc(tc_smem(sB), lbo_b, 128);
       for (int i = 0; i < nt && !*abort_flag; ++i) {
         const int buf = i & 1;
         if (!mbar_wait(bar(buf), (i >> 1) & 1)) {
@@ -331,7 +322,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
         }
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         const uint32_t acc = tmem + (uint32_t)(buf * 2 * kTcN);
-        const uint64_t db = buf ? db1 : db0;
         // K step s moves the start-address field (address / 16) by a constant
 #pragma unroll
         for (int s = 0; s < kTcKp / 8; ++s) {
@@ -351,17 +341,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
   } else {
     // ----------------------------------------------------------------- producer
     for (int i = 0; i < nt && !*abort_flag; ++i) {
-      const int buf = i & 1;
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
-      // staging buffer `buf` held tile i - 2
-      const bool ok = i < 2 || mbar_wait(bar(9 + buf), ((i - 2) >> 1) & 1);
+      const bool ok = i < 1 || mbar_wait(bar(8), (i - 1) & 1);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
       }
       if (lane == 0) {
-        tc_expect_tx(bar(7 + buf), (uint32_t)kTcStageBytes);
-        tc_tma_load_2d(stage + buf * kTcKp * kTcN, &b.map[e], n0, 0, bar(7 + buf));
+        tc_expect_tx(bar(7), (uint32_t)kTcStageBytes);
+        tc_tma_load_2d(stage, &b.map[e], n0, 0, bar(7));
       }
     }
   }
