@@ -325,7 +325,61 @@ def case_vort_yvel():
           ux00=ux00, uz00=uz00, out3=out3, out2=out2, slice_in=vs, slice_out=sm, slice_out_m10=sm10)
 
 
+SAMPLE_SEED, N_SAMPLES = 1234, 4096
+
+
+def _sample(a):
+    """A fixed seeded sample of a large state (the fixture keeps it, its norm
+    and the energy history instead of the whole array)."""
+    flat = np.asarray(a).ravel()
+    idx = np.sort(np.random.default_rng(SAMPLE_SEED).choice(flat.size, N_SAMPLES, replace=False))
+    return idx, flat[idx]
+
+
+def case_config1():
+    """Nonlinear perturbation at the size of BASELINE config 1: 49x65x49 modes
+    (48x65x48), Re=5000, Lx=2pi, Lz=pi, dt=0.005, E0=1e-3, |kx|,|kz| <= 8,
+    seed 0; 10 steps. States kept as seeded samples plus norms."""
+    shape, lx, lz = (48, 65, 48), 2 * math.pi, math.pi
+    re, dt, n = 5000.0, 0.005, 10
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (8, 8), 1e-3, seed=0)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=False)
+    nse.activate_jit()
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={1, n})
+    idx, s0 = _sample(u0)
+    _, s1 = _sample(states[1])
+    _, sn = _sample(states[n])
+    _save("config1_49x65x49", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n,
+          kmax=np.array([8, 8]), e0=1e-3, seed=0, idx=idx, u0_sample=s0, u1_sample=s1, un_sample=sn,
+          u0_norm=np.linalg.norm(u0), u1_norm=np.linalg.norm(states[1]), un_norm=np.linalg.norm(states[n]),
+          energy=en)
+
+
+def case_config2_dual():
+    """Reference dual-solver gradient at the size of BASELINE config 2:
+    33x65x33 modes (32x65x32), Re=3000, Lx=2pi, Lz=pi, dt=0.01, T=0.5
+    (50 steps), linearised, E0=1e-6, |kx|,|kz| <= 8, seed 2. Gradient kept as a
+    seeded sample plus its norm."""
+    shape, lx, lz = (32, 65, 32), 2 * math.pi, math.pi
+    re, dt, n = 3000.0, 0.01, 50
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (8, 8), 1e-6, seed=2)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=True)
+    nse.activate_jit()
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse, checkpointing=False)
+    grad = np.asarray(dual.get_grad()).copy()
+    gain = float(dual.gain)
+    idx, s0 = _sample(u0)
+    _, sg = _sample(grad)
+    _save("config2_dual_33x65x33", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n,
+          kmax=np.array([8, 8]), e0=1e-6, seed=2, idx=idx, u0_sample=s0, grad_sample=sg,
+          u0_norm=np.linalg.norm(u0), grad_norm=np.linalg.norm(grad), gain=gain)
+
+
 CASES = {
+    "config1": case_config1,
+    "config2_dual": case_config2_dual,
     "vort_yvel": case_vort_yvel,
     "lsc": case_lsc,
     "lin_pert": case_lin_pert,

@@ -1,0 +1,71 @@
+"""FP64 parity at the sizes of the benchmark configurations, against the
+reference run under the NumPy shim (tests/golden/config1_49x65x49.npz,
+config2_dual_33x65x33.npz from make_golden.py): the seeded input is rebuilt
+here from the same seed helper, and each large state is compared through a
+fixed seeded sample of 4096 entries plus its full norm, so the fixtures stay
+small while every part of the state can be reached."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from jax_spectral_dns import _native
+from jax_spectral_dns._plan import StepPlan, to_device_layout, to_reference_layout
+from jax_spectral_dns.domain import PhysicalDomain
+from jax_spectral_dns.field import FourierField, VectorField
+from jax_spectral_dns.navier_stokes_perturbation import NavierStokesVelVortPerturbation
+from jax_spectral_dns.navier_stokes_perturbation_dual import NavierStokesVelVortPerturbationDual
+from jax_spectral_dns.seeds import cheb_points, mode_counts, seeded_velocity_hat
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def _check(full, d, key, tol=TOL):
+    """Sampled entries and the norm of `full` against the fixture's."""
+    flat = np.asarray(full).ravel()
+    sample = d[key + "_sample"]
+    assert np.linalg.norm(flat[d["idx"]] - sample) < tol * np.linalg.norm(sample), key
+    assert abs(np.linalg.norm(flat) / float(d[key + "_norm"]) - 1) < tol, key
+
+
+def _seed(d):
+    shape, (lx, lz) = tuple(int(x) for x in d["shape"]), d["lengths"]
+    u0 = seeded_velocity_hat(shape, (lx, lz), tuple(int(k) for k in d["kmax"]), float(d["e0"]), seed=int(d["seed"]))
+    _check(u0, d, "u0", 1e-14)  # the seed helper rebuilds the reference's input
+    return shape, lx, lz, u0
+
+
+def test_nonlinear_perturbation_at_config1_size(cuda):
+    """49x65x49 modes, Re = 5000, dt = 0.005: 1 and 10 steps and the energy history."""
+    d = golden("config1_49x65x49")
+    shape, lx, lz, u0 = _seed(d)
+    modes, phys = mode_counts(shape)
+    plan = StepPlan(modes, phys, lx, lz, _native.JSD_KIND_PERTURBATION, float(d["re"]), float(d["dt"]),
+                    linearise=False, base_u=1 - cheb_points(modes[1]) ** 2)
+    st = to_device_layout(u0)
+    dp = torch.zeros(1, dtype=torch.float64, device="cuda")
+    energies = [plan.energy(st).item()]
+    n = int(d["n_steps"])
+    for t in range(n):
+        plan.step(st, dp, t, 1)
+        energies.append(plan.energy(st).item())
+        if t == 0:
+            _check(to_reference_layout(st).cpu().numpy(), d, "u1")
+    _check(to_reference_layout(st).cpu().numpy(), d, "un")
+    np.testing.assert_allclose(np.array(energies), d["energy"], rtol=TOL)
+
+
+def test_dual_gradient_at_config2_size(cuda):
+    """33x65x33 modes, Re = 3000, T = 0.5: the drop-in dual class's gradient
+    and gain against the reference dual solver's."""
+    d = golden("config2_dual_33x65x33")
+    shape, lx, lz, u0 = _seed(d)
+    dom = PhysicalDomain.create(shape, (True, False, True), scale_factors=(lx, 1.0, lz), aliasing=3 / 2)
+    vf = VectorField.FromData(FourierField, dom, torch.as_tensor(u0, device="cuda"), name="velocity_hat")
+    n, dt = int(d["n_steps"]), float(d["dt"])
+    nse = NavierStokesVelVortPerturbation(vf, Re=float(d["re"]), dt=dt, end_time=n * dt, linearise=True)
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse)
+    grad = dual.get_grad().cpu().numpy()
+    _check(grad, d, "grad")
+    assert abs(dual.gain / float(d["gain"]) - 1) < TOL

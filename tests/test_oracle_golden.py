@@ -90,3 +90,19 @@ def test_coupling_off_with_linearise_switch():
     assert rel(u1, d["u1"]) < 1e-12
     u, _, _ = O.run(st, d["u0"], n)
     assert rel(u, d["un"]) < 1e-12
+
+
+def test_oracle_at_config1_size():
+    """The oracle's first step at 49x65x49 modes (Re = 5000, dt = 0.005, every
+    |kx|, |kz| <= 8 populated) against the reference's, through the fixture's
+    seeded sample and norm (tests/golden/config1_49x65x49.npz)."""
+    from jax_spectral_dns.seeds import seeded_velocity_hat
+
+    d = golden("config1_49x65x49")
+    shape, (lx, lz) = tuple(int(x) for x in d["shape"]), d["lengths"]
+    u0 = seeded_velocity_hat(shape, (lx, lz), tuple(int(k) for k in d["kmax"]), float(d["e0"]), seed=int(d["seed"]))
+    st = O.make_stepper("perturbation", shape, lx, lz, float(d["re"]), float(d["dt"]), linearise=False)
+    u1, _, _ = O.run(st, u0, 1)
+    f = u1.ravel()
+    assert np.linalg.norm(f[d["idx"]] - d["u1_sample"]) < 1e-12 * np.linalg.norm(d["u1_sample"])
+    assert abs(np.linalg.norm(u1) / float(d["u1_norm"]) - 1) < 1e-12
