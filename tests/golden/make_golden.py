@@ -377,7 +377,33 @@ def case_config2_dual():
           u0_norm=np.linalg.norm(u0), grad_norm=np.linalg.norm(grad), gain=gain)
 
 
+def case_config4():
+    """The benchmark workload itself: NS with constant mass flux, Re_tau = 180,
+    box 4pi x 2 x 4pi/3, 129x129x129 modes (128x129x128), dt = 0.002, the
+    seeded Reichardt-plus-perturbation field of bench.py (|kx|, |kz| <= 16,
+    seed 0); one step. State kept as a seeded sample plus norms, with dPdx
+    and the energy before and after."""
+    shape, lx, lz = (128, 129, 128), 4 * math.pi, 4 * math.pi / 3
+    re_tau, dt, n = 180.0, 0.002, 1
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.turbulent_channel_hat(shape, (lx, lz), re_tau, (16, 16), seed=0)
+    nse = NavierStokesVelVort(_vf(dom, u0), Re_tau=re_tau, dt=dt, end_time=n * dt, constant_mass_flux=True)
+    nse.activate_jit()
+    dpdx0 = float(nse.dPdx)
+    flow_rate = float(nse.flow_rate)
+    t0 = time.time()
+    states, en, dps = _run_forward(nse, dom, u0, dpdx0, n, keep={1})
+    print("config4 step seconds", round(time.time() - t0, 1), flush=True)
+    idx, s0 = _sample(u0)
+    _, s1 = _sample(states[1])
+    _save("config4_129x129x129", shape=np.array(shape), lengths=np.array([lx, lz]), re_tau=re_tau, dt=dt,
+          n_steps=n, kmax=np.array([16, 16]), seed=0, idx=idx, u0_sample=s0, u1_sample=s1,
+          u0_norm=np.linalg.norm(u0), u1_norm=np.linalg.norm(states[1]), energy=en, dpdx=dps,
+          flow_rate=flow_rate)
+
+
 CASES = {
+    "config4": case_config4,
     "config1": case_config1,
     "config2_dual": case_config2_dual,
     "vort_yvel": case_vort_yvel,

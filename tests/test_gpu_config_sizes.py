@@ -69,3 +69,29 @@ def test_dual_gradient_at_config2_size(cuda):
     grad = dual.get_grad().cpu().numpy()
     _check(grad, d, "grad")
     assert abs(dual.gain / float(d["gain"]) - 1) < TOL
+
+
+def test_channel_step_at_benchmark_size(cuda):
+    """The benchmark workload (129x129x129 modes, constant mass flux, Re_tau =
+    180, dt = 0.002, bench.py's seeded field): one step against the reference's
+    own step, through the fixture's sample and norm, with dPdx, the flow-rate
+    target and the energy."""
+    from jax_spectral_dns.seeds import turbulent_channel_hat
+
+    d = golden("config4_129x129x129")
+    shape, (lx, lz) = tuple(int(x) for x in d["shape"]), d["lengths"]
+    re_tau, dt = float(d["re_tau"]), float(d["dt"])
+    u0 = turbulent_channel_hat(shape, (lx, lz), re_tau, tuple(int(k) for k in d["kmax"]), seed=int(d["seed"]))
+    _check(u0, d, "u0", 1e-14)
+    modes, phys = mode_counts(shape)
+    probe = StepPlan(modes, phys, lx, lz, 0, re_tau, dt)
+    q0 = probe.flow_rate(to_device_layout(u0)[0]).item()
+    assert abs(q0 / float(d["flow_rate"]) - 1) < 1e-13
+    del probe
+    p = StepPlan(modes, phys, lx, lz, 0, re_tau, dt, constant_mass_flux=True, flow_rate_target=q0)
+    st = to_device_layout(u0)
+    dp = torch.full((1,), float(d["dpdx"][0]), dtype=torch.float64, device="cuda")
+    p.step(st, dp, 0, 1)
+    _check(to_reference_layout(st).cpu().numpy(), d, "u1")
+    assert abs(dp.item() - float(d["dpdx"][1])) < 1e-8 * max(1.0, abs(float(d["dpdx"][1])))
+    assert abs(p.energy(st).item() / float(d["energy"][1]) - 1) < TOL
