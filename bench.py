@@ -242,9 +242,12 @@ def run_ours(args):
             ms, state, dpdx = timed(plans[pr])
             results[pr] = {"ms": ms, "state": state, "dpdx": dpdx, "energy": plans[pr].energy(state).item()}
     finite = all(bool(torch.isfinite(torch.view_as_real(r["state"])).all()) for r in results.values())
-    mixed_err = None
+    mixed_err = profile_err = None
     if "mixed" in results and "fp64" in results:
         mixed_err = abs(results["mixed"]["energy"] / results["fp64"]["energy"] - 1)
+        # mean profile: the (kx, kz) = (0, 0) mode of u over y
+        prof = {pr: to_reference_layout(results[pr]["state"])[0, 0, :, 0].real for pr in ("fp64", "mixed")}
+        profile_err = (torch.linalg.norm(prof["mixed"] - prof["fp64"]) / torch.linalg.norm(prof["fp64"])).item()
     # headline form: mixed when its energy error against FP64 meets the 1e-6 bar
     if args.precision == "both":
         head = "mixed" if (mixed_err is not None and mixed_err <= 1e-6) else "fp64"
@@ -377,6 +380,7 @@ def run_ours(args):
             "mixed_over_fp64": (forms_out["mixed"]["steps_per_s"] / forms_out["fp64"]["steps_per_s"]
                                 if len(forms_out) == 2 else None),
             "mixed_energy_rel_err_vs_fp64": mixed_err,
+            "mixed_mean_profile_rel_err_vs_fp64": profile_err,
             "mixed_error_steps": args.warmup + args.steps,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "api": "StepPlan.step on host (pinned) state"},
