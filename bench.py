@@ -43,6 +43,29 @@ def _dist():
     return rank, world, local
 
 
+def aggregate_over_ranks(local_ms: float, local_steps: int, device=None):
+    """(max of the ranks' times, sum of the ranks' steps): the timing is the
+    slowest replica's and the work is all replicas'. One MAX and one SUM
+    all-reduce when a process group of more than one rank is up; the local
+    values otherwise."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1):
+        return float(local_ms), int(local_steps)
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    n = torch.tensor([float(local_steps)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t.item()), int(round(n.item()))
+
+
+def split_runs(specs, rank: int, world: int):
+    """This rank's share of an ensemble's independent runs (round robin): the
+    replicas need no collective to step them."""
+    return list(specs)[rank::world]
+
+
 def _peaks():
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -204,10 +227,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(x: float) -> float:
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return aggregate_over_ranks(x, 0, device=dev)[0]
 
     def timed(plan, sampler=None):
         """W warm-up steps, then K steps timed with CUDA events on the
@@ -528,8 +548,13 @@ def run_ensemble(args):
 
     rank, world, local = _dist()
     torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     specs = draw_ensemble(args.ensemble, seed=0, horizon_scale=args.ensemble_horizon_scale)
-    mine = specs[rank::world]  # replicas: runs split across GPUs, no collective
+    mine = split_runs(specs, rank, world)  # replicas: runs split across GPUs, no collective while stepping
     bat = BatchedEnsemble(mine, streams=4, chunk=100)
     bat.run()  # warm-up
     bat.reset()
@@ -544,12 +569,15 @@ def run_ensemble(args):
     e_pool = ens.energies()
     ens.reset()
     ms_seq = ens.run_sequential()
+    local_steps = sum(s.steps for s in mine)
+    ms, steps = aggregate_over_ranks(ms, local_steps, device=torch.device("cuda", local))
+    ms_pool, _ = aggregate_over_ranks(ms_pool, 0, device=torch.device("cuda", local))
+    ms_seq, _ = aggregate_over_ranks(ms_seq, 0, device=torch.device("cuda", local))
     if rank == 0:
-        steps = sum(s.steps for s in mine)
         print(json.dumps({
             "metric": "ensemble steps/s (independent perturbation runs, mixed grids)",
-            "value": steps / (ms / 1e3), "unit": "steps/s", "n_gpus": world, "runs": len(mine),
-            "total_steps": steps, "ms": ms, "groups": len({(s.n, s.ny) for s in mine}),
+            "value": steps / (ms / 1e3), "unit": "steps/s", "n_gpus": world, "runs": len(specs),
+            "total_steps": steps, "ms": ms, "groups_rank0": len({(s.n, s.ny) for s in mine}),
             "stream_pool_steps_per_s": steps / (ms_pool / 1e3), "sequential_steps_per_s": steps / (ms_seq / 1e3),
             "speedup_over_stream_pool": ms_pool / ms, "speedup_over_sequential": ms_seq / ms,
             "energy_max_rel_diff_vs_one_plan_per_run": float(np.abs(e_bat / e_pool - 1).max()),
@@ -558,6 +586,11 @@ def run_ensemble(args):
                                    "E0 logU[1e-6,1e-2], T in {5,10,15,20} x horizon_scale, dt=0.01",
                        "product": "one batch plan per box, one launch set per RK stage for all its runs"},
         }), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
 
 def measure_fp64_peak(dev) -> float:
     import torch
