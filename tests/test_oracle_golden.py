@@ -4,6 +4,8 @@ These pin the oracle: each fixture was produced by the reference package
 itself (tests/golden/make_golden.py), so agreement to ~1e-12 here means the
 oracle restates the reference's arithmetic, quirks included.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -106,3 +108,19 @@ def test_oracle_at_config1_size():
     f = u1.ravel()
     assert np.linalg.norm(f[d["idx"]] - d["u1_sample"]) < 1e-12 * np.linalg.norm(d["u1_sample"])
     assert abs(np.linalg.norm(u1) / float(d["u1_norm"]) - 1) < 1e-12
+
+
+@pytest.mark.skipif(not os.environ.get("JSD_SLOW_TESTS"), reason="about 3 minutes on CPU; set JSD_SLOW_TESTS=1")
+def test_oracle_dual_gradient_at_config2_size():
+    """The oracle's dual gradient at 33x65x33 modes (Re = 3000, T = 0.5,
+    linearised) against the reference dual solver's, through the fixture's
+    seeded sample and norm (tests/golden/config2_dual_33x65x33.npz)."""
+    from jax_spectral_dns.seeds import seeded_velocity_hat
+
+    d = golden("config2_dual_33x65x33")
+    shape, (lx, lz) = tuple(int(x) for x in d["shape"]), d["lengths"]
+    u0 = seeded_velocity_hat(shape, (lx, lz), tuple(int(k) for k in d["kmax"]), float(d["e0"]), seed=int(d["seed"]))
+    g, gain, _, _ = O.dual_gradient(shape, lx, lz, float(d["re"]), float(d["dt"]), int(d["n_steps"]), u0, True)
+    f = g.ravel()
+    assert np.linalg.norm(f[d["idx"]] - d["grad_sample"]) < 1e-12 * np.linalg.norm(d["grad_sample"])
+    assert abs(gain / float(d["gain"]) - 1) < 1e-12
