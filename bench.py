@@ -340,6 +340,8 @@ def run_ours(args):
                             "traffic": _ncu_traffic("k_oz8_gemm", head), "share_of_kernel_time": k["ms"] / total_k}
             elif dom == "gemm":
                 fp64_peak = measure_fp64_peak(dev)
+                ny = modes[1]
+                same_shape = measure_fp64_same_shape(dev, ny - 2, ny, 3 * 2 * modes[0] * modes[2])
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e12
                 mixed_sites = head == "mixed" and any(plans[head].eig_kernel(i)[0] == 1 for i in (1, 2))
                 label = ("k_dgemm + k_oz8_gemm (eigenbasis products: FP64 DMMA at one site, FP64-accurate "
@@ -349,6 +351,9 @@ def run_ours(args):
                             "frac": achieved / fp64_peak,
                             "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 has no "
                                            "entry in MEASURED_PEAKS.json)",
+                            "cublas_same_shape_tflops": same_shape,
+                            "same_shape_note": "cuBLAS FP64 on one eigenbasis-in batch's shape ((Ny-2) x Ny "
+                                               "times Ny x 3 fields), measured in this run",
                             "traffic": _ncu_traffic("k_dgemm", head), "share_of_kernel_time": k["ms"] / total_k}
             else:
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e9
@@ -610,6 +615,27 @@ def measure_fp64_peak(dev) -> float:
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1))
     return 2 * n ** 3 / (best / 1e3) / 1e12
+
+
+def measure_fp64_same_shape(dev, m: int, k: int, n: int) -> float:
+    """cuBLAS FP64 (torch.matmul) TFLOP/s on the eigenbasis products' own
+    shape: an m x k operator times k x n fields (n = 3 fields' columns)."""
+    import torch
+
+    a = torch.randn(m, k, dtype=torch.float64, device=dev)
+    b = torch.randn(k, n, dtype=torch.float64, device=dev)
+    for _ in range(3):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e9
+    for _ in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return 2.0 * m * k * n / (best / 1e3) / 1e12
 
 
 def main():
