@@ -339,21 +339,25 @@ def _sample(a):
 def case_config1():
     """Nonlinear perturbation at the size of BASELINE config 1: 49x65x49 modes
     (48x65x48), Re=5000, Lx=2pi, Lz=pi, dt=0.005, E0=1e-3, |kx|,|kz| <= 8,
-    seed 0; 10 steps. States kept as seeded samples plus norms."""
+    seed 0; 100 steps. States after 1, 10, 50 and 100 steps kept as seeded
+    samples plus norms, with the energy after every step."""
     shape, lx, lz = (48, 65, 48), 2 * math.pi, math.pi
-    re, dt, n = 5000.0, 0.005, 10
+    re, dt, n = 5000.0, 0.005, 100
+    keep = (1, 10, 50, 100)
     dom = _domain(shape, lx, lz)
     u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (8, 8), 1e-3, seed=0)
     nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=False)
     nse.activate_jit()
-    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep={1, n})
+    states, en, _ = _run_forward(nse, dom, u0, 0.0, n, keep=set(keep))
     idx, s0 = _sample(u0)
-    _, s1 = _sample(states[1])
-    _, sn = _sample(states[n])
+    extra = {}
+    for k in keep:
+        _, sk = _sample(states[k])
+        extra[f"u{k}_sample"] = sk
+        extra[f"u{k}_norm"] = np.linalg.norm(states[k])
     _save("config1_49x65x49", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n,
-          kmax=np.array([8, 8]), e0=1e-3, seed=0, idx=idx, u0_sample=s0, u1_sample=s1, un_sample=sn,
-          u0_norm=np.linalg.norm(u0), u1_norm=np.linalg.norm(states[1]), un_norm=np.linalg.norm(states[n]),
-          energy=en)
+          kmax=np.array([8, 8]), e0=1e-3, seed=0, idx=idx, u0_sample=s0, u0_norm=np.linalg.norm(u0),
+          kept_steps=np.array(keep), energy=en, **extra)
 
 
 def case_config2_dual():
@@ -381,10 +385,10 @@ def case_config4():
     """The benchmark workload itself: NS with constant mass flux, Re_tau = 180,
     box 4pi x 2 x 4pi/3, 129x129x129 modes (128x129x128), dt = 0.002, the
     seeded Reichardt-plus-perturbation field of bench.py (|kx|, |kz| <= 16,
-    seed 0); one step. State kept as a seeded sample plus norms, with dPdx
-    and the energy before and after."""
+    seed 0); 3 steps. States after 1 and 3 steps kept as seeded samples plus
+    norms, with dPdx and the energy after every step."""
     shape, lx, lz = (128, 129, 128), 4 * math.pi, 4 * math.pi / 3
-    re_tau, dt, n = 180.0, 0.002, 1
+    re_tau, dt, n = 180.0, 0.002, 3
     dom = _domain(shape, lx, lz)
     u0 = seeds.turbulent_channel_hat(shape, (lx, lz), re_tau, (16, 16), seed=0)
     nse = NavierStokesVelVort(_vf(dom, u0), Re_tau=re_tau, dt=dt, end_time=n * dt, constant_mass_flux=True)
@@ -392,14 +396,15 @@ def case_config4():
     dpdx0 = float(nse.dPdx)
     flow_rate = float(nse.flow_rate)
     t0 = time.time()
-    states, en, dps = _run_forward(nse, dom, u0, dpdx0, n, keep={1})
-    print("config4 step seconds", round(time.time() - t0, 1), flush=True)
+    states, en, dps = _run_forward(nse, dom, u0, dpdx0, n, keep={1, n})
+    print("config4 seconds per step", round((time.time() - t0) / n, 1), flush=True)
     idx, s0 = _sample(u0)
     _, s1 = _sample(states[1])
+    _, s3 = _sample(states[n])
     _save("config4_129x129x129", shape=np.array(shape), lengths=np.array([lx, lz]), re_tau=re_tau, dt=dt,
-          n_steps=n, kmax=np.array([16, 16]), seed=0, idx=idx, u0_sample=s0, u1_sample=s1,
-          u0_norm=np.linalg.norm(u0), u1_norm=np.linalg.norm(states[1]), energy=en, dpdx=dps,
-          flow_rate=flow_rate)
+          n_steps=n, kmax=np.array([16, 16]), seed=0, idx=idx, u0_sample=s0, u1_sample=s1, u3_sample=s3,
+          u0_norm=np.linalg.norm(u0), u1_norm=np.linalg.norm(states[1]), u3_norm=np.linalg.norm(states[n]),
+          energy=en, dpdx=dps, flow_rate=flow_rate)
 
 
 CASES = {
