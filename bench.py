@@ -5,13 +5,20 @@ Navier-Stokes equations): box 4 pi x 2 x 4 pi/3, 129 x 129 x 129 Fourier /
 Chebyshev modes (the reference's 128 x 129 x 128 configuration; its dealiased
 physical grid is 194 x 129 x 194), Re_tau = 180, dt = 0.002, constant mass
 flux, initial field = Reichardt mean profile + seeded solenoidal perturbation
-(|kx|, |kz| <= 16, 10% of the centreline velocity). FP64 throughout.
+(|kx|, |kz| <= 16, 10% of the centreline velocity).
+
+Two forms are timed: plain FP64, and mixed precision (FP32 transforms and
+products, split-TF32 y-derivatives on the tensor cores, FP64-accurate solves).
+The headline is the mixed form when its energy after a fixed 1000-step run
+agrees with the FP64 form's to 1e-6, else the FP64 form. Side legs (adjoint
+gradients/s, the 48x65x48 perturbation case, gain ascent) print their own JSON
+lines first; the headline line comes last.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 N > 1 (torchrun) runs independent replicas, one per GPU (the step does not
-shard); value = total steps of all ranks / max rank time.
-`--impl reference` times the CPU restatement of the reference algorithm
+shard: no data-path collective); value = total steps of all ranks / max rank
+time. `--impl reference` times the CPU restatement of the reference algorithm
 (oracle/) on the host cores on a bounded sample of the same workload.
 """
 from __future__ import annotations
@@ -200,6 +207,43 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+ACC_STEPS, ACC_EVERY = 1000, 50
+
+
+def accuracy_leg(plans, u0_dev, dpdx0, n_steps=ACC_STEPS, every=ACC_EVERY):
+    """Every form stepped n_steps (1000) from the same seeded field, whatever
+    --steps is, with the energy recorded every `every` steps: the mixed form's
+    relative energy error against the FP64 form (which the tests pin to the
+    reference) after n_steps and over the history, and the relative error of
+    the mean profile u_00(y)."""
+    import torch
+    from jax_spectral_dns._plan import GraphedSteps, to_reference_layout
+
+    out, hist, final = {"steps": n_steps}, {}, {}
+    dev = u0_dev.device
+    for pr, plan in plans.items():
+        st = u0_dev.clone()
+        dp = torch.tensor([dpdx0], dtype=torch.float64, device=dev)
+        g = GraphedSteps(plan, st, dp, 0, every)
+        energies = [plan.energy(st)]
+        for _ in range(n_steps // every):
+            g.replay()
+            energies.append(plan.energy(st))
+        plan.check_device_errors()
+        hist[pr] = torch.cat(energies).cpu()
+        final[pr] = to_reference_layout(st)[0, 0, :, 0].real.clone()
+        del g
+    if "fp64" in hist and "mixed" in hist:
+        rel = (hist["mixed"] / hist["fp64"] - 1).abs()
+        out["mixed_energy_rel_err_vs_fp64"] = float(rel[-1])
+        out["mixed_energy_history_max_rel_err"] = float(rel.max())
+        out["mixed_mean_profile_rel_err_vs_fp64"] = float(
+            torch.linalg.norm(final["mixed"] - final["fp64"]) / torch.linalg.norm(final["fp64"]))
+    out["energy_final"] = {pr: float(h[-1]) for pr, h in hist.items()}
+    out["energy_growth"] = {pr: float(h[-1] / h[0]) for pr, h in hist.items()}
+    return out
+
+
 def run_ours(args):
     import numpy as np
     import torch
@@ -229,7 +273,7 @@ def run_ours(args):
     def max_over_ranks(x: float) -> float:
         return aggregate_over_ranks(x, 0, device=dev)[0]
 
-    def timed(plan, sampler=None):
+    def timed(plan):
         """W warm-up steps, then K steps timed with CUDA events on the
         launching stream, barrier + synchronize on both sides. The K steps
         are one CUDA-graph replay (captured before the timed region)."""
@@ -250,6 +294,8 @@ def run_ours(args):
         torch.cuda.synchronize()
         barrier()
         torch.cuda.synchronize()
+        # a kernel that gave up a bounded wait or a non-finite state voids the leg
+        plan.check_device_errors()
         return max_over_ranks(ev0.elapsed_time(ev1)), state, dpdx
 
     forms = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
@@ -261,14 +307,11 @@ def run_ours(args):
                                  device=dev, precision=pr, autotune=args.autotune)
             ms, state, dpdx = timed(plans[pr])
             results[pr] = {"ms": ms, "state": state, "dpdx": dpdx, "energy": plans[pr].energy(state).item()}
+    clock_summary = clocks.summary()
     finite = all(bool(torch.isfinite(torch.view_as_real(r["state"])).all()) for r in results.values())
-    mixed_err = profile_err = None
-    if "mixed" in results and "fp64" in results:
-        mixed_err = abs(results["mixed"]["energy"] / results["fp64"]["energy"] - 1)
-        # mean profile: the (kx, kz) = (0, 0) mode of u over y
-        prof = {pr: to_reference_layout(results[pr]["state"])[0, 0, :, 0].real for pr in ("fp64", "mixed")}
-        profile_err = (torch.linalg.norm(prof["mixed"] - prof["fp64"]) / torch.linalg.norm(prof["fp64"])).item()
-    # headline form: mixed when its energy error against FP64 meets the 1e-6 bar
+    acc = accuracy_leg(plans, u0_dev, dpdx0)
+    mixed_err = acc.get("mixed_energy_rel_err_vs_fp64")
+    # headline form: mixed when its 1000-step energy error against FP64 meets the 1e-6 bar
     if args.precision == "both":
         head = "mixed" if (mixed_err is not None and mixed_err <= 1e-6) else "fp64"
     else:
@@ -288,6 +331,7 @@ def run_ours(args):
         if n:
             kernels[name] = {"ms": tms, "launches": n, "work": work}
     plan.profile(False)
+    plan.check_device_errors()
 
     # end to end through the public step call with host buffers: every step
     # copies the state host->device from pinned memory, steps, copies it back
@@ -305,6 +349,7 @@ def run_ours(args):
         host_out.copy_(st.transpose(-3, -2), non_blocking=True)
     e1.record(stream)
     torch.cuda.synchronize()
+    plan.check_device_errors()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1) / n_e2e)
     e2e_value = world / (e2e_ms / 1e3)
     state_bytes = host_in.numel() * host_in.element_size()
@@ -352,8 +397,6 @@ def run_ours(args):
                             "peak_source": "cuBLAS FP64 GEMM 8192^3 measured in this run (FP64 has no "
                                            "entry in MEASURED_PEAKS.json)",
                             "cublas_same_shape_tflops": same_shape,
-                            "same_shape_note": "cuBLAS FP64 on one eigenbasis-in batch's shape ((Ny-2) x Ny "
-                                               "times Ny x 3 fields), measured in this run",
                             "traffic": _ncu_traffic("k_dgemm", head), "share_of_kernel_time": k["ms"] / total_k}
             else:
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e9
@@ -366,30 +409,31 @@ def run_ours(args):
             if roofline["traffic"] is not None:
                 roofline["traffic_source"] = ("dram__bytes_read.sum + dram__bytes_write.sum per launch, "
                                               f"profiles/{roofline['kernel'].split()[0]}_channel_128x129x128.md")
-        per_kernel = {k: {"avg_us": 1e3 * v["ms"] / v["launches"], "launches": v["launches"],
-                          "share": v["ms"] / total_k} for k, v in kernels.items()}
+        per_kernel = {k: {"avg_us": round(1e3 * v["ms"] / v["launches"], 2), "launches": v["launches"],
+                          "share": round(v["ms"] / total_k, 4)} for k, v in kernels.items()}
         for k, v in kernels.items():
             if k in ("gemm", "sgemm"):
-                per_kernel[k]["tflops"] = v["work"] / (v["ms"] / 1e3) / 1e12
+                per_kernel[k]["tflops"] = round(v["work"] / (v["ms"] / 1e3) / 1e12, 2)
             else:
-                per_kernel[k]["gbs"] = v["work"] / (v["ms"] / 1e3) / 1e9
-        adj = None if args.no_adjoint else adjoint_leg(dev)
-        mixed_check = None if args.no_mixed_check else mixed_check_leg(dev, args.autotune)
-        ascent = None if args.no_ascent else ascent_leg(dev)
+                per_kernel[k]["gbs"] = round(v["work"] / (v["ms"] / 1e3) / 1e9, 1)
+        # side legs and kernel choices on their own lines, before the headline
+        details = {pr: {"gemm_configs": {site: cfg for site, (cfg, _) in plans[pr].gemm_configs().items()},
+                        "split_kernel": plans[pr].split_kernel(), "xmid_variant": plans[pr].xmid_variant(),
+                        "eig_kernels": {site: plans[pr].eig_kernel(i) for i, site in ((1, "eig_in"), (2, "eig_out"))}}
+                   for pr in plans}
+        print(json.dumps({"leg": "kernel_choices", "forms": details, "kernels": per_kernel}), flush=True)
+        if not args.no_adjoint:
+            print(json.dumps({"leg": "adjoint", **adjoint_leg(dev)}), flush=True)
+        if not args.no_mixed_check:
+            print(json.dumps({"leg": "perturbation_48x65x48", **mixed_check_leg(dev, args.autotune)}), flush=True)
+        if not args.no_ascent:
+            print(json.dumps({"leg": "gain_ascent", **ascent_leg(dev)}), flush=True)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             rate, sec, sample, threads = cpu_reference_leg(1, 0)
             cpu = {"value": rate, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample}
-        forms_out = {pr: {"steps_per_s": world * args.steps / (r["ms"] / 1e3), "ms_per_step": r["ms"] / args.steps,
-                          "energy_after": r["energy"],
-                          "gemm_configs": {site: cfg for site, (cfg, _) in plans[pr].gemm_configs().items()},
-                          "split_kernel": plans[pr].split_kernel()[0],
-                          "split_kernel_ms": plans[pr].split_kernel()[1],
-                          "xmid_variant": plans[pr].xmid_variant()[0],
-                          "xmid_variant_ms": plans[pr].xmid_variant()[1],
-                          "eig_kernels": {site: plans[pr].eig_kernel(i)[0] for i, site in ((1, "eig_in"), (2, "eig_out"))},
-                          "eig_kernel_ms": {site: plans[pr].eig_kernel(i)[1] for i, site in ((1, "eig_in"), (2, "eig_out"))}}
-                     for pr, r in results.items()}
+        forms_out = {pr: {"steps_per_s": round(world * args.steps / (r["ms"] / 1e3), 2),
+                          "ms_per_step": round(r["ms"] / args.steps, 4)} for pr, r in results.items()}
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -397,22 +441,18 @@ def run_ours(args):
             "dtype": "f64" if head == "fp64" else "mixed: f32 transforms/products, 3xtf32 y-derivatives, f64 solves",
             "data": "synthetic (seeded Reichardt mean + solenoidal perturbation)",
             "config": {"workload": WORKLOAD, "modes": list(modes), "fft_sizes": list(plan.fft_sizes),
-                       "reference_physical_grid": list(phys), "parallelism": f"replicas x{world}",
+                       "parallelism": f"replicas x{world}",
                        "l2": "working set per step ~1 GB > 126 MB L2 (no flush needed)",
-                       "cuda_graph": bool(args.graph),
-                       "precision": head},
+                       "cuda_graph": bool(args.graph), "precision": head},
             "forms": forms_out,
             "mixed_over_fp64": (forms_out["mixed"]["steps_per_s"] / forms_out["fp64"]["steps_per_s"]
                                 if len(forms_out) == 2 else None),
-            "mixed_energy_rel_err_vs_fp64": mixed_err,
-            "mixed_mean_profile_rel_err_vs_fp64": profile_err,
-            "mixed_error_steps": args.warmup + args.steps,
+            "accuracy_1000_steps": acc,
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "api": "StepPlan.step on host (pinned) state"},
             "gpu_launches": plan.launches(args.steps),
-            "roofline": roofline, "kernels": per_kernel, "clocks": clocks.summary(),
-            "cpu_baseline": cpu, "finite": finite, "adjoint": adj, "perturbation_48x65x48": mixed_check,
-            "gain_ascent": ascent,
+            "roofline": roofline, "clocks": clock_summary, "cpu_baseline": cpu, "finite": finite,
+            "device_errors": "none (jsd_device_error read after every timed region)",
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -659,6 +699,11 @@ def main():
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="headline form; 'both' times FP64 and mixed and reports mixed beside FP64")
     args = ap.parse_args()
+    world = _dist()[1]
+    if 0 < args.ensemble < world:
+        # every rank must own at least one run: an empty rank would skip the
+        # stepping but its peers would still wait for it in the aggregation
+        ap.error(f"--ensemble {args.ensemble} is smaller than the number of ranks ({world})")
     if args.impl == "reference":
         run_reference(args)
     elif args.ensemble > 0:

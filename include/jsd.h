@@ -28,14 +28,15 @@
 extern "C" {
 #endif
 
-#define JSD_ABI_VERSION 2  /* 2: jsd_desc gained n_batch, re_tau_batch */
+#define JSD_ABI_VERSION 3  /* 2: jsd_desc gained n_batch, re_tau_batch; 3: JSD_ERR_NONFINITE, wait limit */
 
 enum jsd_status {
   JSD_OK = 0,
   JSD_ERR_ARG = -1,      /* invalid argument or unsupported configuration */
   JSD_ERR_CUDA = -2,     /* CUDA runtime error (message has the detail) */
   JSD_ERR_NOMEM = -3,    /* device allocation failed */
-  JSD_ERR_STATE = -4     /* call out of order (e.g. dual step without history) */
+  JSD_ERR_STATE = -4,    /* call out of order (e.g. dual step without history) */
+  JSD_ERR_NONFINITE = -5 /* the state became NaN or infinite (reported by jsd_device_error) */
 };
 
 enum jsd_kind {
@@ -169,7 +170,10 @@ int jsd_batch_active(const jsd_plan* plan);
  * Limit: ny <= 4096. The per-plane scratch is a fixed 32 KiB device array
  * inside the library, held by every GPU that loads it until the process exits.
  * The first call on a device looks up that array's address (with that device
- * current); make that first call before any stream capture. All calls share
+ * current) and keeps it for the life of the process, so it assumes the
+ * device's primary context is not reset or recreated in between (after
+ * cudaDeviceReset the kept address is stale); make that first call before
+ * any stream capture. All calls share
  * the array, so calls that overlap on the GPU (e.g. on two streams) race;
  * each call overwrites the entries it reads, so sequential calls need no
  * clearing. Calls no cudaMalloc/cudaFree. */
@@ -236,10 +240,21 @@ int jsd_set_split_kernel(jsd_plan* plan, int kernel);
 int jsd_eig_kernel(const jsd_plan* plan, int site, float* times_ms);
 int jsd_set_eig_kernel(jsd_plan* plan, int site, int kernel);
 
-/* JSD_ERR_CUDA (and clears the flag) when a kernel of the plan gave up a
- * bounded wait since the last check (its results are then invalid);
- * synchronises the stream. No counterpart in the reference. */
+/* Device-side failure detection; synchronises the stream and clears the
+ * plan's error flag. Returns JSD_ERR_CUDA when a kernel of the plan gave up a
+ * bounded wait since the last check (its results are then invalid), else
+ * JSD_ERR_NONFINITE when a stage produced a NaN or an infinity (every stage
+ * checks the new state as it reconstructs it), else 0. The reference's only
+ * check is a host assert on the objective (gradient_descent_solver.py:125). */
 int jsd_device_error(jsd_plan* plan, void* stream);
+
+/* Polls of an mbarrier before a pipeline wait of the plan's tcgen05 kernels
+ * gives up and raises the wait bit of the error flag (0 restores the
+ * default, 4194304). The kernel then stops, waits for its own copies and MMAs
+ * in flight, frees its tensor memory and returns. No counterpart in the
+ * reference. */
+int jsd_set_wait_limit(jsd_plan* plan, int polls);
+int jsd_wait_limit(const jsd_plan* plan);
 
 /* Number of kernel launches one call of jsd_step issues per time step after
  * its first; the first step of each call issues jsd_launches_first_step_extra

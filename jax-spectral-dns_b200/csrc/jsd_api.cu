@@ -183,11 +183,13 @@ struct jsd_plan {
   int eig_kernel[3] = {0, 0, 0};  // per GemmSite (eigen sites): 0 DMMA, 1 Ozaki int8
   struct OzMap {
     const double* B = nullptr;
-    int N = 0, K = 0, ldb = 0, box = 0;
+    int N = 0, K = 0, ldb = 0, box_cols = 0, box_rows = 0, swizzle = 0;
     CUtensorMap map;
   };
-  OzMap oz_maps[16];  // tensor maps of the B operands seen so far (round robin)
+  static constexpr int kMapCache = 32;
+  OzMap oz_maps[kMapCache];  // tensor maps of the operands seen so far (round robin)
   int oz_map_next = 0;
+  int wait_limit = kWaitPolls;  // polls before a pipeline wait of the tcgen05 kernels gives up
   float eig_ms[3][2] = {};        // autotuner timings per eigen site: DMMA (best tile), Ozaki
   double* re_run = nullptr;     // Reynolds number per run of a batch (device)
   double* lr_ns = nullptr;      // Linv_ns R_ns per run and stage (row-parallel mean-flow update)
@@ -313,7 +315,8 @@ void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M,
 // y-derivatives D * f of up to kGemmMaxBatch fields: FP64 DMMA, or 3xTF32 in
 // the mixed-precision mode
 // Split-TF32 y-derivatives on tcgen05 (rows 0 .. tc_rows-1 of D).
-int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_rows, CUtensorMap* out);
+int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_cols, int box_rows, bool swizzle128,
+                  CUtensorMap* out);
 
 // Split-TF32 y-derivatives on tcgen05 (all Ny <= 129 rows of D; row 128 in FP64).
 int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
@@ -326,14 +329,14 @@ int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int c
   b.xrow = p->tc_xrow;
   for (int i = 0; i < count; ++i) {
     if (reinterpret_cast<uintptr_t>(src[i]) % 16) return fail(JSD_ERR_STATE, "tcgen05 y-derivative needs 16-byte aligned rows");
-    int rc = oz_tensor_map(p, src[i], b.N, b.K, b.ldb, kTcKp, &b.map[b.count]);
+    int rc = oz_tensor_map(p, src[i], b.N, b.K, b.ldb, 32, kTcKp, false, &b.map[b.count]);
     if (rc) return rc;
     b.C[b.count++] = dst[i];
   }
   const int tiles = (b.N + kTcN - 1) / kTcN * b.count;
   ProfScope ps(p, JSD_PROF_SGEMM, 2.0 * b.M * (double)b.K * b.N * count, s);
   k_tc05_dfield<<<tiles < p->num_sms ? tiles : p->num_sms, kTcThreads, kTcSmem, s>>>(p->tc_ahi, p->tc_alo, b,
-                                                                                      p->errflag);
+                                                                                      p->errflag, p->wait_limit);
   JSD_LAUNCHED("k_tc05_dfield");
   return 0;
 }
@@ -416,24 +419,28 @@ EncodeTiledFn tensor_map_encoder() {
   return fn;
 }
 
-// 2-D tensor map of B (N doubles per row, `rows` rows, row stride ldb), box
-// 32 x box_rows, zero fill outside; cached per plan
-int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_rows, CUtensorMap* out) {
+// 2-D tensor map of a row-major FP64 matrix (N doubles per row, `rows` rows,
+// row stride ldb), box box_cols x box_rows, zero fill outside on loads and no
+// writes outside on stores, optionally with the 128-byte swizzle; cached per plan
+int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_cols, int box_rows, bool swizzle128,
+                  CUtensorMap* out) {
   for (const auto& m : p->oz_maps)
-    if (m.B == B && m.N == N && m.K == rows && m.ldb == ldb && m.box == box_rows) {
+    if (m.B == B && m.N == N && m.K == rows && m.ldb == ldb && m.box_cols == box_cols && m.box_rows == box_rows &&
+        m.swizzle == (int)swizzle128) {
       *out = m.map;
       return 0;
     }
   EncodeTiledFn enc = tensor_map_encoder();
   if (!enc) return fail(JSD_ERR_CUDA, "cuTensorMapEncodeTiled is not available");
   auto& slot = p->oz_maps[p->oz_map_next];
-  p->oz_map_next = (p->oz_map_next + 1) % 16;
+  p->oz_map_next = (p->oz_map_next + 1) % jsd_plan::kMapCache;
   const cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)ldb * sizeof(double)};
-  const cuuint32_t box[2] = {32u, (cuuint32_t)box_rows};
+  const cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
   const cuuint32_t estr[2] = {1, 1};
   const CUresult r = enc(&slot.map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double*>(B), dims, strides, box,
-                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     slot.B = nullptr;
@@ -443,7 +450,9 @@ int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int bo
   slot.N = N;
   slot.K = rows;
   slot.ldb = ldb;
-  slot.box = box_rows;
+  slot.box_cols = box_cols;
+  slot.box_rows = box_rows;
+  slot.swizzle = (int)swizzle128;
   *out = slot.map;
   return 0;
 }
@@ -462,9 +471,10 @@ int launch_ozaki(const jsd_plan* pc, const GemmBatch& b, cudaStream_t s) {
     int k = 0;
     while (k < 4 && p->oz_src[k] != g.A) ++k;
     if (k == 4 || g.alpha != 1.0) return fail(JSD_ERR_STATE, "operator has no int8 slice pack");
-    if (reinterpret_cast<uintptr_t>(g.B) % 16 || b.ldb % 2 || b.N % 2)
-      return fail(JSD_ERR_STATE, "int8 eigenbasis product needs 16-byte aligned rows");
-    int rc = oz_tensor_map(p, g.B, b.N, g.K < kOzK ? g.K : kOzK, b.ldb, kOzK, &o.map[o.count]);
+    if (reinterpret_cast<uintptr_t>(g.C) % 16 || b.ldc % 2 || b.N % 2)
+      return fail(JSD_ERR_STATE, "int8 eigenbasis product needs 16-byte aligned output rows");
+    // TMA stores of 16 x 32 output blocks into the tensor part's rows (< 128)
+    int rc = oz_tensor_map(p, g.C, b.N, g.M < kOzM ? g.M : kOzM, b.ldc, kOzOutCols, 32, true, &o.cmap[o.count]);
     if (rc) return rc;
     OzEntry& e = o.e[o.count++];
     e.a = p->oz_a[k];
@@ -478,7 +488,8 @@ int launch_ozaki(const jsd_plan* pc, const GemmBatch& b, cudaStream_t s) {
   }
   const long long tiles = (long long)((o.N + kOzN - 1) / kOzN) * o.count;
   ProfScope ps(const_cast<jsd_plan*>(p), JSD_PROF_GEMM, gemm_flops(b), s);
-  k_oz8_gemm<<<(int)std::min<long long>(tiles, p->num_sms), kOzThreads, kOzSmem, s>>>(o, p->errflag);
+  k_oz8_gemm<<<(int)std::min<long long>(tiles, p->num_sms), kOzThreads, kOzSmem, s>>>(o, p->errflag,
+                                                                                       p->wait_limit);
   JSD_LAUNCHED("k_oz8_gemm");
   return 0;
 }
@@ -790,7 +801,7 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     rc = launch_eig(p, b, ny, kSiteEigOut, s);
     if (rc) return rc;
   }
-  k_reconstruct<<<grid_for(fs, blk), blk, 0, s>>>(g, p->dvn, p->om, p->uw00, u, v, w);
+  k_reconstruct<<<grid_for(fs, blk), blk, 0, s>>>(g, p->dvn, p->om, p->uw00, u, v, w, p->errflag);
   JSD_LAUNCHED("k_reconstruct");
   // the back-transform left V^-1 v, V^-1 omega_y and dv/dy of the new state
   p->ev_valid = p->om_valid = p->dv_valid = true;
@@ -1140,10 +1151,22 @@ int jsd_device_error(jsd_plan* plan, void* stream) {
   JSD_CUDA(cudaStreamSynchronize(s));
   if (h) {
     JSD_CUDA(cudaMemsetAsync(plan->errflag, 0, sizeof(int), s));
-    return fail(JSD_ERR_CUDA, "a kernel's bounded wait expired (tcgen05 accumulator or bulk copy did not complete)");
+    JSD_CUDA(cudaStreamSynchronize(s));
+    if (h & kErrWaitExpired)
+      return fail(JSD_ERR_CUDA, "a kernel's bounded wait expired (tcgen05 accumulator or bulk copy did not complete)");
+    return fail(JSD_ERR_NONFINITE, "the state became non-finite (NaN or infinity after a stage)");
   }
   return 0;
 }
+
+int jsd_set_wait_limit(jsd_plan* plan, int polls) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  if (polls < 0) return fail(JSD_ERR_ARG, "wait limit must be >= 0 (0 restores the default)");
+  plan->wait_limit = polls == 0 ? kWaitPolls : polls;
+  return 0;
+}
+
+int jsd_wait_limit(const jsd_plan* plan) { return plan ? plan->wait_limit : 0; }
 
 int jsd_xmid_variant(const jsd_plan* plan, float* times_ms) {
   if (!plan) return -1;

@@ -12,6 +12,10 @@
 
 namespace jsd {
 
+// bits of a plan's device error flag
+constexpr int kErrWaitExpired = 1;  // a pipeline wait of a tcgen05 kernel gave up (its results are invalid)
+constexpr int kErrNonFinite = 2;    // a stage produced a NaN or an infinity
+
 struct Geo {
   int mx, ny, mz;    // Fourier modes in x and z (odd), Chebyshev points in y
   int kx_max, kz_max;  // K = m / 2

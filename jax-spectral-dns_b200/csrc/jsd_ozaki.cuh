@@ -25,24 +25,28 @@
 // diagonal p + q: 32 MMAs of N = 32..256 per tile instead of 36 x 4 narrow
 // ones, so the operands are read from shared memory once per wide product.
 //
-// One persistent CTA of 26 warps per SM, each CTA a contiguous range of
+// One persistent CTA of 25 warps per SM, each CTA a contiguous range of
 // 32-column tiles:
-//   * warp 25 (producer): loads the next tile's 128 x 32 FP64 block of B into
-//     a staging buffer with one 2-D TMA copy (cp.async.bulk.tensor, mbarrier
-//     completion; rows past K and columns past N arrive as zeros);
-//   * warps 0-15 (converters, warp w = rows 8w..8w+7, lane = column): read
-//     the staged tile, release the staging buffer, exchange partial column
-//     maxima through an mbarrier, cut the 8-row chunk into the 8 slices and
-//     store them in the canonical K-major core-matrix layout;
-//   * warp 24 (issuer): keeps A's 8 slices resident (bulk copy, reloaded when
+//   * warps 0-15 (converters, warp w = rows 8w..8w+7, lane = column): load
+//     their 8 x 32 block of the tile straight from global memory (a warp reads
+//     256 contiguous bytes per row) one tile ahead into registers, exchange
+//     the exponents of their partial column maxima through an mbarrier, cut
+//     the block into the 8 slices and store them in the canonical K-major
+//     core-matrix layout;
+//   * warp 16 (issuer): keeps A's 8 slices resident (bulk copy, reloaded when
 //     the operator changes), issues the 32 MMAs (kind::i8, M = 128) into one of
 //     two accumulator sets of 8 x 32 TMEM columns and commits to an mbarrier;
-//   * warps 16-23 (epilogue, TMEM lane quadrant = warp % 4 = row block, half of
+//   * warps 17-24 (epilogue, TMEM lane quadrant = warp % 4 = row block, half of
 //     the columns each): read the 8 accumulators (tcgen05.ld, two per wait),
-//     combine, scale, add the FP64 extras and store.
-// Every mbarrier wait has an iteration limit; on expiry the kernel raises the
-// error flag, every role stops at its next tile, the issuer waits (bounded) for
-// its last MMAs, and the CTA frees its TMEM and returns.
+//     combine, scale and add the FP64 extras, write the 32 x 16 block into a
+//     128-byte-swizzled shared-memory slot and store it with one TMA store
+//     (rows and columns outside C are not written).
+// A column holding a NaN or an infinity gets a NaN column scale, so the whole
+// output column is NaN as in an FP64 product (the slices alone would drop it).
+// Every mbarrier wait has an iteration limit (a kernel argument); on expiry
+// the kernel raises the error flag, every role stops at its next tile, the
+// issuer waits (bounded) for its operand copy and its last MMAs, the epilogue
+// warps for their TMA stores, and the CTA frees its TMEM and returns.
 #pragma once
 
 #include <cuda.h>  // CUtensorMap (the encoder is reached through the runtime's driver entry point)
@@ -64,20 +68,23 @@ constexpr int kOzASlice = kOzM * kOzK;               // bytes per A slice (16384
 constexpr int kOzABytes = kOzSlices * kOzASlice;     // 131072
 constexpr int kOzBRows = kOzSlices * kOzN;           // stacked B operand rows (256)
 constexpr int kOzBBytes = kOzBRows * kOzK;           // 32768
-constexpr int kOzStageRows = kOzK + 1;               // staged FP64 rows (row 128: the K = 129 extra)
-constexpr int kOzStageBytes = kOzStageRows * kOzN * 8;  // 33024
 constexpr int kOzTmemCols = 2 * kOzDiags * kOzN;     // 512: two accumulator sets
 constexpr int kOzConvWarps = 16, kOzEpiWarps = 8;
 constexpr int kOzConvRows = kOzK / kOzConvWarps;  // B rows per converter lane (8)
-constexpr int kOzIssuerWarp = kOzConvWarps + kOzEpiWarps, kOzProducerWarp = kOzIssuerWarp + 1;
-constexpr int kOzThreads = 32 * (kOzProducerWarp + 1);  // 832
-// side data per tile buffer (doubles): column scales, B row 128, extra-row
-// dot products (read by the epilogue), partial maxima and partial dots per
-// converter warp (exchanged among the converters)
-constexpr int kOzSideScale = 0, kOzSideBx = kOzN, kOzSideDot = 2 * kOzN, kOzSidePMax = 3 * kOzN,
-              kOzSidePDot = kOzSidePMax + kOzConvWarps * kOzN;
-constexpr int kOzSideDoubles = kOzSidePDot + kOzConvWarps * kOzN;
-constexpr size_t kOzSmem = (size_t)kOzABytes + kOzBBytes + kOzStageBytes + 2 * sizeof(double) * kOzSideDoubles + 128;
+constexpr int kOzIssuerWarp = kOzConvWarps;
+constexpr int kOzThreads = 32 * (kOzConvWarps + 1 + kOzEpiWarps);  // 800
+constexpr int kOzOutCols = kOzN / 2;                 // columns per epilogue warp (16 doubles = 128 bytes)
+constexpr int kOzOutSlot = 32 * kOzOutCols * 8;      // 4096: one epilogue warp's swizzled output block
+// per tile buffer (doubles): column scales, B row 128 (K = 129), row-128 dots (M = 129)
+constexpr int kOzSideScale = 0, kOzSideBx = kOzN, kOzSideDot = 2 * kOzN, kOzSideDoubles = 3 * kOzN;
+// partial-maximum exponents of a column that is all zero / holds a NaN or an infinity
+constexpr int kOzExpZero = -1000, kOzExpBad = 1 << 20;
+// shared memory: A slices | B slices | output slots | side data | exchange (exponents, dots) | barriers
+constexpr size_t kOzOffB = kOzABytes, kOzOffOut = kOzOffB + kOzBBytes, kOzOffSide = kOzOffOut + kOzEpiWarps * kOzOutSlot;
+constexpr size_t kOzOffPExp = kOzOffSide + 2 * sizeof(double) * kOzSideDoubles;
+constexpr size_t kOzOffPDot = kOzOffPExp + 2 * sizeof(int) * kOzConvWarps * kOzN;
+constexpr size_t kOzOffBars = kOzOffPDot + 2 * sizeof(double) * kOzConvWarps * kOzN;
+constexpr size_t kOzSmem = kOzOffBars + 128 + 1024;  // + alignment of the dynamic shared memory base
 
 // byte offset of element (row r, k) of an R-row int8 operand in the canonical
 // K-major layout: core matrix (row group r/8, K chunk k/16) of 8 rows x 16
@@ -149,24 +156,34 @@ struct OzEntry {
   int M, K;
 };
 
-// map[i]: 2-D tensor map of entry i's B (inner N doubles, outer min(K, 128)
-// rows, row stride ldb), box 32 x 128: one TMA load per tile
+// cmap[i]: 2-D tensor map of entry i's C for TMA stores (inner N doubles,
+// outer min(M, 128) rows, row stride ldc), box 16 x 32, 128-byte swizzle
 struct OzBatch {
-  CUtensorMap map[kGemmMaxBatch];
+  CUtensorMap cmap[kGemmMaxBatch];
   OzEntry e[kGemmMaxBatch];
   int count;
   int N, ldb, ldc;
 };
 
-// entry e by selects (a runtime index into the kernel parameter would copy the
-// parameter array to local memory)
-__device__ __forceinline__ OzEntry oz_entry(const OzBatch& b, int e) {
-  OzEntry r = b.e[0];
-#pragma unroll
-  for (int i = 1; i < kGemmMaxBatch; ++i)
-    if (e == i) r = b.e[i];
-  return r;
-}
+// one field of entry e by selects (a runtime index into the kernel parameter
+// would copy it to local memory; one field is cheaper in registers than the
+// whole entry)
+#define JSD_OZ_FIELD(name, type)                                   \
+  __device__ __forceinline__ type oz_##name(const OzBatch& b, int e) { \
+    type r = b.e[0].name;                                          \
+    _Pragma("unroll") for (int i = 1; i < kGemmMaxBatch; ++i)      \
+      if (e == i) r = b.e[i].name;                                 \
+    return r;                                                      \
+  }
+JSD_OZ_FIELD(B, const double*)
+JSD_OZ_FIELD(C, double*)
+JSD_OZ_FIELD(a, const int8_t*)
+JSD_OZ_FIELD(row_scale, const double*)
+JSD_OZ_FIELD(xrow, const double*)
+JSD_OZ_FIELD(xcol, const double*)
+JSD_OZ_FIELD(M, int)
+JSD_OZ_FIELD(K, int)
+#undef JSD_OZ_FIELD
 
 #if defined(__CUDA_ARCH__)
 // S32 accumulator, signed int8 A and B, both K-major, M = 128, N as given
@@ -199,18 +216,21 @@ __device__ __forceinline__ double oz_i2d(uint32_t x) {
 #endif
 
 __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constant__ OzBatch b,
-                                                             int* __restrict__ err) {
+                                                             int* __restrict__ err, int spin) {
 #if defined(__CUDA_ARCH__)
-  extern __shared__ __align__(1024) unsigned char osm[];
-  unsigned char* sA = osm;                                     // 8 A slices
-  unsigned char* sB = osm + kOzABytes;                         // stacked B slices
-  double* stage = reinterpret_cast<double*>(sB + kOzBBytes);   // staged FP64 tile, row k at 32 k
-  double* side = stage + kOzStageRows * kOzN;                  // two tile buffers
-  uint64_t* bars = reinterpret_cast<uint64_t*>(side + 2 * kOzSideDoubles);
-  // bars: 0,1 full (B slices + side data of tile parity); 2,3 mma done; 4,5
-  // epilogue done; 6 A loaded; 7 staged tile ready; 8 staging released;
-  // 9 partial maxima exchanged
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 10);
+  extern __shared__ unsigned char osm_raw[];
+  // 1024-byte alignment: the swizzled output slots repeat their pattern every 1024 bytes
+  unsigned char* osm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(osm_raw) + 1023) & ~uintptr_t(1023));
+  unsigned char* sA = osm;                                        // 8 A slices
+  unsigned char* sB = osm + kOzOffB;                              // stacked B slices
+  unsigned char* sOut = osm + kOzOffOut;                          // epilogue output slots
+  double* side = reinterpret_cast<double*>(osm + kOzOffSide);     // two tile buffers
+  int* pexp = reinterpret_cast<int*>(osm + kOzOffPExp);           // [2][16][32] partial-maximum exponents
+  double* pdot = reinterpret_cast<double*>(osm + kOzOffPDot);     // [2][16][32] partial row-128 dots
+  uint64_t* bars = reinterpret_cast<uint64_t*>(osm + kOzOffBars);
+  // bars: 0,1 full (B slices + side data of tile parity); 2,3 mma done;
+  // 4,5 epilogue done; 6 A loaded; 7 partial exponents exchanged
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 8);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto bar = [&](int i) { return tc_smem(&bars[i]); };
@@ -222,9 +242,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
     mbar_init(bar(4), 32 * kOzEpiWarps);
     mbar_init(bar(5), 32 * kOzEpiWarps);
     mbar_init(bar(6), 1);
-    mbar_init(bar(7), 1);
-    mbar_init(bar(8), 32 * kOzConvWarps);
-    mbar_init(bar(9), 32 * kOzConvWarps);
+    mbar_init(bar(7), 32 * kOzConvWarps);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -245,61 +263,73 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
   const int nt = t_end - t_begin;
   auto fail_now = [&]() {
     *abort_flag = 1;
-    atomicExch(err, 1);
+    atomicOr(err, kErrWaitExpired);
   };
 
   if (warp < kOzConvWarps) {
     // ---------------------------------------------------------------- converters
     const int n = lane, k0 = kOzConvRows * warp;
+    // this lane's 8 values (and, for K = 129, row 128) of tile i: loaded one tile
+    // ahead, once tile i - 1 is cut
+    double v[kOzConvRows], bx = 0.0;
+    auto load_tile = [&](int i, double* dst, double& dbx) {
+      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
+      const int K = oz_K(b, e), kt = K < kOzK ? K : kOzK;
+      const bool cv = n0 + n < b.N;
+      const double* src = oz_B(b, e) + n0 + n;
+#pragma unroll
+      for (int j = 0; j < kOzConvRows; ++j)
+        dst[j] = (cv && k0 + j < kt) ? __ldg(src + (size_t)(k0 + j) * b.ldb) : 0.0;
+      dbx = (warp == 0 && cv && K > kOzK) ? __ldg(src + (size_t)kOzK * b.ldb) : 0.0;
+    };
+    if (nt > 0) load_tile(0, v, bx);
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
-      const OzEntry E = oz_entry(b, e);
-      const int kt = E.K < kOzK ? E.K : kOzK;
-      const bool cv = n0 + n < b.N;
-      bool ok = mbar_wait(bar(7), i & 1);
-      if (!__all_sync(0xffffffffu, ok)) {
-        fail_now();
-        break;
-      }
-      double v[kOzConvRows];
-#pragma unroll
-      for (int j = 0; j < kOzConvRows; ++j) v[j] = (cv && k0 + j < kt) ? stage[(k0 + j) * kOzN + n] : 0.0;
-      const double bx = (E.K > kOzK && cv) ? stage[kOzK * kOzN + n] : 0.0;
-      tc_arrive(bar(8));  // staging may be refilled
-      double* sd = side + buf * kOzSideDoubles;
+      const int t = t_begin + i, e = t / tiles_n;
+      const int K = oz_K(b, e), kt = K < kOzK ? K : kOzK;
       double mx = 0.0, dot = 0.0;
+      bool bad = false;
 #pragma unroll
-      for (int j = 0; j < kOzConvRows; ++j) mx = fmax(mx, fabs(v[j]));
-      if (E.M > kOzM) {
+      for (int j = 0; j < kOzConvRows; ++j) {
+        mx = fmax(mx, fabs(v[j]));
+        bad |= !isfinite(v[j]);
+      }
+      if (oz_M(b, e) > kOzM) {
+        const double* xrow = oz_xrow(b, e);
 #pragma unroll
         for (int j = 0; j < kOzConvRows; ++j)
-          if (k0 + j < kt) dot = fma(__ldg(E.xrow + k0 + j), v[j], dot);
+          if (k0 + j < kt) dot = fma(__ldg(xrow + k0 + j), v[j], dot);
       }
-      sd[kOzSidePMax + warp * kOzN + n] = mx;
-      sd[kOzSidePDot + warp * kOzN + n] = dot;
-      tc_arrive(bar(9));
-      ok = mbar_wait(bar(9), i & 1);
+      pexp[(buf * kOzConvWarps + warp) * kOzN + n] = bad ? kOzExpBad : (mx > 0.0 ? oz_exponent(mx) : kOzExpZero);
+      pdot[(buf * kOzConvWarps + warp) * kOzN + n] = dot;
+      tc_arrive(bar(7));
+      bool ok = mbar_wait(bar(7), i & 1, spin);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
       }
-      double cm = sd[kOzSidePMax + n];
+      int em = pexp[(buf * kOzConvWarps) * kOzN + n];
 #pragma unroll
-      for (int w = 1; w < kOzConvWarps; ++w) cm = fmax(cm, sd[kOzSidePMax + w * kOzN + n]);
-      const int eb = oz_exponent(cm);
+      for (int w = 1; w < kOzConvWarps; ++w) em = max(em, pexp[(buf * kOzConvWarps + w) * kOzN + n]);
+      const bool col_bad = em == kOzExpBad;
+      const int eb = (em == kOzExpZero || col_bad) ? 0 : em;
       const double sc = oz_pow2(56 - eb);
       uint32_t wd[kOzSlices][kOzConvRows / 4];
       {
         double xs[kOzConvRows];
 #pragma unroll
-        for (int j = 0; j < kOzConvRows; ++j) xs[j] = v[j] * sc;
+        for (int j = 0; j < kOzConvRows; ++j) xs[j] = col_bad ? 0.0 : v[j] * sc;
         oz_pack<kOzConvRows / 4>(xs, wd);
       }
+      // the next tile's values are in flight while this one waits for its
+      // slice buffer (the loads only land in registers at the next tile's use)
+      const double bx_cur = bx;
+      if (i + 1 < nt) load_tile(i + 1, v, bx);
       // the B slices are free once the previous tile's MMAs completed; the
-      // side buffer once the epilogue of the tile two back is done
-      ok = (i < 1 || mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1)) &&
-           (i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1));
+      // side buffer once the epilogue of the tile two back is done (which also
+      // frees the accumulator set this tile's MMAs will use)
+      ok = (i < 1 || mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1, spin)) &&
+           (i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1, spin));
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
@@ -309,69 +339,16 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
       for (int q = 0; q < kOzSlices; ++q)
         *reinterpret_cast<uint2*>(sB + oz_offset(kOzBRows, q * kOzN + n, k0)) = make_uint2(wd[q][0], wd[q][1]);
       if (warp == 0) {
-        double x = sd[kOzSidePDot + n];
+        double* sd = side + buf * kOzSideDoubles;
+        double x = pdot[(buf * kOzConvWarps) * kOzN + n];
 #pragma unroll
-        for (int w = 1; w < kOzConvWarps; ++w) x += sd[kOzSidePDot + w * kOzN + n];
+        for (int w = 1; w < kOzConvWarps; ++w) x += pdot[(buf * kOzConvWarps + w) * kOzN + n];
         sd[kOzSideDot + n] = x;
-        sd[kOzSideScale + n] = oz_pow2(eb);
-        sd[kOzSideBx + n] = bx;
+        sd[kOzSideScale + n] = col_bad ? __longlong_as_double(0x7ff8000000000000LL) : oz_pow2(eb);
+        sd[kOzSideBx + n] = bx_cur;
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       tc_arrive(bar(buf));
-    }
-  } else if (warp < kOzConvWarps + kOzEpiWarps) {
-    // ----------------------------------------------------------------- epilogue
-    const int ew = warp - kOzConvWarps, quad = warp & 3, half = ew >> 2;
-    const int row = 32 * quad + lane, c0 = 16 * half;
-    for (int i = 0; i < nt && !*abort_flag; ++i) {
-      const int buf = i & 1;
-      const bool ok = mbar_wait(bar(2 + buf), (i >> 1) & 1) && mbar_wait(bar(buf), (i >> 1) & 1);
-      if (!__all_sync(0xffffffffu, ok)) {  // tcgen05.ld below needs the whole warp
-        fail_now();
-        break;
-      }
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
-      const OzEntry E = oz_entry(b, e);
-      const uint32_t tbase =
-          tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * kOzDiags * kOzN) + (uint32_t)c0;
-      double r[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) r[j] = 0.0;
-#pragma unroll
-      for (int d = kOzDiags - 1; d >= 1; d -= 2) {  // two loads per wait, highest diagonal first
-        uint32_t hi[16], lo[16];
-        oz_ld16(tbase + (uint32_t)(d * kOzN), hi);
-        oz_ld16(tbase + (uint32_t)((d - 1) * kOzN), lo);
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          r[j] = fma(r[j], 0.0078125, oz_i2d(hi[j]));
-          r[j] = fma(r[j], 0.0078125, oz_i2d(lo[j]));
-        }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      const double* sd = side + buf * kOzSideDoubles;
-      const int mt = E.M < kOzM ? E.M : kOzM;
-      if (row < mt) {
-        const double sa = __ldg(E.row_scale + row);
-        const double xc = E.K > kOzK ? __ldg(E.xcol + row) : 0.0;
-        double* out = E.C + (size_t)row * b.ldc + n0 + c0;
-        if (n0 + c0 + 16 <= b.N) {
-#pragma unroll
-          for (int j = 0; j < 16; j += 2) {
-            const double o0 = fma(xc, sd[kOzSideBx + c0 + j], r[j] * sa * sd[kOzSideScale + c0 + j]);
-            const double o1 = fma(xc, sd[kOzSideBx + c0 + j + 1], r[j + 1] * sa * sd[kOzSideScale + c0 + j + 1]);
-            *reinterpret_cast<double2*>(out + j) = make_double2(o0, o1);
-          }
-        } else {
-#pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (n0 + c0 + j < b.N) out[j] = fma(xc, sd[kOzSideBx + c0 + j], r[j] * sa * sd[kOzSideScale + c0 + j]);
-        }
-      }
-      if (E.M > kOzM && ew == 0 && n0 + lane < b.N) E.C[(size_t)kOzM * b.ldc + n0 + lane] = sd[kOzSideDot + lane];
-      tc_arrive(bar(4 + buf));
     }
   } else if (warp == kOzIssuerWarp) {
     // ------------------------------------------------------------------- issuer
@@ -381,24 +358,26 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
       for (int i = 0; i < nt && !*abort_flag; ++i) {
         const int buf = i & 1;
         const int t = t_begin + i, e = t / tiles_n;
-        const OzEntry E = oz_entry(b, e);
-        if (E.a != cur) {
+        const int8_t* a = oz_a(b, e);
+        if (a != cur) {
           // the MMAs of the previous tile read the resident slices: let them finish
-          if (i > 0 && !mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1)) {
+          if (i > 0 && !mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1, spin)) {
             fail_now();
             break;
           }
           tc_expect_tx(bar(6), (uint32_t)kOzABytes);
           for (int h = 0; h < 4; ++h)
-            tc_bulk_g2s(sA + h * (kOzABytes / 4), E.a + h * (kOzABytes / 4), (uint32_t)(kOzABytes / 4), bar(6));
-          if (!mbar_wait(bar(6), a_loads & 1)) {
+            tc_bulk_g2s(sA + h * (kOzABytes / 4), a + h * (kOzABytes / 4), (uint32_t)(kOzABytes / 4), bar(6));
+          if (!mbar_wait(bar(6), a_loads & 1, spin)) {
             fail_now();
+            // the operand copy may still be writing shared memory: let it land
+            if (!mbar_wait(bar(6), a_loads & 1, kDrainPolls)) atomicOr(err, kErrWaitExpired);
             break;
           }
           ++a_loads;
-          cur = E.a;
+          cur = a;
         }
-        if (!mbar_wait(bar(buf), (i >> 1) & 1)) {
+        if (!mbar_wait(bar(buf), (i >> 1) & 1, spin)) {
           fail_now();
           break;
         }
@@ -423,28 +402,65 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         issued = i + 1;
       }
       // no MMA may still run when the CTA frees its tensor memory
-      if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1)) fail_now();
+      if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, kDrainPolls)) fail_now();
     }
   } else {
-    // ----------------------------------------------------------------- producer
+    // ----------------------------------------------------------------- epilogue
+    const int ew = warp - kOzIssuerWarp - 1, quad = warp & 3, half = ew >> 2;
+    const int row = 32 * quad + lane, c0 = kOzOutCols * half;
+    unsigned char* slot = sOut + ew * kOzOutSlot;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
-      const OzEntry E = oz_entry(b, e);
-      const int ncols = b.N - n0 < kOzN ? b.N - n0 : kOzN;  // even: N is even
-      const bool ok = i < 1 || mbar_wait(bar(8), (i - 1) & 1);
-      if (!__all_sync(0xffffffffu, ok)) {
+      const int buf = i & 1;
+      const bool ok = mbar_wait(bar(2 + buf), (i >> 1) & 1, spin) && mbar_wait(bar(buf), (i >> 1) & 1, spin);
+      if (!__all_sync(0xffffffffu, ok)) {  // tcgen05.ld below needs the whole warp
         fail_now();
         break;
       }
-      if (lane == 0) {
-        // rows >= min(K, 128) and columns >= N lie outside the tensor map and arrive as zeros
-        const bool extra = E.K > kOzK;
-        tc_expect_tx(bar(7), (uint32_t)(kOzK * kOzN * 8 + (extra ? ncols * 8 : 0)));
-        tc_tma_load_2d(stage, &b.map[e], n0, 0, bar(7));
-        if (extra)  // the K = 129 row, staged as row 128
-          tc_bulk_g2s(stage + kOzK * kOzN, E.B + (size_t)kOzK * b.ldb + n0, (uint32_t)(ncols * 8), bar(7));
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
+      const uint32_t tbase =
+          tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * kOzDiags * kOzN) + (uint32_t)c0;
+      double r[kOzOutCols];
+#pragma unroll
+      for (int j = 0; j < kOzOutCols; ++j) r[j] = 0.0;
+#pragma unroll
+      for (int d = kOzDiags - 1; d >= 1; d -= 2) {  // two loads per wait, highest diagonal first
+        uint32_t hi[16], lo[16];
+        oz_ld16(tbase + (uint32_t)(d * kOzN), hi);
+        oz_ld16(tbase + (uint32_t)((d - 1) * kOzN), lo);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < kOzOutCols; ++j) {
+          r[j] = fma(r[j], 0.0078125, oz_i2d(hi[j]));
+          r[j] = fma(r[j], 0.0078125, oz_i2d(lo[j]));
+        }
       }
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      const double* sd = side + buf * kOzSideDoubles;
+      const int M = oz_M(b, e), mt = M < kOzM ? M : kOzM;
+      const double sa = row < mt ? __ldg(oz_row_scale(b, e) + row) : 0.0;
+      const double xc = (row < mt && oz_K(b, e) > kOzK) ? __ldg(oz_xcol(b, e) + row) : 0.0;
+      // the slot's previous TMA store must have read it before it is rewritten
+      if (lane == 0) tc_bulk_wait_read();
+      __syncwarp();
+      // 128-byte swizzle: 16-byte chunk j of row `lane` sits at chunk j ^ (lane & 7)
+#pragma unroll
+      for (int j = 0; j < kOzOutCols; j += 2) {
+        const double o0 = fma(xc, sd[kOzSideBx + c0 + j], r[j] * sa * sd[kOzSideScale + c0 + j]);
+        const double o1 = fma(xc, sd[kOzSideBx + c0 + j + 1], r[j + 1] * sa * sd[kOzSideScale + c0 + j + 1]);
+        *reinterpret_cast<double2*>(slot + lane * 128 + ((((j >> 1) ^ lane) & 7) << 4)) = make_double2(o0, o1);
+      }
+      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+      __syncwarp();
+      if (lane == 0 && 32 * quad < mt && n0 + c0 < b.N) {
+        tc_tma_store_2d(&b.cmap[e], n0 + c0, 32 * quad, slot);
+        tc_bulk_commit();
+      }
+      if (M > kOzM && ew == 0 && n0 + lane < b.N) oz_C(b, e)[(size_t)kOzM * b.ldc + n0 + lane] = sd[kOzSideDot + lane];
+      tc_arrive(bar(4 + buf));
     }
+    // this warp's stores read its slot and write C: both done before the CTA ends
+    if (lane == 0) tc_bulk_wait_all();
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();

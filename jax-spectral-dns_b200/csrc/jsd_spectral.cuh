@@ -770,10 +770,14 @@ __global__ void __launch_bounds__(32 * kMeanFlowRows) k_mean_flow_rows(
 // u, w from continuity and omega_y (rk_not_00, navier_stokes.py:1506-1527);
 // the (0,0) mode from the mean-flow solve; walls zeroed (domain.py:630-647).
 // (g.ny = Chebyshev points, g.nb runs; uw00 holds 2 Ny entries per run)
+// u, w of the new state from continuity, the (0,0) mean flow and the wall
+// rows; raises kErrNonFinite in `err` when any value it reads (dv/dy, omega_y
+// and the mean flow, from which all of u, v, w follow) is not finite.
 __global__ void k_reconstruct(Geo g, const double2* __restrict__ dvn, const double2* __restrict__ omn,
                               const double2* __restrict__ uw00, double2* __restrict__ u, double2* __restrict__ v,
-                              double2* __restrict__ w) {
+                              double2* __restrict__ w, int* __restrict__ err) {
   const size_t total = (size_t)g.ny * g.nb * g.nk;
+  bool bad = false;
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
     const int plane = (int)(t / g.nk);
     const int r = (int)(t - (size_t)plane * g.nk);
@@ -784,18 +788,22 @@ __global__ void k_reconstruct(Geo g, const double2* __restrict__ dvn, const doub
       continue;
     }
     if (ix == 0 && iz == 0) {
-      u[t] = uw00[(size_t)run * 2 * g.ny + y];
-      w[t] = uw00[(size_t)run * 2 * g.ny + g.ny + y];
+      const double2 a = uw00[(size_t)run * 2 * g.ny + y], c = uw00[(size_t)run * 2 * g.ny + g.ny + y];
+      bad |= !(isfinite(a.x) && isfinite(a.y) && isfinite(c.x) && isfinite(c.y));
+      u[t] = a;
+      w[t] = c;
       continue;
     }
     const double kx = kx_of(g, ix), kz = kz_of(g, iz);
     const double mk2 = -(kx * kx + kz * kz);
     const double2 dv = dvn[t], om = omn[t];
+    bad |= !(isfinite(dv.x) && isfinite(dv.y) && isfinite(om.x) && isfinite(om.y));
     const double2 uu = cadd(cmul_ik(dv, -kx), cmul_ik(om, kz));
     const double2 ww = csub(cmul_ik(dv, -kz), cmul_ik(om, kx));
     u[t] = make_double2(uu.x / mk2, uu.y / mk2);
     w[t] = make_double2(ww.x / mk2, ww.y / mk2);
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(err, kErrNonFinite);
 }
 
 // ---------------------------------------------------------------------------

@@ -21,9 +21,10 @@
 //   * warps 17-24 (epilogue, TMEM lane quadrant = warp % 4, half of the
 //     columns each): read both accumulators (tcgen05.ld), add them in FP64 and
 //     store; the last row (Ny = 129) from the converters' partial dots.
-// Every mbarrier wait has an iteration limit; on expiry the kernel raises the
-// error flag, every role stops at its next tile, the issuer waits (bounded) for
-// its last MMAs, and the CTA frees its TMEM and returns.
+// Every mbarrier wait has an iteration limit (a kernel argument); on expiry the
+// kernel raises the error flag, every role stops at its next tile, the issuer
+// waits (bounded) for its operand copy and its last MMAs, the producer for its
+// last staged load, and the CTA frees its TMEM and returns.
 //
 // Canonical K-major layout without swizzle (units of 16 bytes = 4 TF32): a core
 // matrix is 8 rows x 16 bytes stored contiguously; core matrix (row group g,
@@ -41,6 +42,12 @@
 #include "jsd_gemm.cuh"
 
 namespace jsd {
+
+// Polls of an mbarrier before a pipeline wait gives up (the plan's default;
+// jsd_set_wait_limit changes it), and before a CTA that gave up stops waiting
+// for its own copies and MMAs in flight before it tears down.
+constexpr int kWaitPolls = 1 << 22;
+constexpr int kDrainPolls = 1 << 22;
 
 constexpr int kTcM = 128;                      // accumulator rows (TMEM lanes)
 constexpr int kTcKp = 136;                     // padded K (17 MMA steps of 8)
@@ -101,9 +108,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
 }
 
-// true when the phase of `parity` completed within the iteration limit
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int i = 0; i < (1 << 22); ++i) {
+// true when the phase of `parity` completed within `limit` polls
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit) {
+  for (int i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred P1;\n\tmbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
@@ -115,6 +122,20 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   }
   return false;
 }
+
+// TMA store of a 2-D box from shared memory (x: innermost, a multiple of 16
+// bytes, both coordinates >= 0; elements outside the tensor are not written),
+// tracked in the issuing thread's bulk async-group
+__device__ __forceinline__ void tc_tma_store_2d(const CUtensorMap* map, int x, int y, const void* src) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];\n" ::"l"(map), "r"(x),
+               "r"(y), "r"(tc_smem(src))
+               : "memory");
+}
+__device__ __forceinline__ void tc_bulk_commit() { asm volatile("cp.async.bulk.commit_group;\n" ::: "memory"); }
+// the shared-memory sources of this thread's bulk stores may be overwritten
+__device__ __forceinline__ void tc_bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+// this thread's bulk stores are complete
+__device__ __forceinline__ void tc_bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 
 __device__ __forceinline__ void tc_arrive(uint32_t bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
@@ -159,7 +180,7 @@ __device__ __forceinline__ float tf32_round_dev(float x) {
 __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __restrict__ a_hi,
                                                                const float* __restrict__ a_lo,
                                                                const __grid_constant__ Tc05Batch b,
-                                                               int* __restrict__ err) {
+                                                               int* __restrict__ err, int spin) {
 #if defined(__CUDA_ARCH__)
   extern __shared__ __align__(1024) unsigned char tsm[];
   unsigned char* sAh = tsm;
@@ -205,7 +226,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
   const int ksteps = (b.K + 7) / 8;  // <= kTcKp / 8
   auto fail_now = [&]() {
     *abort_flag = 1;
-    atomicExch(err, 1);
+    atomicOr(err, kErrWaitExpired);
   };
 
   if (warp < kTcConvWarps) {
@@ -215,7 +236,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
       const int buf = i & 1;
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
       const bool cv = n0 + n < b.N;
-      bool ok = mbar_wait(bar(7), i & 1);
+      bool ok = mbar_wait(bar(7), i & 1, spin);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
@@ -239,8 +260,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
       }
       // the B operand is free once the previous tile's MMAs completed; the
       // partial dots once the epilogue of the tile two back is done
-      ok = (i < 1 || mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1)) &&
-           (i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1));
+      ok = (i < 1 || mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1, spin)) &&
+           (i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1, spin));
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
@@ -263,7 +284,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
     const int mt = b.M < kTcM ? b.M : kTcM;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
-      const bool ok = mbar_wait(bar(2 + buf), (i >> 1) & 1) && mbar_wait(bar(buf), (i >> 1) & 1);
+      const bool ok = mbar_wait(bar(2 + buf), (i >> 1) & 1, spin) && mbar_wait(bar(buf), (i >> 1) & 1, spin);
       if (!__all_sync(0xffffffffu, ok)) {  // tcgen05.ld below needs the whole warp
         fail_now();
         break;
@@ -310,13 +331,17 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
       tc_expect_tx(bar(6), (uint32_t)(2 * kTcASize));
       tc_bulk_g2s(sAh, a_hi, (uint32_t)kTcASize, bar(6));
       tc_bulk_g2s(sAl, a_lo, (uint32_t)kTcASize, bar(6));
-      if (!mbar_wait(bar(6), 0)) fail_now();
+      if (!mbar_wait(bar(6), 0, spin)) {
+        fail_now();
+        // the operand copy may still be writing shared memory: let it land
+        if (!mbar_wait(bar(6), 0, kDrainPolls)) atomicOr(err, kErrWaitExpired);
+      }
       constexpr uint32_t lbo_a = kTcM * 16, lbo_b = kTcBRows * 16;
       const uint64_t dah = tc05_desc(tc_smem(sAh), lbo_a, 128), dal = tc05_desc(tc_smem(sAl), lbo_a, 128);
       const uint64_t db = tc05_desc(tc_smem(sB), lbo_b, 128);
       for (int i = 0; i < nt && !*abort_flag; ++i) {
         const int buf = i & 1;
-        if (!mbar_wait(bar(buf), (i >> 1) & 1)) {
+        if (!mbar_wait(bar(buf), (i >> 1) & 1, spin)) {
           fail_now();
           break;
         }
@@ -336,13 +361,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
         issued = i + 1;
       }
       // no MMA may still run when the CTA frees its tensor memory
-      if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1)) fail_now();
+      if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, kDrainPolls)) fail_now();
     }
   } else {
     // ----------------------------------------------------------------- producer
+    int loads = 0;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
-      const bool ok = i < 1 || mbar_wait(bar(8), (i - 1) & 1);
+      const bool ok = i < 1 || mbar_wait(bar(8), (i - 1) & 1, spin);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         break;
@@ -351,7 +377,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
         tc_expect_tx(bar(7), (uint32_t)kTcStageBytes);
         tc_tma_load_2d(stage, &b.map[e], n0, 0, bar(7));
       }
+      ++loads;
     }
+    // one staged load at most is in flight (the next is issued only after the
+    // converters read the previous one): wait for it before the CTA's shared
+    // memory is released (returns at once when every load was consumed)
+    if (lane == 0 && loads > 0 && !mbar_wait(bar(7), (loads - 1) & 1, kDrainPolls)) atomicOr(err, kErrWaitExpired);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();

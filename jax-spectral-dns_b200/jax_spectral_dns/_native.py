@@ -53,9 +53,13 @@ EXPORTED = (
     "jsd_energy_runs", "jsd_set_batch_active", "jsd_batch_active",
     "jsd_split_kernel", "jsd_set_split_kernel", "jsd_device_error",
     "jsd_set_coupling_term", "jsd_set_base_flow", "jsd_eig_kernel", "jsd_set_eig_kernel",
+    "jsd_set_wait_limit", "jsd_wait_limit",
 )
 
-ABI_VERSION = 2  # JSD_ABI_VERSION of include/jsd.h this binding is written for
+ABI_VERSION = 3  # JSD_ABI_VERSION of include/jsd.h this binding is written for
+
+# status codes (enum jsd_status)
+JSD_ERR_ARG, JSD_ERR_CUDA, JSD_ERR_NOMEM, JSD_ERR_STATE, JSD_ERR_NONFINITE = -1, -2, -3, -4, -5
 
 # GEMM call sites of a plan (jsd_gemm_config) and the number of DMMA tile configurations
 GEMM_SITES = {"dfield": 0, "eig_in": 1, "eig_out": 2}
@@ -67,7 +71,17 @@ _lib = None
 
 
 class NativeError(RuntimeError):
-    pass
+    """A native call returned an error status (``code``: the JSD_ERR_* value)."""
+
+    def __init__(self, msg: str, code: int = 0):
+        super().__init__(msg)
+        self.code = code
+
+
+class DeviceFailure(NativeError):
+    """The device reported a failure after the fact: a kernel's bounded wait
+    expired (code JSD_ERR_CUDA) or the state became non-finite (code
+    JSD_ERR_NONFINITE). Results since the last check are invalid."""
 
 
 def load(path: str = LIB_PATH):
@@ -108,6 +122,8 @@ def load(path: str = LIB_PATH):
     lib.jsd_eig_kernel.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_set_eig_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.jsd_device_error.argtypes = [vp, vp]
+    lib.jsd_set_wait_limit.argtypes = [vp, ctypes.c_int]
+    lib.jsd_wait_limit.argtypes = [vp]
     lib.jsd_set_coupling_term.argtypes = [vp, ctypes.c_int]
     lib.jsd_set_base_flow.argtypes = [vp, vp, vp, vp]
     lib.jsd_set_batch_active.argtypes = [vp, ctypes.c_int]
@@ -126,7 +142,7 @@ def load(path: str = LIB_PATH):
     return lib
 
 
-def check(rc: int, what: str):
+def check(rc: int, what: str, exc=NativeError):
     if rc != 0:
         msg = load().jsd_last_error().decode(errors="replace")
-        raise NativeError(f"{what} failed ({rc}): {msg}")
+        raise exc(f"{what} failed ({rc}): {msg}", rc)

@@ -170,8 +170,18 @@ class StepPlan:
         _native.check(self.lib.jsd_set_eig_kernel(self.handle, int(site), int(kernel)), "jsd_set_eig_kernel")
 
     def check_device_errors(self) -> None:
-        """Raise when a kernel of this plan gave up a bounded wait."""
-        _native.check(self.lib.jsd_device_error(self.handle, _stream_ptr()), "jsd_device_error")
+        """Raise DeviceFailure when a kernel of this plan gave up a bounded wait
+        or a stage produced a NaN or an infinity since the last check
+        (synchronises the current stream; clears the flag)."""
+        _native.check(self.lib.jsd_device_error(self.handle, _stream_ptr()), "jsd_device_error",
+                      _native.DeviceFailure)
+
+    def set_wait_limit(self, polls: int) -> None:
+        """Polls before a pipeline wait of the tcgen05 kernels gives up (0: default)."""
+        _native.check(self.lib.jsd_set_wait_limit(self.handle, int(polls)), "jsd_set_wait_limit")
+
+    def wait_limit(self) -> int:
+        return int(self.lib.jsd_wait_limit(self.handle))
 
     def gemm_configs(self) -> dict:
         """{site: (configuration id, [per-configuration autotune ms])}."""

@@ -127,6 +127,7 @@ class GainProblem:
         if self.full_trajectory and not self.linearise and self.n_steps > 0:
             self._fwd_traj(self.n_steps)
             self._traj_owner = cps  # the recorded trajectory belongs to this forward pass
+            self.fwd.check_device_errors()
             return self.w_fwd.clone(), cps
         self._traj_owner = None
         t = 0
@@ -136,6 +137,7 @@ class GainProblem:
             t += n
             if t < self.n_steps:
                 cps.append(self.w_fwd.clone())
+        self.fwd.check_device_errors()
         return self.w_fwd.clone(), cps
 
     def backward_dual(self, uT: torch.Tensor, cps) -> torch.Tensor:
@@ -156,6 +158,8 @@ class GainProblem:
                 self._traj_owner = None  # w_traj now holds this recomputed segment
             # dual step t of this segment uses the segment state n - t
             self._dual_steps(n)
+        self.fwd.check_device_errors()
+        self.dual.check_device_errors()
         return self.w_dual.clone()
 
     def gain_and_dual(self, u0_dev: torch.Tensor):

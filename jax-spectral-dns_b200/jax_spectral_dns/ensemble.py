@@ -119,6 +119,8 @@ class Ensemble:
             main.wait_stream(s)
         stop.record(main)
         torch.cuda.synchronize(self.device)
+        for plan in self.plans:
+            plan.check_device_errors()
         return start.elapsed_time(stop)
 
     def run_sequential(self, runs: Optional[List[int]] = None) -> float:
@@ -130,6 +132,8 @@ class Ensemble:
             self._replay(i)
         stop.record(main)
         torch.cuda.synchronize(self.device)
+        for plan in self.plans:
+            plan.check_device_errors()
         return start.elapsed_time(stop)
 
     def energies(self) -> np.ndarray:
@@ -240,6 +244,8 @@ class BatchedEnsemble:
             main.wait_stream(s)
         stop.record(main)
         torch.cuda.synchronize(self.device)
+        for g in self.groups:
+            g["plan"].check_device_errors()
         return start.elapsed_time(stop)
 
     def energies(self) -> np.ndarray:

@@ -248,6 +248,7 @@ class NavierStokesVelVort(Equation):
         st = to_device_layout(vel_hat_data)
         dp = torch.tensor([float(dPdx)], dtype=torch.float64, device=st.device)
         plan.step(st, dp, int(time_step), 1)
+        plan.check_device_errors()
         return to_reference_layout(st), float(dp.item())
 
     def perform_time_step(self, vel_hat_data=None, dPdx=None, time_step: Optional[int] = None
@@ -275,6 +276,15 @@ class NavierStokesVelVort(Equation):
         (n_steps + 1, 3, Ny, Mx, Mz) including the initial one."""
         plan = self.get_plan(first_step)
         self._prepare_plan_history(plan)
+        used = {id(plan): plan}
+        out = self._run_device(plan, used, state, dpdx, first_step, n_steps, keep_trajectory)
+        # the results are visible to the caller from here on: raise if a
+        # kernel gave up a bounded wait or the state became non-finite
+        for p in used.values():
+            p.check_device_errors()
+        return out
+
+    def _run_device(self, plan, used, state, dpdx, first_step, n_steps, keep_trajectory):
         if self._time_dependent():
             traj = dps = None
             if keep_trajectory:
@@ -284,6 +294,7 @@ class NavierStokesVelVort(Equation):
                 dps[0] = dpdx[0]
             for t in range(n_steps):
                 plan = self.get_plan(first_step + t)
+                used[id(plan)] = plan
                 self._prepare_plan_history(plan)
                 self._prepare_step(plan, first_step + t)
                 plan.step(state, dpdx, first_step + t, 1)

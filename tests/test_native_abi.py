@@ -44,8 +44,27 @@ def test_binding_covers_header(lib):
 
 
 def test_abi_version_and_error_strings(lib):
-    assert lib.jsd_abi_version() == 2
+    from jax_spectral_dns import _native
+
+    assert lib.jsd_abi_version() == _native.ABI_VERSION == 3
     assert isinstance(lib.jsd_last_error(), bytes)
+
+
+def test_status_codes_match_header():
+    """The binding's status codes are the header's enum values."""
+    from jax_spectral_dns import _native
+
+    src = open(HEADER).read()
+    codes = dict(re.findall(r"(JSD_ERR_[A-Z]+) = (-\d+)", src))
+    assert "JSD_ERR_NONFINITE" in codes
+    for name, val in codes.items():
+        assert getattr(_native, name) == int(val), name
+
+
+def test_wait_limit_argument_checks_without_gpu(lib):
+    """jsd_set_wait_limit validates before touching a plan."""
+    assert lib.jsd_set_wait_limit(None, 10) == -1
+    assert lib.jsd_wait_limit(None) == 0
 
 
 def test_plan_create_rejects_bad_descriptor_without_gpu(lib):

@@ -55,3 +55,15 @@ def test_single_process_aggregation_is_local():
     assert not dist.is_initialized()
     assert bench.aggregate_over_ranks(7.5, 42) == (7.5, 42)
     assert bench.split_runs("abcde", 0, 1) == list("abcde")
+
+
+def test_ensemble_smaller_than_world_is_rejected():
+    """An ensemble with fewer runs than ranks would leave a rank without work
+    while its peers wait for it in the aggregation: bench.py refuses it."""
+    import subprocess
+
+    env = dict(os.environ, WORLD_SIZE="4", RANK="0", LOCAL_RANK="0")
+    res = subprocess.run([sys.executable, os.path.join(REPO, "bench.py"), "--ensemble", "3"], env=env,
+                         capture_output=True, text=True, timeout=120)
+    assert res.returncode == 2
+    assert "smaller than the number of ranks" in res.stderr
