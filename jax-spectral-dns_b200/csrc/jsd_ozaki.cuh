@@ -3,15 +3,20 @@
 //
 // C (M x N) = A (M x K) B (K x N), A a constant operator (M, K <= 129), B a
 // batch of FP64 fields. Each row i of A and each column j of B is scaled by a
-// power of two so that its largest entry is below 1, and the scaled values
-// are cut into 8 signed 7-bit integer slices (56 bits):
-//   a_ik = 2^ea_i sum_p alpha_ikp 2^(-7p),  b_kj = 2^eb_j sum_q beta_kjq 2^(-7q),
-//   alpha, beta in [-127, 127], p, q = 1..8.
+// power of two and cut into 8 signed 7-bit integer slices:
+//   a_ik = 2^ea_i sum_p alpha_ikp 2^(-7p),  b_kj = 2^(eb_j + 2) sum_q beta_kjq 2^(-7q),
+//   p, q = 1..8. A's digits (packed once on the host) are sign-magnitude,
+//   alpha in [-127, 127], of |a| / 2^ea < 1 (56 bits). B's digits (cut on the
+//   device every call) are balanced base-128 digits, beta in [-64, 63], of the
+//   integer trunc(b 2^(54 - eb)), |.| < 2^54: adding the bias 64 sum_j 128^j
+//   makes it a non-negative 56-bit integer whose 7-bit fields minus 64 are the
+//   digits, so slicing a value costs one conversion, one 64-bit add and a
+//   field extraction per slice (54 bits, against FP64's 53).
 // The products alpha_p beta_q are exact int8 tensor-core GEMMs with exact
 // int32 accumulation; the pairs with p + q <= 9 (36 products) are kept and
 // summed per diagonal d = p + q into 8 int32 accumulators in tensor memory (at
-// most 8 pairs x K=128 x 127^2 < 2^31), which the epilogue combines in FP64:
-//   c_ij = 2^(ea_i + eb_j - 14) sum_d acc_d 2^(-7 (d - 2)).
+// most 8 pairs x K=128 x 127 x 64 < 2^31), which the epilogue combines in FP64:
+//   c_ij = 2^(ea_i - 14) 2^(eb_j + 2) sum_d acc_d 2^(-7 (d - 2)).
 // The error bound is of the order of an FP64 GEMM's (the dropped terms and the
 // slice remainders are below 2^-56 of |a_i|max |b_j|max per product), so the
 // products stay FP64-accurate while the arithmetic runs at int8 tensor rate.
@@ -25,7 +30,7 @@
 // diagonal p + q: 32 MMAs of N = 32..256 per tile instead of 36 x 4 narrow
 // ones, so the operands are read from shared memory once per wide product.
 //
-// One persistent CTA of 25 warps per SM, each CTA a contiguous range of
+// One persistent CTA of 21 warps per SM, each CTA a contiguous range of
 // 32-column tiles:
 //   * warps 0-15 (converters, warp w = rows 8w..8w+7, lane = column): load
 //     their 8 x 32 block of the tile straight from global memory (a warp reads
@@ -36,11 +41,12 @@
 //   * warp 16 (issuer): keeps A's 8 slices resident (bulk copy, reloaded when
 //     the operator changes), issues the 32 MMAs (kind::i8, M = 128) into one of
 //     two accumulator sets of 8 x 32 TMEM columns and commits to an mbarrier;
-//   * warps 17-24 (epilogue, TMEM lane quadrant = warp % 4 = row block, half of
-//     the columns each): read the 8 accumulators (tcgen05.ld, two per wait),
+//   * warps 17-20 (epilogue, TMEM lane quadrant = warp % 4 = row block): per
+//     16-column half, read the 8 accumulators (tcgen05.ld, two per wait),
 //     combine, scale and add the FP64 extras, write the 32 x 16 block into a
 //     128-byte-swizzled shared-memory slot and store it with one TMA store
-//     (rows and columns outside C are not written).
+//     (rows and columns outside C are not written). 21 warps keep at most 6 on
+//     a scheduler, which leaves each thread 80 registers.
 // A column holding a NaN or an infinity gets a NaN column scale, so the whole
 // output column is NaN as in an FP64 product (the slices alone would drop it).
 // Every mbarrier wait has an iteration limit (a kernel argument); on expiry
@@ -69,18 +75,19 @@ constexpr int kOzABytes = kOzSlices * kOzASlice;     // 131072
 constexpr int kOzBRows = kOzSlices * kOzN;           // stacked B operand rows (256)
 constexpr int kOzBBytes = kOzBRows * kOzK;           // 32768
 constexpr int kOzTmemCols = 2 * kOzDiags * kOzN;     // 512: two accumulator sets
-constexpr int kOzConvWarps = 16, kOzEpiWarps = 8;
+constexpr int kOzConvWarps = 16, kOzEpiWarps = 4;
 constexpr int kOzConvRows = kOzK / kOzConvWarps;  // B rows per converter lane (8)
 constexpr int kOzIssuerWarp = kOzConvWarps;
-constexpr int kOzThreads = 32 * (kOzConvWarps + 1 + kOzEpiWarps);  // 800
-constexpr int kOzOutCols = kOzN / 2;                 // columns per epilogue warp (16 doubles = 128 bytes)
-constexpr int kOzOutSlot = 32 * kOzOutCols * 8;      // 4096: one epilogue warp's swizzled output block
+constexpr int kOzThreads = 32 * (kOzConvWarps + 1 + kOzEpiWarps);  // 672
+constexpr int kOzOutCols = kOzN / 2;                 // columns per epilogue pass (16 doubles = 128 bytes)
+constexpr int kOzOutSlot = 32 * kOzOutCols * 8;      // 4096: one epilogue pass's swizzled output block
 // per tile buffer (doubles): column scales, B row 128 (K = 129), row-128 dots (M = 129)
 constexpr int kOzSideScale = 0, kOzSideBx = kOzN, kOzSideDot = 2 * kOzN, kOzSideDoubles = 3 * kOzN;
 // partial-maximum exponents of a column that is all zero / holds a NaN or an infinity
 constexpr int kOzExpZero = -1000, kOzExpBad = 1 << 20;
 // shared memory: A slices | B slices | output slots | side data | exchange (exponents, dots) | barriers
-constexpr size_t kOzOffB = kOzABytes, kOzOffOut = kOzOffB + kOzBBytes, kOzOffSide = kOzOffOut + kOzEpiWarps * kOzOutSlot;
+constexpr size_t kOzOffB = kOzABytes, kOzOffOut = kOzOffB + kOzBBytes,
+                 kOzOffSide = kOzOffOut + 2 * kOzEpiWarps * kOzOutSlot;
 constexpr size_t kOzOffPExp = kOzOffSide + 2 * sizeof(double) * kOzSideDoubles;
 constexpr size_t kOzOffPDot = kOzOffPExp + 2 * sizeof(int) * kOzConvWarps * kOzN;
 constexpr size_t kOzOffBars = kOzOffPDot + 2 * sizeof(double) * kOzConvWarps * kOzN;
@@ -93,22 +100,26 @@ __host__ __device__ __forceinline__ int oz_offset(int R, int r, int k) {
   return ((k >> 4) * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 15);
 }
 
-// 2^e as a double (|e| well inside the normal range)
+// 2^e as a double (|e| well inside the normal range; on the device built from
+// the exponent field)
 __host__ __device__ __forceinline__ double oz_pow2(int e) {
 #if defined(__CUDA_ARCH__)
-  return ldexp(1.0, e);
+  return __longlong_as_double((long long)(e + 1023) << 52);
 #else
   return std::ldexp(1.0, e);
 #endif
 }
 
-// exponent e with |x| < 2^e for every |x| <= m (0 for m = 0)
+// exponent e with |x| < 2^e for every |x| <= m (0 for m = 0), clamped at -900:
+// frexp's exponent, on the device read from the exponent field (a subnormal m
+// has e <= -1022, so the clamp covers it)
 __host__ __device__ __forceinline__ int oz_exponent(double m) {
   if (!(m > 0.0)) return 0;
-  int e = 0;
 #if defined(__CUDA_ARCH__)
-  (void)frexp(m, &e);
+  const int biased = (int)((unsigned long long)__double_as_longlong(m) >> 52) & 0x7ff;
+  const int e = biased == 0 ? -1022 : biased - 1022;
 #else
+  int e = 0;
   (void)std::frexp(m, &e);
 #endif
   return e < -900 ? -900 : e;
@@ -142,6 +153,46 @@ __host__ __device__ __forceinline__ void oz_pack(const double* xs, uint32_t (*w)
       for (int k = 0; k < 4; ++k) W |= (uint32_t)((a[k] >> sh) & 127u) << (8 * k);
       const uint32_t nW = (0x80808080u - W) ^ 0x80808080u;
       w[q][g] = W ^ ((W ^ nW) & neg);
+    }
+  }
+}
+
+// 64 sum_{j<8} 128^j: makes trunc(xs) + kOzBias non-negative and below 2^56
+// for |xs| < 2^54, with every 7-bit field of the sum equal to its balanced
+// digit + 64
+constexpr unsigned long long kOzBias = 0x0081020408102040ull;
+
+// Balanced base-128 slices of 4 G integer-valued doubles |xs| < 2^54 (B's
+// side), packed little-endian: byte j of w[q] (G words) is digit q + 1 of
+// xs[j] (weight 128^(7 - q)) as a signed byte in [-64, 63].
+template <int G>
+__host__ __device__ __forceinline__ void oz_pack_b(const double* xs, uint32_t (*w)[G], double scale = 1.0) {
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    uint32_t lo[4], hi[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const unsigned long long z = (unsigned long long)(long long)(xs[4 * g + k] * scale) + kOzBias;
+      lo[k] = (uint32_t)z;
+      hi[k] = (uint32_t)(z >> 32);
+    }
+#pragma unroll
+    for (int q = 0; q < kOzSlices; ++q) {
+      const int sh = 49 - 7 * q;  // lowest bit of the field of digit q + 1
+      uint32_t W = 0u;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        uint32_t f;
+        if (sh >= 32)
+          f = hi[k] >> (sh - 32);
+        else if (sh + 7 <= 32)
+          f = lo[k] >> sh;
+        else
+          f = (lo[k] >> sh) | (hi[k] << (32 - sh));
+        W |= (f & 127u) << (8 * k);
+      }
+      // field f in [0, 127] -> byte f - 64: flip bit 6, and set bit 7 where bit 6 was clear
+      w[q][g] = (W ^ 0x40404040u) ^ ((~W & 0x40404040u) << 1);
     }
   }
 }
@@ -207,6 +258,18 @@ __device__ __forceinline__ void oz_ld16(uint32_t taddr, uint32_t* r) {
       : "r"(taddr));
 }
 
+// *p when c, else 0, as a volatile load: it is issued where it stands (so a
+// prefetch does not move up beside the values still being sliced) and is only
+// waited for where its value is first used
+__device__ __forceinline__ double oz_load_if(const double* p, bool c) {
+  double x = 0.0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t@p ld.global.nc.L1::no_allocate.f64 %0, [%1];\n\t}\n"
+      : "+d"(x)
+      : "l"(p), "r"((int)c));
+  return x;
+}
+
 // int32 -> double with one FP64 add instead of a conversion: the bit pattern
 // 0x43300000:(x ^ 2^31) is the double 2^52 + 2^31 + x (exact below 2^53)
 __device__ __forceinline__ double oz_i2d(uint32_t x) {
@@ -269,24 +332,37 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
   if (warp < kOzConvWarps) {
     // ---------------------------------------------------------------- converters
     const int n = lane, k0 = kOzConvRows * warp;
-    // this lane's 8 values (and, for K = 129, row 128) of tile i: loaded one tile
-    // ahead, once tile i - 1 is cut
+    // tile i = entry e, columns n0..n0+31, walked incrementally (tile t_begin + i);
+    // the entry's fields are re-selected only when the entry changes
+    int e = t_begin / tiles_n, n0 = (t_begin - e * tiles_n) * kOzN;
+    int en = e, n0n = n0;  // the next tile, whose values are prefetched
+    int K = oz_K(b, e), M = oz_M(b, e), Kn = K;
+    const double* xrow = oz_xrow(b, e);
+    const double* Bn = oz_B(b, e);
+    // this lane's 8 values (and, for K = 129, row 128) of the tile: loaded one
+    // tile ahead, once the previous tile is cut
     double v[kOzConvRows], bx = 0.0;
-    auto load_tile = [&](int i, double* dst, double& dbx) {
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
-      const int K = oz_K(b, e), kt = K < kOzK ? K : kOzK;
-      const bool cv = n0 + n < b.N;
-      const double* src = oz_B(b, e) + n0 + n;
+    auto load_next = [&]() {
+      const int kt = Kn < kOzK ? Kn : kOzK;
+      const bool cv = n0n + n < b.N;
+      const double* src = Bn + (size_t)k0 * b.ldb + n0n + n;
 #pragma unroll
-      for (int j = 0; j < kOzConvRows; ++j)
-        dst[j] = (cv && k0 + j < kt) ? __ldg(src + (size_t)(k0 + j) * b.ldb) : 0.0;
-      dbx = (warp == 0 && cv && K > kOzK) ? __ldg(src + (size_t)kOzK * b.ldb) : 0.0;
+      for (int j = 0; j < kOzConvRows; ++j, src += b.ldb) v[j] = oz_load_if(src, cv && k0 + j < kt);
+      bx = oz_load_if(Bn + (size_t)kOzK * b.ldb + n0n + n, warp == 0 && cv && Kn > kOzK);
+      n0n += kOzN;
+      if (n0n >= b.N) {
+        n0n = 0;
+        ++en;
+        if (en < b.count) {
+          Kn = oz_K(b, en);
+          Bn = oz_B(b, en);
+        }
+      }
     };
-    if (nt > 0) load_tile(0, v, bx);
+    if (nt > 0) load_next();
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
-      const int t = t_begin + i, e = t / tiles_n;
-      const int K = oz_K(b, e), kt = K < kOzK ? K : kOzK;
+      const int kt = K < kOzK ? K : kOzK;
       double mx = 0.0, dot = 0.0;
       bool bad = false;
 #pragma unroll
@@ -294,8 +370,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         mx = fmax(mx, fabs(v[j]));
         bad |= !isfinite(v[j]);
       }
-      if (oz_M(b, e) > kOzM) {
-        const double* xrow = oz_xrow(b, e);
+      if (M > kOzM) {
 #pragma unroll
         for (int j = 0; j < kOzConvRows; ++j)
           if (k0 + j < kt) dot = fma(__ldg(xrow + k0 + j), v[j], dot);
@@ -311,20 +386,24 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
       int em = pexp[(buf * kOzConvWarps) * kOzN + n];
 #pragma unroll
       for (int w = 1; w < kOzConvWarps; ++w) em = max(em, pexp[(buf * kOzConvWarps + w) * kOzN + n]);
+      // warp 0: the row-128 dot of the column (partials summed in warp order),
+      // reduced now while few registers are live
+      double dsum = 0.0;
+      if (warp == 0 && M > kOzM) {
+        dsum = pdot[(buf * kOzConvWarps) * kOzN + n];
+#pragma unroll
+        for (int w = 1; w < kOzConvWarps; ++w) dsum += pdot[(buf * kOzConvWarps + w) * kOzN + n];
+      }
       const bool col_bad = em == kOzExpBad;
       const int eb = (em == kOzExpZero || col_bad) ? 0 : em;
-      const double sc = oz_pow2(56 - eb);
+      // a NaN / infinity column is sliced as zeros (its NaN scale marks it)
+      const double sc = col_bad ? 0.0 : oz_pow2(54 - eb);
       uint32_t wd[kOzSlices][kOzConvRows / 4];
-      {
-        double xs[kOzConvRows];
-#pragma unroll
-        for (int j = 0; j < kOzConvRows; ++j) xs[j] = col_bad ? 0.0 : v[j] * sc;
-        oz_pack<kOzConvRows / 4>(xs, wd);
-      }
+      oz_pack_b<kOzConvRows / 4>(v, wd, sc);
       // the next tile's values are in flight while this one waits for its
       // slice buffer (the loads only land in registers at the next tile's use)
       const double bx_cur = bx;
-      if (i + 1 < nt) load_tile(i + 1, v, bx);
+      if (i + 1 < nt) load_next();
       // the B slices are free once the previous tile's MMAs completed; the
       // side buffer once the epilogue of the tile two back is done (which also
       // frees the accumulator set this tile's MMAs will use)
@@ -340,15 +419,23 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         *reinterpret_cast<uint2*>(sB + oz_offset(kOzBRows, q * kOzN + n, k0)) = make_uint2(wd[q][0], wd[q][1]);
       if (warp == 0) {
         double* sd = side + buf * kOzSideDoubles;
-        double x = pdot[(buf * kOzConvWarps) * kOzN + n];
-#pragma unroll
-        for (int w = 1; w < kOzConvWarps; ++w) x += pdot[(buf * kOzConvWarps + w) * kOzN + n];
-        sd[kOzSideDot + n] = x;
-        sd[kOzSideScale + n] = col_bad ? __longlong_as_double(0x7ff8000000000000LL) : oz_pow2(eb);
+        sd[kOzSideDot + n] = dsum;
+        sd[kOzSideScale + n] = col_bad ? __longlong_as_double(0x7ff8000000000000LL) : oz_pow2(eb + 2);
         sd[kOzSideBx + n] = bx_cur;
       }
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       tc_arrive(bar(buf));
+      // advance to the next tile
+      n0 += kOzN;
+      if (n0 >= b.N) {
+        n0 = 0;
+        ++e;
+        if (e < b.count) {
+          K = oz_K(b, e);
+          M = oz_M(b, e);
+          xrow = oz_xrow(b, e);
+        }
+      }
     }
   } else if (warp == kOzIssuerWarp) {
     // ------------------------------------------------------------------- issuer
@@ -406,9 +493,13 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
     }
   } else {
     // ----------------------------------------------------------------- epilogue
-    const int ew = warp - kOzIssuerWarp - 1, quad = warp & 3, half = ew >> 2;
-    const int row = 32 * quad + lane, c0 = kOzOutCols * half;
-    unsigned char* slot = sOut + ew * kOzOutSlot;
+    // warp quad = TMEM lane quadrant = row block; two passes of 16 columns
+    const int ew = warp - kOzIssuerWarp - 1, quad = warp & 3;
+    const int row = 32 * quad + lane;
+    int e = t_begin / tiles_n, n0 = (t_begin - e * tiles_n) * kOzN;
+    int M = oz_M(b, e), mt = M < kOzM ? M : kOzM;
+    double sa = row < mt ? __ldg(oz_row_scale(b, e) + row) : 0.0;
+    double xc = (row < mt && oz_K(b, e) > kOzK) ? __ldg(oz_xcol(b, e) + row) : 0.0;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
       const bool ok = mbar_wait(bar(2 + buf), (i >> 1) & 1, spin) && mbar_wait(bar(buf), (i >> 1) & 1, spin);
@@ -417,49 +508,61 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kOzN;
-      const uint32_t tbase =
-          tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * kOzDiags * kOzN) + (uint32_t)c0;
-      double r[kOzOutCols];
+      const double* sd = side + buf * kOzSideDoubles;
+#pragma unroll 1
+      for (int half = 0; half < 2; ++half) {
+        const int c0 = kOzOutCols * half;
+        unsigned char* slot = sOut + (2 * ew + half) * kOzOutSlot;
+        const uint32_t tbase =
+            tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * kOzDiags * kOzN) + (uint32_t)c0;
+        double r[kOzOutCols];
 #pragma unroll
-      for (int j = 0; j < kOzOutCols; ++j) r[j] = 0.0;
+        for (int j = 0; j < kOzOutCols; ++j) r[j] = 0.0;
 #pragma unroll
-      for (int d = kOzDiags - 1; d >= 1; d -= 2) {  // two loads per wait, highest diagonal first
-        uint32_t hi[16], lo[16];
-        oz_ld16(tbase + (uint32_t)(d * kOzN), hi);
-        oz_ld16(tbase + (uint32_t)((d - 1) * kOzN), lo);
-        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        for (int d = kOzDiags - 1; d >= 1; d -= 2) {  // two loads per wait, highest diagonal first
+          uint32_t hi[16], lo[16];
+          oz_ld16(tbase + (uint32_t)(d * kOzN), hi);
+          oz_ld16(tbase + (uint32_t)((d - 1) * kOzN), lo);
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-        for (int j = 0; j < kOzOutCols; ++j) {
-          r[j] = fma(r[j], 0.0078125, oz_i2d(hi[j]));
-          r[j] = fma(r[j], 0.0078125, oz_i2d(lo[j]));
+          for (int j = 0; j < kOzOutCols; ++j) {
+            r[j] = fma(r[j], 0.0078125, oz_i2d(hi[j]));
+            r[j] = fma(r[j], 0.0078125, oz_i2d(lo[j]));
+          }
+        }
+        // the slot's previous TMA store must have read it before it is rewritten
+        if (lane == 0) tc_bulk_wait_read();
+        __syncwarp();
+        // 128-byte swizzle: 16-byte chunk j of row `lane` sits at chunk j ^ (lane & 7)
+#pragma unroll
+        for (int j = 0; j < kOzOutCols; j += 2) {
+          const double o0 = fma(xc, sd[kOzSideBx + c0 + j], r[j] * sa * sd[kOzSideScale + c0 + j]);
+          const double o1 = fma(xc, sd[kOzSideBx + c0 + j + 1], r[j + 1] * sa * sd[kOzSideScale + c0 + j + 1]);
+          *reinterpret_cast<double2*>(slot + lane * 128 + ((((j >> 1) ^ lane) & 7) << 4)) = make_double2(o0, o1);
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncwarp();
+        if (lane == 0 && 32 * quad < mt && n0 + c0 < b.N) {
+          tc_tma_store_2d(&b.cmap[e], n0 + c0, 32 * quad, slot);
+          tc_bulk_commit();
         }
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      const double* sd = side + buf * kOzSideDoubles;
-      const int M = oz_M(b, e), mt = M < kOzM ? M : kOzM;
-      const double sa = row < mt ? __ldg(oz_row_scale(b, e) + row) : 0.0;
-      const double xc = (row < mt && oz_K(b, e) > kOzK) ? __ldg(oz_xcol(b, e) + row) : 0.0;
-      // the slot's previous TMA store must have read it before it is rewritten
-      if (lane == 0) tc_bulk_wait_read();
-      __syncwarp();
-      // 128-byte swizzle: 16-byte chunk j of row `lane` sits at chunk j ^ (lane & 7)
-#pragma unroll
-      for (int j = 0; j < kOzOutCols; j += 2) {
-        const double o0 = fma(xc, sd[kOzSideBx + c0 + j], r[j] * sa * sd[kOzSideScale + c0 + j]);
-        const double o1 = fma(xc, sd[kOzSideBx + c0 + j + 1], r[j + 1] * sa * sd[kOzSideScale + c0 + j + 1]);
-        *reinterpret_cast<double2*>(slot + lane * 128 + ((((j >> 1) ^ lane) & 7) << 4)) = make_double2(o0, o1);
-      }
-      asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      __syncwarp();
-      if (lane == 0 && 32 * quad < mt && n0 + c0 < b.N) {
-        tc_tma_store_2d(&b.cmap[e], n0 + c0, 32 * quad, slot);
-        tc_bulk_commit();
-      }
       if (M > kOzM && ew == 0 && n0 + lane < b.N) oz_C(b, e)[(size_t)kOzM * b.ldc + n0 + lane] = sd[kOzSideDot + lane];
       tc_arrive(bar(4 + buf));
+      n0 += kOzN;
+      if (n0 >= b.N) {
+        n0 = 0;
+        ++e;
+        if (e < b.count) {
+          M = oz_M(b, e);
+          mt = M < kOzM ? M : kOzM;
+          sa = row < mt ? __ldg(oz_row_scale(b, e) + row) : 0.0;
+          xc = (row < mt && oz_K(b, e) > kOzK) ? __ldg(oz_xcol(b, e) + row) : 0.0;
+        }
+      }
     }
-    // this warp's stores read its slot and write C: both done before the CTA ends
+    // this warp's stores read its slots and write C: both done before the CTA ends
     if (lane == 0) tc_bulk_wait_all();
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");

@@ -1,5 +1,6 @@
 // Host-side check of the Ozaki int8 product (jsd_ozaki.cuh): packs A with
-// oz_pack_a and 32-column tiles of B the way the converter warps do (slices
+// oz_pack_a and 32-column tiles of B the way the converter warps do (balanced
+// digits of oz_pack_b; slices
 // stacked into one 256-row operand), emulates the tensor-core products by
 // reading both operands back through their canonical-layout offsets (int32
 // accumulation per diagonal), combines like
@@ -54,13 +55,13 @@ static void run_case(int M, int K, int N, unsigned long long seed) {
       }
       xdot[lane] = dot;
       const int eb = oz_exponent(mx);
-      colscale[lane] = oz_pow2(eb);
-      const double sc = oz_pow2(56 - eb);
+      colscale[lane] = oz_pow2(eb + 2);
+      const double sc = oz_pow2(54 - eb);
       for (int k0 = 0; k0 < kOzK; k0 += 16) {
         double xs[16];
         for (int j = 0; j < 16; ++j) xs[j] = v[k0 + j] * sc;
         uint32_t w[kOzSlices][4];
-        oz_pack<4>(xs, w);
+        oz_pack_b<4>(xs, w);
         for (int q = 0; q < kOzSlices; ++q)
           for (int j = 0; j < 16; ++j)
             bs[oz_offset(kOzBRows, q * kOzN + lane, k0) + j] = (unsigned char)((w[q][j >> 2] >> (8 * (j & 3))) & 0xFFu);
