@@ -145,6 +145,25 @@ int jsd_energy_runs(jsd_plan* plan, const void* state, double* out, void* stream
  * numbers. No counterpart in the reference. */
 int jsd_set_batch_active(jsd_plan* plan, int n_runs);
 
+/* Discrete adjoint of the linearised perturbation step: replaces `cotangent`
+ * (device, state layout), the gradient of an objective with respect to the
+ * state after n_steps steps of this plan, by its gradient with respect to the
+ * state before them, i.e. applies the exact transpose of n_steps steps (for
+ * the real inner product of the real and imaginary parts) in reverse. The
+ * linearised step is linear and the same every step, so no forward states are
+ * needed. Linearised perturbation plans of one run, coupling term on, no
+ * mass-flux control. Stands in for jax.grad through the reference's forward
+ * solve (optimiser.py:120, with navier_stokes.py:1219-1813); unlike the
+ * reference's dual solver (navier_stokes_perturbation_dual.py:850-1120), which
+ * it does not replace, it is the exact derivative of the discrete step. */
+int jsd_step_adjoint(jsd_plan* plan, void* cotangent, int n_steps, void* stream);
+
+/* Gradient of jsd_energy's value with respect to the real and imaginary parts
+ * of every coefficient of `state`, written to `out` (device, state layout):
+ * the derivative of VectorField.no_hat().energy() (field.py:607-611,
+ * 1468-1474). */
+int jsd_energy_grad(jsd_plan* plan, const void* state, void* out, void* stream);
+
 /* coupling_term of the perturbation and dual equations
  * (navier_stokes_perturbation.py:401-415; the extra terms of
  * navier_stokes_perturbation.py:217-237 and ..._dual.py:270-292 when off).

@@ -32,6 +32,7 @@
 #include "jsd_spectral_sq.cuh"
 #include "jsd_tc05.cuh"
 #include "jsd_ozaki.cuh"
+#include "jsd_adjoint.cuh"
 
 using namespace jsd;
 
@@ -219,6 +220,12 @@ struct jsd_plan {
   std::vector<void*> allocs;
   const double2* history = nullptr;
   int n_history = 0;
+  // Discrete adjoint of the linearised perturbation step (jsd_step_adjoint):
+  // transposed operators (padded to lda), transposed mean-flow matrices per
+  // stage, and small cotangent buffers of the (0,0) system
+  double *VinvD_T = nullptr, *Vinv_T = nullptr, *Vfull_T = nullptr, *DVfull_T = nullptr, *D_T = nullptr;
+  double *lr_T = nullptr, *li_T = nullptr;
+  double2 *adj_conv = nullptr, *adj_x00 = nullptr, *adj_ub = nullptr;
   // Carried between stages of one jsd_step call: vnt / omnt hold V^-1 v and
   // V^-1 omega_y of the current state, dvn holds dv/dy of the current state.
   bool ev_valid = false, om_valid = false, dv_valid = false;
@@ -820,6 +827,84 @@ int mass_flux(jsd_plan* p, double2* state, double* dpdx, cudaStream_t s) {
   JSD_LAUNCHED("k_roundtrip_shift");
   JSD_CUDA(cudaMemcpyAsync(state, p->tmp, fs * sizeof(double2), cudaMemcpyDeviceToDevice, s));
   p->om_valid = false;  // u changed; v (and so V^-1 v, dv/dy) did not
+  return 0;
+}
+
+// Transpose of one stage of the linearised perturbation step (jsd_adjoint.cuh):
+// lam holds the cotangent of the stage's output state on entry and of its
+// input state on return. hv_old / hg_old carry the cotangents of the terms a
+// stage hands to the next (`last`: none, for the last stage of a step);
+// adj_conv[st] the cotangent of the stage's conv00.
+int stage_adj(jsd_plan* p, double2* lam, int st, bool last, cudaStream_t s) {
+  const Geo& g = p->g;
+  const size_t fs = (size_t)g.ny * g.nk;
+  const int ny = g.ny, ni = g.ny - 2;
+  const size_t E = p->edoubles;
+  const size_t rowd = 2 * (size_t)g.nk;
+  double2 *lu = lam, *lv = lam + fs, *lw = lam + 2 * fs;
+  const int blk = 256;
+  // 9'
+  k_reconstruct_adj<<<grid_for(fs, blk), blk, 0, s>>>(g, lu, lw, p->dvn, p->om, p->adj_ub);
+  JSD_LAUNCHED("k_reconstruct_adj");
+  // 8': cotangents of V^-1 v (from v and from dv/dy) and of V^-1 omega_y
+  {
+    GemmBatch b = gemm_batch(p);
+    add_entry(b, p->Vfull_T, (const double*)lv, p->T + 0 * E, ni, ny);
+    add_entry(b, p->DVfull_T, (const double*)p->dvn, p->T + 1 * E, ni, ny);
+    add_entry(b, p->Vfull_T, (const double*)p->om, p->T + 2 * E, ni, ny);
+    int rc = launch_gemm(p, b, ni, kSiteEigIn, s);
+    if (rc) return rc;
+  }
+  // 6'
+  {
+    EigTables t{p->lam, p->c0, p->cN, p->sgn, p->w0, p->wN, nullptr};
+    StageCoef sc{kAlpha[st], kBeta[st], kGamma[st], kXi[st], p->desc.dt, p->desc.dt_explicit, p->desc.re_tau,
+                 st == 0 ? 1 : 0};
+    const int N = 2 * g.nk;
+    k_eigen_update_adj<<<(N + kEigCols - 1) / kEigCols, kEigCols * kEigParts, 0, s>>>(
+        g, t, sc, last ? 1 : 0, p->T + 0 * E, p->T + 1 * E, p->T + 2 * E, p->hv_old, p->hg_old, p->X1, p->T + 3 * E,
+        p->vnt, p->omnt, p->vnt_alt, (double*)p->tmp);
+    JSD_LAUNCHED("k_eigen_update_adj");
+  }
+  // 7'
+  {
+    const size_t n2 = 2 * (size_t)ny;
+    const double dte = p->desc.dt_explicit;
+    const unsigned grid = (unsigned)((n2 + kMeanFlowRows - 1) / kMeanFlowRows);
+    k_mean_flow_adj<<<grid, 32 * kMeanFlowRows, 0, s>>>(g, p->lr_T + (size_t)st * n2 * n2, p->li_T + (size_t)st * n2 * n2,
+                                                        p->adj_ub, dte * kGamma[st], dte * kXi[st], p->adj_x00,
+                                                        p->adj_conv + (size_t)st * n2,
+                                                        st > 0 ? p->adj_conv + (size_t)(st - 1) * n2 : nullptr);
+    JSD_LAUNCHED("k_mean_flow_adj");
+  }
+  // 5': cotangents of q (all rows), H1, h_g, the interior of v and of omega_y
+  {
+    GemmBatch b = gemm_batch(p);
+    add_entry(b, p->VinvD_T, p->X1, (double*)p->q, ny, ni);
+    add_entry(b, p->Vinv_T, p->T + 3 * E, (double*)p->H1 + rowd, ni, ni);
+    add_entry(b, p->Vinv_T, p->vnt, (double*)p->hg + rowd, ni, ni);
+    add_entry(b, p->Vinv_T, p->omnt, (double*)p->tmp + rowd, ni, ni);
+    add_entry(b, p->Vinv_T, p->vnt_alt, (double*)p->Dfld + rowd, ni, ni);
+    int rc = launch_gemm(p, b, ny, kSiteEigOut, s);
+    if (rc) return rc;
+  }
+  // 4' .. 2': the state cotangent but D^T dv_bar, and dv_bar
+  {
+    const size_t n2 = 2 * (size_t)ny;
+    k_linear_terms_adj<<<grid_for(fs, blk), blk, 0, s>>>(g, p->ub, p->dub, p->q, p->H1, p->hg,
+                                                        p->adj_conv + (size_t)st * n2, p->Dfld, p->tmp, p->adj_x00,
+                                                        lu, lv, lw, p->Dfld + fs);
+    JSD_LAUNCHED("k_linear_terms_adj");
+  }
+  // 1': v_bar += D^T dv_bar
+  {
+    GemmBatch b = gemm_batch(p);
+    add_entry(b, p->D_T, (const double*)(p->Dfld + fs), (double*)(p->Dfld + 2 * fs), ny, ny);
+    int rc = launch_gemm(p, b, ny, kSiteDfield, s);
+    if (rc) return rc;
+  }
+  k_add_field<<<grid_for(fs, blk), blk, 0, s>>>(fs, p->Dfld + 2 * fs, lv);
+  JSD_LAUNCHED("k_add_field");
   return 0;
 }
 
@@ -1440,6 +1525,35 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
       }
     }
     JSD_TRY(upload(p, &p->lr_ns, lr.data(), lr.size()));
+    if (d->kind == JSD_KIND_PERTURBATION && d->linearise && nb == 1 && !d->constant_mass_flux) {
+      // transposes for the discrete adjoint (jsd_step_adjoint)
+      std::vector<double> lrT(lr.size()), liT(lr.size());
+      for (size_t m = 0; m < 3; ++m)
+        for (size_t i = 0; i < n2; ++i)
+          for (size_t j = 0; j < n2; ++j) {
+            lrT[m * n2 * n2 + j * n2 + i] = lr[m * n2 * n2 + i * n2 + j];
+            liT[m * n2 * n2 + j * n2 + i] = d->lhs_inv_ns[m * n2 * n2 + i * n2 + j];
+          }
+      JSD_TRY(upload(p, &p->lr_T, lrT.data(), lrT.size()));
+      JSD_TRY(upload(p, &p->li_T, liT.data(), liT.size()));
+      auto transpose = [](const double* a, int rows, int cols) {
+        std::vector<double> t((size_t)rows * cols);
+        for (int r = 0; r < rows; ++r)
+          for (int c = 0; c < cols; ++c) t[(size_t)c * rows + r] = a[(size_t)r * cols + c];
+        return t;
+      };
+      const std::vector<double> vdT = transpose(VinvD.data(), ni, ny), viT = transpose(d->Vinv, ni, ni),
+                                vfT = transpose(Vfull.data(), ny, ni), dvT = transpose(DVfull.data(), ny, ni),
+                                dT = transpose(d->D, ny, ny);
+      JSD_TRY(upload_padded(p, &p->VinvD_T, vdT.data(), ny, ni, p->lda));
+      JSD_TRY(upload_padded(p, &p->Vinv_T, viT.data(), ni, ni, p->lda));
+      JSD_TRY(upload_padded(p, &p->Vfull_T, vfT.data(), ni, ny, p->lda));
+      JSD_TRY(upload_padded(p, &p->DVfull_T, dvT.data(), ni, ny, p->lda));
+      JSD_TRY(upload_padded(p, &p->D_T, dT.data(), ny, ny, p->lda));
+      JSD_TRY(dev_alloc(p, (void**)&p->adj_conv, 3 * n2 * sizeof(double2)));
+      JSD_TRY(dev_alloc(p, (void**)&p->adj_x00, n2 * sizeof(double2)));
+      JSD_TRY(dev_alloc(p, (void**)&p->adj_ub, n2 * sizeof(double2)));
+    }
   }
   if (d->base_u) JSD_TRY(upload(p, &p->ub, d->base_u, ny));
   if (d->base_du) JSD_TRY(upload(p, &p->dub, d->base_du, ny));
@@ -1552,6 +1666,39 @@ int jsd_energy_runs(jsd_plan* plan, const void* state, double* out, void* stream
   k_weighted_total_runs_sliced<<<g.nb, 32, 0, s>>>(g.ny, g.nb, plan->yw, plan->partial, 0.25 * g.c_inv * g.c_inv,
                                                     out);
   JSD_LAUNCHED("k_weighted_total_runs_sliced");
+  return 0;
+}
+
+int jsd_step_adjoint(jsd_plan* plan, void* cotangent, int n_steps, void* stream) {
+  if (!plan || !cotangent || n_steps < 0) return fail(JSD_ERR_ARG, "null argument");
+  if (!plan->VinvD_T)
+    return fail(JSD_ERR_ARG, "the discrete adjoint covers linearised perturbation plans of one run without "
+                             "mass-flux control");
+  if (!plan->coupling) return fail(JSD_ERR_ARG, "the discrete adjoint needs coupling_term on");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t n2 = 2 * (size_t)plan->g.ny;
+  double2* lam = static_cast<double2*>(cotangent);
+  for (int t = 0; t < n_steps; ++t) {
+    JSD_CUDA(cudaMemsetAsync(plan->adj_conv, 0, 3 * n2 * sizeof(double2), s));
+    for (int st = 2; st >= 0; --st) {
+      int rc = stage_adj(plan, lam, st, st == 2, s);
+      if (rc) return rc;
+    }
+  }
+  // the workspace the forward step carries between stages was overwritten
+  plan->ev_valid = plan->om_valid = plan->dv_valid = false;
+  return 0;
+}
+
+int jsd_energy_grad(jsd_plan* plan, const void* state, void* out, void* stream) {
+  if (!plan || !state || !out) return fail(JSD_ERR_ARG, "null argument");
+  if (plan->g.nb > 1) return fail(JSD_ERR_ARG, "single-run entry point called on a batch plan (see jsd_energy_runs)");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const Geo& g = plan->g;
+  const size_t total = 3 * (size_t)g.ny * g.nk;
+  k_energy_grad<<<grid_for(total, 256), 256, 0, s>>>(g, static_cast<const double2*>(state), plan->yw,
+                                                    0.5 * g.c_inv * g.c_inv, static_cast<double2*>(out));
+  JSD_LAUNCHED("k_energy_grad");
   return 0;
 }
 

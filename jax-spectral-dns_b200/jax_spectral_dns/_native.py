@@ -53,7 +53,7 @@ EXPORTED = (
     "jsd_energy_runs", "jsd_set_batch_active", "jsd_batch_active",
     "jsd_split_kernel", "jsd_set_split_kernel", "jsd_device_error",
     "jsd_set_coupling_term", "jsd_set_base_flow", "jsd_eig_kernel", "jsd_set_eig_kernel",
-    "jsd_set_wait_limit", "jsd_wait_limit",
+    "jsd_set_wait_limit", "jsd_wait_limit", "jsd_step_adjoint", "jsd_energy_grad",
 )
 
 ABI_VERSION = 3  # JSD_ABI_VERSION of include/jsd.h this binding is written for
@@ -124,6 +124,8 @@ def load(path: str = LIB_PATH):
     lib.jsd_device_error.argtypes = [vp, vp]
     lib.jsd_set_wait_limit.argtypes = [vp, ctypes.c_int]
     lib.jsd_wait_limit.argtypes = [vp]
+    lib.jsd_step_adjoint.argtypes = [vp, vp, ctypes.c_int, vp]
+    lib.jsd_energy_grad.argtypes = [vp, vp, vp, vp]
     lib.jsd_set_coupling_term.argtypes = [vp, ctypes.c_int]
     lib.jsd_set_base_flow.argtypes = [vp, vp, vp, vp]
     lib.jsd_set_batch_active.argtypes = [vp, ctypes.c_int]

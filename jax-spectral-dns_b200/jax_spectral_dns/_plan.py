@@ -221,6 +221,22 @@ class StepPlan:
                       "jsd_step_trajectory")
         return traj
 
+    def step_adjoint(self, cotangent: torch.Tensor, n_steps: int) -> None:
+        """Discrete adjoint (linearised perturbation plans): replace the gradient
+        with respect to the state after n_steps steps, in place, by the gradient
+        with respect to the state before them (jsd_step_adjoint)."""
+        assert cotangent.is_contiguous() and cotangent.dtype == torch.complex128 and cotangent.device.type == "cuda"
+        _native.check(self.lib.jsd_step_adjoint(self.handle, ctypes.c_void_p(cotangent.data_ptr()), int(n_steps),
+                                                _stream_ptr()), "jsd_step_adjoint")
+
+    def energy_grad(self, state: torch.Tensor) -> torch.Tensor:
+        """Gradient of energy(state) with respect to the real and imaginary parts
+        of the coefficients (device layout, complex128)."""
+        out = torch.empty_like(state)
+        _native.check(self.lib.jsd_energy_grad(self.handle, ctypes.c_void_p(state.data_ptr()),
+                                               ctypes.c_void_p(out.data_ptr()), _stream_ptr()), "jsd_energy_grad")
+        return out
+
     def set_history(self, states: Optional[torch.Tensor]):
         """Forward trajectory (n, 3, Ny, Mx, Mz) for the dual equations."""
         self._history = states

@@ -1,22 +1,31 @@
-"""Gain G = E(T)/E(0) as a differentiable torch function, backward by the dual step.
+"""Gain G = E(T)/E(0) as a differentiable torch function.
 
 The reference obtains the gradient of the transient-growth gain either with
 jax.value_and_grad through the forward solve (optimiser.py:120) or with its
 dual solver (navier_stokes_perturbation_dual.py:850-1120): forward run, dual run
 backward from -u(T) with Re and dt negated (dual step t frozen at the forward
 state u(T - t)), gradient (u0 - v0) / E0 in the energy inner product. This
-module puts the dual-solver gradient behind ``torch.autograd.Function``:
+module provides both behind ``torch.autograd.Function``:
 
-* forward: N = int(T/dt) native forward steps, keeping the state every K steps
-  (checkpoints) instead of the whole trajectory;
-* backward: for each K-step segment, last first, recompute the segment's
-  K + 1 forward states from its checkpoint (only the nonlinear dual needs
-  them), register them with the dual plan and take K dual steps.
-
-Memory is N/K + K + 1 states instead of N + 1; the cost is one forward pass,
-one recompute pass and one dual pass (about 3 forward costs). With K >= N the
-forward pass itself records the N + 1 states (there is one segment and nothing
-to recompute): N + 1 states of memory, one forward and one dual pass.
+* ``gradient="discrete"`` (the default for the linearised equations): the
+  exact derivative of the computed gain, like jax.grad of the forward solve.
+  The linearised step is a fixed linear map S, so dG/du0 =
+  (S^T)^N grad E(u_N) / E0 - G grad E(u0) / E0, with S^T applied by the
+  hand-written transpose of the step (jsd_step_adjoint) and grad E by
+  jsd_energy_grad; no forward states are kept, and the cost is one forward and
+  one adjoint pass.
+* ``gradient="dual"`` (the nonlinear equations): the reference's continuous
+  dual. Forward: N = int(T/dt) native forward steps, keeping the state every
+  K steps (checkpoints) instead of the whole trajectory; backward: for each
+  K-step segment, last first, recompute the segment's K + 1 forward states
+  from its checkpoint (only the nonlinear dual needs them), register them with
+  the dual plan and take K dual steps. Memory is N/K + K + 1 states instead of
+  N + 1; the cost is one forward pass, one recompute pass and one dual pass
+  (about 3 forward costs). With K >= N the forward pass itself records the
+  N + 1 states (there is one segment and nothing to recompute): N + 1 states
+  of memory, one forward and one dual pass. The continuous dual approximates
+  the derivative of the discrete gain (to O(dt), and less well where the
+  dealiasing truncation matters).
 
 Gradients. With the dual field v0 (the dual run started from -u(T)),
 dE(T) = <-v0, du> and dE(0) = <u0, du> in the energy inner product
@@ -24,11 +33,11 @@ dE(T) = <-v0, du> and dE(0) = <u0, du> in the energy inner product
 dG = <(-v0 - G u0) / E0, du>. The reference's ``get_grad`` returns
 (u0 - v0) / E0, which equals it along directions orthogonal to u0 (the
 energy sphere its optimisers move on); ``dual_gradient`` returns that
-reference quantity, the autograd backward returns the full derivative. The
-autograd gradient is the Euclidean one for the real and imaginary parts of
-the spectral coefficients (torch's convention for a real loss of a complex
-input): the energy-metric gradient scaled by 2 * (c^2/4) * w_y per
-coefficient, so that sum Re(conj(grad) * du) = dG for Hermitian du.
+reference quantity. The autograd gradient is the Euclidean one for the real
+and imaginary parts of the spectral coefficients (torch's convention for a
+real loss of a complex input), so that sum Re(conj(grad) * du) = dG; for the
+dual it is the energy-metric gradient scaled by 2 * (c^2/4) * w_y per
+coefficient, exact for Hermitian du.
 """
 from __future__ import annotations
 
@@ -47,13 +56,20 @@ class GainProblem:
     """Forward and dual plans for a perturbation problem about U = u_max (1 - y^2)."""
 
     def __init__(self, modes, phys, lx, lz, re, dt, end_time, linearise, u_max=1.0, checkpoint_every=10,
-                 precision="fp64", device="cuda", use_graphs=True):
+                 precision="fp64", device="cuda", use_graphs=True, gradient: Optional[str] = None):
         self.modes, self.phys = tuple(modes), tuple(phys)
         self.lx, self.lz = float(lx), float(lz)
         self.re_tau = float(re) / u_max
         self.dt = float(dt)
         self.n_steps = max(0, int(end_time / dt))
         self.linearise = bool(linearise)
+        if gradient is None:
+            gradient = "discrete" if self.linearise else "dual"
+        if gradient not in ("discrete", "dual"):
+            raise ValueError("gradient must be 'discrete' or 'dual'")
+        if gradient == "discrete" and not self.linearise:
+            raise ValueError("the discrete adjoint covers the linearised equations; use gradient='dual'")
+        self.gradient = gradient
         self.K = max(1, min(int(checkpoint_every), max(1, self.n_steps)))
         self.full_trajectory = self.K >= self.n_steps  # one segment: record it in the forward pass
         ny = self.modes[1]
@@ -76,6 +92,7 @@ class GainProblem:
         self.w_dp = torch.zeros(1, dtype=torch.float64, device=device)
         self.w_ddp = torch.zeros(1, dtype=torch.float64, device=device)
         self.w_traj = torch.zeros((self.K + 1,) + shape, dtype=torch.complex128, device=device)
+        self.w_adj = torch.zeros(shape, dtype=torch.complex128, device=device)
         self._graphs = {}
         self._traj_owner = None  # checkpoint list of the forward pass whose trajectory w_traj holds
 
@@ -112,6 +129,56 @@ class GainProblem:
                 return GraphedSteps(self.dual, self.w_dual, self.w_ddp, 0, n)
             self.dual.step(self.w_dual, self.w_ddp, 0, n)
         self._run(("dual", n), make)
+
+    def _adj_steps(self, n: int) -> None:
+        """w_adj <- (S^T)^n w_adj (discrete adjoint of n linearised steps)."""
+        if not self.use_graphs:
+            self.fwd.step_adjoint(self.w_adj, n)
+            return
+        g = self._graphs.get(("adj", n))
+        if g is None:
+            probe = self.w_adj.clone()
+            self.fwd.step_adjoint(probe, n)  # loads every kernel before the capture
+            torch.cuda.synchronize(self.w_adj.device)
+            g = torch.cuda.CUDAGraph()
+            stream = torch.cuda.Stream(device=self.w_adj.device)
+            stream.wait_stream(torch.cuda.current_stream(self.w_adj.device))
+            with torch.cuda.stream(stream):
+                with torch.cuda.graph(g, stream=stream):
+                    self.fwd.step_adjoint(self.w_adj, n)
+            torch.cuda.current_stream(self.w_adj.device).wait_stream(stream)
+            self._graphs[("adj", n)] = g
+        g.replay()
+
+    def forward_only(self, u0_dev: torch.Tensor) -> torch.Tensor:
+        """u(T) from u0 (no checkpoints: the linearised adjoint needs none)."""
+        self.w_fwd.copy_(u0_dev)
+        self.w_dp.zero_()
+        t = 0
+        while t < self.n_steps:
+            n = min(self.K, self.n_steps - t)
+            self._fwd_steps(n)
+            t += n
+        self.fwd.check_device_errors()
+        return self.w_fwd.clone()
+
+    def discrete_gradient(self, u0_dev: torch.Tensor, uT: Optional[torch.Tensor] = None):
+        """(gain, dG/du0) with the exact transpose of the linearised step:
+        dG/du0 = (S^T)^N grad E(u_N) / E0 - G grad E(u0) / E0, device layout,
+        Euclidean in the real and imaginary parts."""
+        if uT is None:
+            uT = self.forward_only(u0_dev)
+        e0 = self.energy(u0_dev)
+        gain = self.energy(uT) / e0
+        self.w_adj.copy_(self.fwd.energy_grad(uT) / e0)
+        t = 0
+        while t < self.n_steps:
+            n = min(self.K, self.n_steps - t)
+            self._adj_steps(n)
+            t += n
+        self.fwd.check_device_errors()
+        grad = self.w_adj - (gain / e0) * self.fwd.energy_grad(u0_dev)
+        return gain, grad
 
     # ---- pieces ----------------------------------------------------------
     def energy(self, state: torch.Tensor) -> torch.Tensor:
@@ -174,7 +241,10 @@ class _Gain(torch.autograd.Function):
     @staticmethod
     def forward(ctx, u0, problem: GainProblem):
         u0_dev = to_device_layout(u0.detach(), device=problem.fwd.device)
-        uT, cps = problem.forward_checkpoints(u0_dev)
+        if problem.gradient == "discrete":
+            uT, cps = problem.forward_only(u0_dev), None
+        else:
+            uT, cps = problem.forward_checkpoints(u0_dev)
         e0 = problem.energy(u0_dev)
         gain = problem.energy(uT) / e0
         ctx.problem = problem
@@ -186,6 +256,9 @@ class _Gain(torch.autograd.Function):
     def backward(ctx, grad_out):
         problem = ctx.problem
         u0_dev, uT, cps, e0 = ctx.saved
+        if problem.gradient == "discrete":
+            _, g_euc = problem.discrete_gradient(u0_dev, uT)
+            return to_reference_layout(g_euc).to(ctx.in_device) * grad_out.to(ctx.in_device), None
         v0 = problem.backward_dual(uT, cps)
         G = problem.energy(uT) / e0
         g_energy = (-v0 - G * u0_dev) / e0

@@ -1,6 +1,7 @@
-"""Dual-step gradient of the gain behind torch.autograd.Function, with
-checkpoint/recompute; checked against the reference's dual gradient (golden
-fixtures) and against central finite differences."""
+"""The reference's continuous dual behind torch.autograd.Function
+(gradient="dual"), with checkpoint/recompute; checked against the reference's
+dual gradient (golden fixtures) and against central finite differences. The
+exact discrete adjoint is tested in test_gpu_discrete_adjoint.py."""
 import numpy as np
 import pytest
 import torch
@@ -15,7 +16,8 @@ pytestmark = pytest.mark.gpu
 def _problem(d, linearise, K):
     modes, phys = mode_counts(tuple(d["shape"]))
     n, dt = int(d["n_steps"]), float(d["dt"])
-    return GainProblem(modes, phys, *d["lengths"], float(d["re"]), dt, n * dt, linearise, checkpoint_every=K)
+    return GainProblem(modes, phys, *d["lengths"], float(d["re"]), dt, n * dt, linearise, checkpoint_every=K,
+                       gradient="dual")
 
 
 @pytest.mark.parametrize("K", [1, 3, 50])
@@ -56,7 +58,7 @@ def test_autograd_gain_matches_oracle_derivative(cuda, linearise):
     shape, lx, lz, re, dt, T = (8, 33, 8), 2 * np.pi, np.pi, 3000.0, 0.01, 0.3
     modes, phys = mode_counts(shape)
     u0n = seeded_velocity_hat(shape, (lx, lz), (2, 2), 1e-4, seed=31)
-    p = GainProblem(modes, phys, lx, lz, re, dt, T, linearise, checkpoint_every=7)
+    p = GainProblem(modes, phys, lx, lz, re, dt, T, linearise, checkpoint_every=7, gradient="dual")
     x = torch.as_tensor(u0n, device="cuda").clone().requires_grad_(True)
     G = gain(x, p)
     G.backward()
@@ -82,7 +84,7 @@ def test_autograd_gain_vs_central_differences(cuda, linearise, tol):
     truncation of the -K slots entirely; this test keeps them empty.)"""
     shape, lx, lz = (8, 33, 8), 2 * np.pi, np.pi
     modes, phys = mode_counts(shape)
-    p = GainProblem(modes, phys, lx, lz, 3000.0, 0.01, 0.3, linearise, checkpoint_every=7)
+    p = GainProblem(modes, phys, lx, lz, 3000.0, 0.01, 0.3, linearise, checkpoint_every=7, gradient="dual")
     u0 = torch.as_tensor(seeded_velocity_hat(shape, (lx, lz), (2, 2), 1e-4, seed=31), device="cuda")
     x = u0.clone().requires_grad_(True)
     G = gain(x, p)
