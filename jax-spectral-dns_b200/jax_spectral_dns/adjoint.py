@@ -93,6 +93,8 @@ class GainProblem:
         self.w_ddp = torch.zeros(1, dtype=torch.float64, device=device)
         self.w_traj = torch.zeros((self.K + 1,) + shape, dtype=torch.complex128, device=device)
         self.w_adj = torch.zeros(shape, dtype=torch.complex128, device=device)
+        self.w_traj2 = None  # second segment buffer of the pipelined recompute (allocated on first use)
+        self._side = None
         self._graphs = {}
         self._traj_owner = None  # checkpoint list of the forward pass whose trajectory w_traj holds
 
@@ -113,22 +115,33 @@ class GainProblem:
             self.fwd.step(self.w_fwd, self.w_dp, 0, n)
         self._run(("fwd", n), make)
 
-    def _fwd_traj(self, n: int) -> None:
+    def _traj_buf(self, b: int) -> torch.Tensor:
+        if b == 0:
+            return self.w_traj
+        if self.w_traj2 is None:
+            self.w_traj2 = torch.zeros_like(self.w_traj)
+        return self.w_traj2
+
+    def _fwd_traj(self, n: int, b: int = 0) -> None:
+        traj_buf = self._traj_buf(b)
+
         def make(capture):
             if capture:
-                return GraphedSteps(self.fwd, self.w_fwd, self.w_dp, 0, n, trajectory=self.w_traj)
+                return GraphedSteps(self.fwd, self.w_fwd, self.w_dp, 0, n, trajectory=traj_buf)
             traj = self.fwd.step_trajectory(self.w_fwd, self.w_dp, 0, n)
-            self.w_traj[: n + 1].copy_(traj)
-        self._run(("traj", n), make)
+            traj_buf[: n + 1].copy_(traj)
+        self._run(("traj", n, b), make)
 
-    def _dual_steps(self, n: int) -> None:
+    def _dual_steps(self, n: int, b: int = 0) -> None:
+        traj_buf = self._traj_buf(b)
+
         def make(capture):
             if not self.linearise:
-                self.dual.set_history(self.w_traj[: n + 1])
+                self.dual.set_history(traj_buf[: n + 1])
             if capture:
                 return GraphedSteps(self.dual, self.w_dual, self.w_ddp, 0, n)
             self.dual.step(self.w_dual, self.w_ddp, 0, n)
-        self._run(("dual", n), make)
+        self._run(("dual", n, b), make)
 
     def _adj_steps(self, n: int) -> None:
         """w_adj <- (S^T)^n w_adj (discrete adjoint of n linearised steps)."""
@@ -209,22 +222,51 @@ class GainProblem:
 
     def backward_dual(self, uT: torch.Tensor, cps) -> torch.Tensor:
         """Dual run from -u(T) to t = 0, recomputing each segment's forward
-        states from its checkpoint when the dual needs them."""
+        states from its checkpoint when the dual needs them. The recompute of
+        the next segment (on a second stream, into the other of two segment
+        buffers) overlaps the dual run over the current one; events order each
+        dual run after its segment's recompute and each recompute after the
+        dual run that last read its buffer."""
         self.w_dual.copy_(-uT)
         self.w_ddp.zero_()
         bounds = list(range(0, self.n_steps, self.K)) + [self.n_steps]
-        for seg in range(len(bounds) - 2, -1, -1):
-            s0, s1 = bounds[seg], bounds[seg + 1]
-            n = s1 - s0
-            # (a later forward pass may have overwritten the recorded trajectory:
-            # then the single segment is recomputed like any other)
-            if not self.linearise and not (self._traj_owner is cps and len(bounds) == 2):
-                self.w_fwd.copy_(cps[seg])
-                self.w_dp.zero_()
-                self._fwd_traj(n)
-                self._traj_owner = None  # w_traj now holds this recomputed segment
-            # dual step t of this segment uses the segment state n - t
-            self._dual_steps(n)
+        segs = list(range(len(bounds) - 2, -1, -1))  # last segment first
+        recorded = self._traj_owner is cps and len(bounds) == 2
+        if self.linearise or recorded:
+            # no recompute: the linear dual needs no forward states, and a
+            # single segment recorded by this forward pass is already in w_traj
+            for seg in segs:
+                self._dual_steps(bounds[seg + 1] - bounds[seg])
+        else:
+            main = torch.cuda.current_stream(self.w_dual.device)
+            if self._side is None:
+                self._side = torch.cuda.Stream(device=self.w_dual.device)
+            side = self._side
+            ready = [torch.cuda.Event(), torch.cuda.Event()]
+            free = [torch.cuda.Event(), torch.cuda.Event()]
+            side.wait_stream(main)
+
+            def recompute(i):
+                seg, b = segs[i], i % 2
+                with torch.cuda.stream(side):
+                    if i >= 2:
+                        side.wait_event(free[b])  # the dual run two segments back read this buffer
+                    self.w_fwd.copy_(cps[seg])
+                    self.w_dp.zero_()
+                    self._fwd_traj(bounds[seg + 1] - bounds[seg], b)
+                    ready[b].record(side)
+
+            recompute(0)
+            for i, seg in enumerate(segs):
+                if i + 1 < len(segs):
+                    recompute(i + 1)
+                b = i % 2
+                main.wait_event(ready[b])
+                # dual step t of this segment uses the segment state n - t
+                self._dual_steps(bounds[seg + 1] - bounds[seg], b)
+                free[b].record(main)
+            main.wait_stream(side)
+            self._traj_owner = None  # the segment buffers now hold recomputed segments
         self.fwd.check_device_errors()
         self.dual.check_device_errors()
         return self.w_dual.clone()
