@@ -40,6 +40,34 @@ class Equation:
     def initialize(cls, cleanup: bool = True) -> None:
         Field.initialize(cleanup)
 
+    @classmethod
+    def find_suitable_dt(cls, domain, max_cfl: float = 0.7, U_max=(1.0, 1e-10, 1e-10),
+                         end_time: Optional[float] = None, safety_factor: float = 0.9) -> float:
+        """Time step for a CFL number (equation.py:114-162): the smallest
+        max_cfl * (extent / cells) / U_max over the directions, times the safety
+        factor; with an end time, the step count is raised until its median
+        factor splits it into inner and outer steps no worse than the square
+        root, and dt = end_time / steps."""
+        dT = [abs(max_cfl * (domain.get_extent(i) / domain.number_of_cells(i)) / U_max[i])
+              for i in domain.all_dimensions()]
+        dt = safety_factor * min(dT)
+        if end_time is None:
+            return dt
+
+        def median_factor(n: int) -> int:
+            factors = sorted(f for i in range(1, int(n ** 0.5) + 1) if n % i == 0 for f in (i, n // i))
+            return factors[len(factors) // 2]
+
+        steps = max(0, int(end_time / dt))
+
+        def bad(n: int) -> bool:
+            outer = n // median_factor(n)
+            return abs(n ** 0.5) - outer > outer
+
+        while bad(steps):
+            steps += 1
+        return end_time / steps
+
     def get_dt(self) -> float:
         return self._dt
 

@@ -67,6 +67,23 @@ class PhysicalField(Field):
     def Zeros(cls, domain: PhysicalDomain, name: str = "field"):
         return cls(domain, np.zeros(domain.get_shape_aliasing()), name)
 
+    @classmethod
+    def FromRandom(cls, domain: PhysicalDomain, seed: int = 0, energy_norm: float = 1.0, name: str = "field"):
+        """Uniform random values in [-1, 1] on the physical grid, walls set to
+        zero, scaled to energy `energy_norm` (field.py:1281-1310). The values
+        come from NumPy's PCG64 seeded with `seed` (the reference draws them
+        with jax.random, which is not available here)."""
+        rng = np.random.default_rng(int(seed))
+        out = cls(domain, rng.uniform(-1.0, 1.0, size=domain.get_shape_aliasing()), name)
+        out.update_boundary_conditions()
+        out.normalize_by_energy()
+        out.data = out.data * float(np.sqrt(energy_norm))
+        return out
+
+    def normalize_by_energy(self) -> "PhysicalField":
+        self.data = self.data / float(np.sqrt(self.energy()))
+        return self
+
     def get_domain(self):
         return self.physical_domain
 
@@ -186,6 +203,34 @@ class FourierField(Field):
     def energy(self) -> float:
         return self.no_hat().energy()
 
+    def solve_poisson(self, mat=None) -> "FourierField":
+        """Per-wavenumber Poisson solve with homogeneous Dirichlet rows
+        (field.py:3059-3083, matrix of domain.py:857-889): the reference's
+        inv(-k^2 eye_bc + BC(D2)) is the identity on the wall rows and
+        (D2_int - k^2)^-1 on the interior, applied here in the eigenbasis
+        D2_int = V diag(lam) V^-1 (or with `mat`, (Mx, Mz, Ny, Ny), when given)."""
+        from ._ops import operator_tables
+
+        f = self.data
+        if mat is not None:
+            m = torch.as_tensor(mat, device=f.device).to(torch.complex128)
+            out = torch.einsum("ijkl,ilj->ikj", m, f)
+            return FourierField(self.physical_domain, out, self.name + "_poisson")
+        ny = f.shape[1]
+        t = operator_tables(ny)
+        dev = f.device
+        V = torch.as_tensor(t.V, device=dev).to(torch.complex128)
+        Vinv = torch.as_tensor(t.Vinv, device=dev).to(torch.complex128)
+        lam = torch.as_tensor(t.lam, device=dev)
+        kx = torch.as_tensor(self.fourier_domain.grid[0], device=dev, dtype=torch.float64)
+        kz = torch.as_tensor(self.fourier_domain.grid[2], device=dev, dtype=torch.float64)
+        k2 = kx[:, None] ** 2 + kz[None, :] ** 2                      # (Mx, Mz)
+        inner = torch.einsum("ab,ibj->iaj", Vinv, f[:, 1:-1, :])        # V^-1 rhs_int
+        inner = inner / (lam[None, :, None] - k2[:, None, :])
+        out = f.clone()
+        out[:, 1:-1, :] = torch.einsum("ab,ibj->iaj", V, inner)
+        return FourierField(self.physical_domain, out, self.name + "_poisson")
+
     def _wrap(self, data):
         return FourierField(self.physical_domain, data, self.name)
 
@@ -268,6 +313,34 @@ class VectorField:
 
     def field_2d(self, direction: int) -> "VectorField":
         return VectorField([f.field_2d(direction) for f in self.fields], self.name)
+
+    def all_dimensions(self):
+        return range(len(self.fields))
+
+    def curl(self) -> "VectorField":
+        """(w_y - v_z, u_z - w_x, v_x - u_y) (field.py:917-939); physical or
+        spectral fields alike."""
+        assert len(self) == 3, "rotation only defined in 3 dimensions"
+        u, v, w = self.fields
+        out = [w.diff(1) - v.diff(2), u.diff(2) - w.diff(0), v.diff(0) - u.diff(1)]
+        for f in out:
+            f.time_step = self.get_time_step()
+        return VectorField(out, "curl_" + (self.name or "field"))
+
+    def div(self):
+        """u_x + v_y + w_z (field.py:941-948)."""
+        out = self.fields[0].diff(0)
+        for d in list(self.all_dimensions())[1:]:
+            out = out + self.fields[d].diff(d)
+        out.name = "div_" + self.name if self.name is not None else "div_field"
+        return out
+
+    def normalize_by_energy(self) -> "VectorField":
+        """Divide each component by the square root of the vector field's energy (field.py:666-673)."""
+        en = self.energy()
+        for f in self.fields:
+            f.data = f.data / float(np.sqrt(en))
+        return self
 
     def _map(self, fn) -> "VectorField":
         return VectorField([fn(i, f) for i, f in enumerate(self.fields)], self.name)

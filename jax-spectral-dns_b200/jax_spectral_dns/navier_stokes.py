@@ -26,6 +26,7 @@ from .field import Field, FourierField, PhysicalField, VectorField
 class NavierStokesVelVort(Equation):
     name = "Navier Stokes equation (velocity-vorticity formulation)"
     _kind = _native.JSD_KIND_NS
+    max_cfl = 0.7
 
     def __init__(self, velocity_field: VectorField, **params: Any):
         if "physical_domain" in params:
@@ -35,7 +36,9 @@ class NavierStokesVelVort(Equation):
         domain = physical_domain.hat()
         self._physical_domain: PhysicalDomain = physical_domain
         self._params = dict(params)
-        self.max_cfl = params.get("max_cfl", 0.7)
+        # the CFL limit of the step's fixed parameters (navier_stokes.py:321); the
+        # class attribute max_cfl (0.5 for perturbations) is what the solvers read
+        self._max_cfl = params.get("max_cfl", 0.7)
         self.u_max_over_u_tau = float(params.get("u_max_over_u_tau", 1.0))
         self.Re_tau = self._re_tau_from(params)
         velocity_field.set_name("velocity_hat")
@@ -68,7 +71,7 @@ class NavierStokesVelVort(Equation):
         return self.u_max_over_u_tau
 
     def get_max_cfl(self) -> float:
-        return self.max_cfl
+        return self._max_cfl
 
     def get_number_of_rk_steps(self) -> int:
         return 3

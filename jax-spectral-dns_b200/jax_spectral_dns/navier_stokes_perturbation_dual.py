@@ -25,13 +25,32 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
     name = ("Dual Navier Stokes equation (velocity-vorticity formulation) for perturbations on top of a "
             "base flow.")
     _kind = _native.JSD_KIND_DUAL
+    # objectives (..._dual.py:388-400): the gain E(T)/E(0); the gain of the part
+    # of u(T) with kx != 0 (gain_3d); the gain of u(T) without its (kx, kz) =
+    # (0, 0) mode (gain_no_00); the time-averaged dissipation (not supported)
+    optimisation_modes = ("gain", "gain_3d", "dissipation", "gain_no_00")
+
+    @staticmethod
+    def _objective_part(mode: str, data: torch.Tensor) -> torch.Tensor:
+        """The part of a (3, Mx, Ny, Mz) final state the objective measures."""
+        if mode == "gain":
+            return data
+        out = data.clone()
+        if mode == "gain_3d":
+            out[:, 0] = 0.0  # minus field_2d(0): the kx = 0 modes
+        else:
+            out[:, 0, :, 0] = 0.0  # minus field_2d(0).field_2d(2): the (0, 0) mode
+        return out
 
     def __init__(self, velocity_field: Optional[VectorField], forward_equation: NavierStokesVelVortPerturbation,
                  **params: Any):
         self.epsilon = params.get("epsilon", 1e-5)
         mode = params.get("optimisation_mode", "gain")
-        if mode != "gain":
-            raise NotImplementedError(f"optimisation_mode={mode!r}: only 'gain' is supported")
+        if mode == "dissipation":
+            raise NotImplementedError("optimisation_mode='dissipation' (a source term from the forward history in "
+                                      "every dual step) is not supported")
+        if mode not in self.optimisation_modes:
+            raise ValueError(f"unknown optimisation mode {mode!r}. Valid choices are {self.optimisation_modes}")
         self.optimisation_mode = mode
         if params.get("constant_mass_flux", False):
             raise NotImplementedError("the dual with constant mass flux is not supported")
@@ -116,7 +135,12 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
             self.velocity_field_u_history = traj
             self.dPdx_history = dps
             self._forward_done = True
-        self.set_initial_field("velocity_hat", -1 * nse.get_latest_field("velocity_hat"))
+        # dual initial field: minus the objective's part of u(T) (..._dual.py:904-937)
+        uT = nse.get_latest_field("velocity_hat")
+        part = self._objective_part(self.optimisation_mode, uT.get_data())
+        self.set_initial_field("velocity_hat",
+                               VectorField.FromData(FourierField, self.get_physical_domain(), -part,
+                                                    name="velocity_hat"))
 
     def run_backward_calculation(self) -> None:
         if not self._backward_done:
@@ -128,16 +152,28 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
             self.solve_scan()
             self._backward_done = True
 
-    def get_gain(self) -> float:
+    def _gain_of(self, mode: str) -> float:
         self.run_forward_calculation()
         nse = self.forward_equation
         e0 = nse.energy_of(nse.get_initial_field("velocity_hat").get_data())
-        eT = nse.energy_of(nse.get_latest_field("velocity_hat").get_data())
+        eT = nse.energy_of(self._objective_part(mode, nse.get_latest_field("velocity_hat").get_data()))
         self.gain = eT / e0
         return self.gain
 
+    def get_gain(self) -> float:
+        """E(T) / E(0) (..._dual.py:1058-1063)."""
+        return self._gain_of("gain")
+
+    def get_gain_3d(self) -> float:
+        """Energy of u(T) without its kx = 0 part over E(0) (..._dual.py:1065-1077)."""
+        return self._gain_of("gain_3d")
+
+    def get_gain_no_00(self) -> float:
+        """Energy of u(T) without its (0, 0) mode over E(0) (..._dual.py:1079-1091)."""
+        return self._gain_of("gain_no_00")
+
     def get_objective_fun(self) -> float:
-        return self.get_gain()
+        return self._gain_of(self.optimisation_mode)
 
     def get_objective_fun_name(self) -> str:
         return self.optimisation_mode

@@ -266,6 +266,88 @@ def case_cg_opt():
           u0=u0, gains=np.array(gains), final_guess=final, final_value=float(solver.value))
 
 
+def case_dual_modes():
+    """Reference continuous-adjoint gradients for the objectives gain_3d and
+    gain_no_00 (..._dual.py:388-400, 904-937, 1065-1091): linearised, 9x33x9
+    modes, Re=3000, Lx=2pi, Lz=pi, E0=1e-6, |kx|,|kz| <= 4, dt=0.01, T=0.1."""
+    shape, lx, lz = (8, 33, 8), 2 * math.pi, math.pi
+    re, dt, n = 3000.0, 0.01, 10
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (4, 4), 1e-6, seed=12)
+    out = {}
+    for mode in ("gain_3d", "gain_no_00"):
+        nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=True)
+        nse.activate_jit()
+        dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(
+            nse, checkpointing=False, optimisation_mode=mode)
+        value = float(dual.get_objective_fun())
+        grad = np.asarray(dual.get_grad()).copy()
+        out[mode + "_value"] = value
+        out[mode + "_grad"] = grad
+        print(mode, value, flush=True)
+    _save("dual_modes_9x33x9", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n, u0=u0,
+          **out)
+
+
+def _no_plots():
+    """The solvers plot the gradient after successful steps; plotting is not
+    part of the arithmetic, so the field plot methods are made no-ops here."""
+    from jax_spectral_dns.field import Field, PhysicalField, VectorField as VF
+
+    for cls in (Field, PhysicalField, VF):
+        for nm in ("plot_3d", "plot_center", "plot", "plot_2d"):
+            if hasattr(cls, nm):
+                setattr(cls, nm, lambda *a, **k: None)
+
+
+def case_solvers():
+    """Reference solvers on the linearised pseudo-2D 5x33x5 problem (Re=3000,
+    T=0.2, 20 steps, E0=1e-6): ConjugateGradientDescentSolver with the line
+    search, 3 iterations; SteepestAdaptiveDescentSolver on the same problem
+    with T = 2, initialisation and 2 updates (its trial problems are nonlinear
+    perturbations)."""
+    from jax_spectral_dns.gradient_descent_solver import (ConjugateGradientDescentSolver,
+                                                          SteepestAdaptiveDescentSolver)
+
+    _no_plots()
+    shape, lx, lz = (4, 33, 4), 2 * math.pi, 2 * math.pi * 1e-3
+    re, dt, n = 3000.0, 0.01, 20
+    dom = _domain(shape, lx, lz)
+    u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (1, 0), 1e-6, seed=7)
+    res = {}
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=True)
+    nse.activate_jit()
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse, checkpointing=False)
+    solver = ConjugateGradientDescentSolver(dual, max_iterations=3, step_size=1e-2, use_linesearch=True)
+    solver.initialise(True)
+    ls_values, ls_steps = [], []
+    for it in range(3):
+        solver.update()
+        ls_values.append(float(solver.value))
+        ls_steps.append(float(solver.step_size))
+        solver.i += 1
+    res.update(ls_values=np.array(ls_values), ls_steps=np.array(ls_steps),
+               ls_final=np.asarray(solver.current_guess.get_data()).copy())
+    # the steepest solver re-chooses dt from the CFL number (about 0.2 here), so
+    # it needs a horizon of several such steps: T = 2 (200 steps of 0.01 at first)
+    nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=10 * n * dt, linearise=True)
+    nse.activate_jit()
+    dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse, checkpointing=False)
+    st = SteepestAdaptiveDescentSolver(dual, max_iterations=3, step_size=1e-2)
+    st.initialise(True)
+    sd_values, sd_steps, sd_dts = [float(st.value)], [float(st.step_size)], [float(st.dual_problem.forward_equation.get_dt())]
+    for it in range(2):
+        st.update()
+        sd_values.append(float(st.value))
+        sd_steps.append(float(st.step_size))
+        sd_dts.append(float(st.dual_problem.forward_equation.get_dt()))
+        st.i += 1
+    res.update(sd_values=np.array(sd_values), sd_steps=np.array(sd_steps), sd_dts=np.array(sd_dts),
+               sd_final=np.asarray(st.current_guess.get_data()).copy())
+    print("line search", ls_values, ls_steps, "steepest", sd_values, sd_steps, sd_dts, flush=True)
+    _save("solvers_5x33x5", shape=np.array(shape), lengths=np.array([lx, lz]), re=re, dt=dt, n_steps=n, u0=u0, **res)
+
+
 def case_lsc():
     """Reference LinearStabilityCalculation (n = 50): eigenvalues, leading
     eigenvectors, optimal gains and coefficients for three (Re, alpha, beta,
@@ -422,6 +504,8 @@ CASES = {
     "dual_lin": case_dual_lin,
     "dual_nonlin": case_dual_nonlin,
     "cg_opt": case_cg_opt,
+    "dual_modes": case_dual_modes,
+    "solvers": case_solvers,
     "instationary": case_instationary,
     "coupling_off": case_coupling_off,
 }
