@@ -11,8 +11,9 @@ Two forms are timed: plain FP64, and mixed precision (FP32 transforms and
 products, split-TF32 y-derivatives on the tensor cores, FP64-accurate solves).
 The headline is the mixed form when its energy after a fixed 1000-step run
 agrees with the FP64 form's to 1e-6, else the FP64 form. Side legs (adjoint
-gradients/s, the 48x65x48 perturbation case, gain ascent) print their own JSON
-lines first; the headline line comes last.
+gradients/s, the 48x65x48 perturbation case, gain ascent, the 256-run ensemble
+on mixed boxes at a tenth of its horizons) print their own JSON lines first;
+the headline line comes last and repeats the ensemble leg's rates.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -428,6 +429,10 @@ def run_ours(args):
             print(json.dumps({"leg": "perturbation_48x65x48", **mixed_check_leg(dev, args.autotune)}), flush=True)
         if not args.no_ascent:
             print(json.dumps({"leg": "gain_ascent", **ascent_leg(dev)}), flush=True)
+        ens = None
+        if world == 1 and args.ensemble_leg_runs > 0:
+            ens = ensemble_leg(args.ensemble_leg_runs, args.ensemble_leg_scale)
+            print(json.dumps({"leg": "ensemble", **ens}), flush=True)
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             rate, sec, sample, threads = cpu_reference_leg(1, 0)
@@ -451,6 +456,9 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "api": "StepPlan.step on host (pinned) state"},
             "gpu_launches": plan.launches(args.steps),
+            "ensemble": ({k: ens[k] for k in ("runs", "horizon_scale", "total_steps", "steps_per_s",
+                                              "sequential_steps_per_s", "speedup_over_sequential")}
+                         if ens else None),
             "roofline": roofline, "clocks": clock_summary, "cpu_baseline": cpu, "finite": finite,
             "device_errors": "none (jsd_device_error read after every timed region)",
         }
@@ -595,6 +603,44 @@ def ascent_leg(dev, iterations=20):
             "note": "host wall clock around whole iterations (forward run, dual run, projection, renormalisation)"}
 
 
+def ensemble_leg(n_runs: int, horizon_scale: float):
+    """The ensemble workload on one GPU: n_runs independent perturbation runs
+    on mixed boxes (draw_ensemble), stepped as one batch plan per box (the
+    product: one launch set per RK stage for all runs of a box) against the
+    same runs one plan each, one after another on one stream. Device time
+    (CUDA events) of one full pass each, after a warm-up pass of the batched
+    form; the per-run plans' graphs are captured and warmed when they are
+    built. Horizons are scaled by horizon_scale to bound the leg's time."""
+    import numpy as np
+    import torch
+
+    from jax_spectral_dns.ensemble import BatchedEnsemble, Ensemble, draw_ensemble
+
+    specs = draw_ensemble(n_runs, seed=0, horizon_scale=horizon_scale)
+    steps = sum(s.steps for s in specs)
+    bat = BatchedEnsemble(specs, streams=4, chunk=100)
+    bat.run()
+    bat.reset()
+    ms = bat.run()
+    e_bat = bat.energies()
+    groups = len(bat.groups)
+    del bat
+    torch.cuda.empty_cache()
+    seq = Ensemble(specs, streams=1, chunk=50)
+    seq.reset()
+    ms_seq = seq.run_sequential()
+    e_seq = seq.energies()
+    del seq
+    torch.cuda.empty_cache()
+    return {"runs": n_runs, "horizon_scale": horizon_scale, "total_steps": steps, "groups": groups,
+            "steps_per_s": steps / (ms / 1e3), "sequential_steps_per_s": steps / (ms_seq / 1e3),
+            "speedup_over_sequential": ms_seq / ms,
+            "energy_max_rel_diff_vs_one_plan_per_run": float(np.abs(e_bat / e_seq - 1).max()),
+            "dtype": "f64",
+            "config": "Nx=Nz in {16,32,48,64} x Ny in {49,65,97}, Re U[2000,6000], E0 logU[1e-6,1e-2], "
+                      "T in {5,10,15,20} x horizon_scale, dt=0.01, nonlinear perturbation runs"}
+
+
 def run_ensemble(args):
     """Aggregate steps/s of an ensemble of independent perturbation runs:
     runs sharing a box stepped as one batch plan per group (the product), the
@@ -709,6 +755,10 @@ def main():
     ap.add_argument("--ensemble", type=int, default=0, help="run the ensemble benchmark with this many runs")
     ap.add_argument("--ensemble-horizon-scale", type=float, default=0.25)
     ap.add_argument("--ensemble-streams", type=int, default=16)
+    ap.add_argument("--ensemble-leg-runs", type=int, default=256,
+                    help="runs of the ensemble leg of the default run (0 skips it)")
+    ap.add_argument("--ensemble-leg-scale", type=float, default=0.1,
+                    help="horizon scale of the ensemble leg of the default run")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch the timed steps directly instead of replaying a captured CUDA graph")
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],

@@ -28,7 +28,8 @@
 extern "C" {
 #endif
 
-#define JSD_ABI_VERSION 3  /* 2: jsd_desc gained n_batch, re_tau_batch; 3: JSD_ERR_NONFINITE, wait limit */
+#define JSD_ABI_VERSION 4  /* 2: jsd_desc gained n_batch, re_tau_batch; 3: JSD_ERR_NONFINITE, wait limit;
+                               4: jsd_set_source */
 
 enum jsd_status {
   JSD_OK = 0,
@@ -115,6 +116,16 @@ int jsd_step(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_st
  * the forward run the dual needs (navier_stokes_perturbation_dual.py:850-939). */
 int jsd_step_trajectory(jsd_plan* plan, void* state, double* dpdx, int first_step, int n_steps, void* states,
                         void* stream);
+
+/* Source terms of the following steps (device arrays owned by the caller,
+ * read in every stage until replaced): hv and hg (state layout of one field,
+ * Ny x Mx x Mz complex) are added to the nonlinear terms h_v and h_g, s00
+ * (2 Ny complex: x then z component) to the (0,0) mean-flow forcing. All
+ * three NULL switches them off. Single-run plans. Replaces the source_hat
+ * hooks of perform_runge_kutta_step (navier_stokes.py:1461-1491, 1697-1703)
+ * that the dual's dissipation objective fills
+ * (navier_stokes_perturbation_dual.py:962-990). */
+int jsd_set_source(jsd_plan* plan, const void* hv, const void* hg, const void* s00);
 
 /* Dual equations: register the forward trajectory u_0 .. u_{n_states-1}
  * (device, n_states consecutive states). Dual step t uses u_{n_states-1-t}

@@ -220,6 +220,8 @@ struct jsd_plan {
   std::vector<void*> allocs;
   const double2* history = nullptr;
   int n_history = 0;
+  // source terms added in every stage (jsd_set_source; caller-owned, device)
+  const double2 *src_hv = nullptr, *src_hg = nullptr, *src_00 = nullptr;
   // Discrete adjoint of the linearised perturbation step (jsd_step_adjoint):
   // transposed operators (padded to lda), transposed mean-flow matrices per
   // stage, and small cotangent buffers of the (0,0) system
@@ -749,6 +751,11 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     else
       k_coupling_off<kDual><<<grid_for(fs, blk), blk, 0, s>>>(gp, u, p->dub, p->H1, p->hg);
     JSD_LAUNCHED("k_coupling_off");
+  }
+  if (p->src_hv) {
+    k_add_source<<<grid_for(fs, blk), blk, 0, s>>>(gp, p->src_hv, p->src_hg, p->src_00, p->H1, p->hg,
+                                                   p->conv + (size_t)st * 2 * gp.ny);
+    JSD_LAUNCHED("k_add_source");
   }
   if (!p->om_valid) {
     k_omega<<<grid_for(fs, blk), blk, 0, s>>>(gp, u, w, p->om);
@@ -1586,6 +1593,17 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
 
 int jsd_plan_destroy(jsd_plan* plan) {
   destroy(plan);
+  return 0;
+}
+
+int jsd_set_source(jsd_plan* plan, const void* hv, const void* hg, const void* s00) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  const bool any = hv || hg || s00, all = hv && hg && s00;
+  if (any && !all) return fail(JSD_ERR_ARG, "source terms: give all three arrays or none");
+  if (any && plan->g.nb != 1) return fail(JSD_ERR_ARG, "source terms need a single-run plan");
+  plan->src_hv = static_cast<const double2*>(hv);
+  plan->src_hg = static_cast<const double2*>(hg);
+  plan->src_00 = static_cast<const double2*>(s00);
   return 0;
 }
 

@@ -130,15 +130,22 @@ __device__ __forceinline__ void sq_fft(C* x, const C* tw, C* xb, int t, bool liv
   __syncwarp();
 }
 
-// sq_fft with the twiddles read from the table w_N^e (e = 0..N-1, typically in
-// shared memory) instead of registers.
+// Row stride of the lane-major twiddle table: entry (j, t) = w_N^(t j) sits at
+// (j - 1) * stride + t, so the lanes of a group read consecutive entries.
+__host__ __device__ constexpr int sq_tw_stride(int s) {
+  return s <= 16 ? 16 : 32;
+}
+
+// sq_fft with the twiddles read from the lane-major table (sq_tw_stride;
+// typically in shared memory) instead of registers.
 template <int S, bool INV, typename C>
 __device__ __forceinline__ void sq_fft_tab(C* x, const C* tab, C* xb, int t, bool live) {
+  constexpr int TS = sq_tw_stride(S);
   if (live) {
     dft_reg<S, INV>(x);
 #pragma unroll
     for (int j = 1; j < S; ++j) {
-      C w = tab[t * j];
+      C w = tab[(j - 1) * TS + t];
       if (INV) w.y = -w.y;
       x[j] = cmul(x[j], w);
     }

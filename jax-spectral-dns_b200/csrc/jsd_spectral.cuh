@@ -361,6 +361,35 @@ __device__ __forceinline__ void write_terms(const Geo& g, int y, int ix, int iz,
   }
 }
 
+// Source terms of a stage (navier_stokes.py:1461-1491, 1697-1703): h_v += hv,
+// h_g += hgs (spectral fields in state layout), and the (0,0) mean-flow
+// forcing gains s00 = (s_x(y), s_z(y)). h_v reaches the solve only as
+// -k^2 H1 (write_terms), so hv enters H1 as -hv / k^2; at kx = kz = 0 the v
+// equation is not solved (the mean flow carries that mode) and the mean-flow
+// forcing -conv00 + s00 takes s00 through conv00 -= s00. The source is fixed
+// over the three stages of a step, so the old terms of the next stage carry it
+// as the reference's do.
+__global__ void k_add_source(Geo g, const double2* __restrict__ hv, const double2* __restrict__ hgs,
+                             const double2* __restrict__ s00, double2* __restrict__ H1, double2* __restrict__ hg,
+                             double2* __restrict__ conv00) {
+  const size_t n = (size_t)g.ny * g.nk, n00 = 2 * (size_t)g.ny;
+  const size_t total = n > n00 ? n : n00;
+  for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < total; o += (size_t)gridDim.x * blockDim.x) {
+    if (o < n) {
+      const int r = (int)(o % g.nk);
+      const int ix = r / g.mz, iz = r - (r / g.mz) * g.mz;
+      const double kx = kx_of(g, ix), kz = kz_of(g, iz);
+      const double k2 = kx * kx + kz * kz;
+      if (k2 > 0.0) {
+        const double2 a = hv[o];
+        H1[o] = make_double2(H1[o].x - a.x / k2, H1[o].y - a.y / k2);
+      }
+      hg[o] = cadd(hg[o], hgs[o]);
+    }
+    if (o < n00) conv00[o] = csub(conv00[o], s00[o]);
+  }
+}
+
 // forward z pass: block (kx in [0, K], y).
 template <typename C>
 __global__ void k_zfwd(Geo g, FftDesc fz, const C* __restrict__ tw, const C* __restrict__ out3,

@@ -21,18 +21,26 @@ namespace jsd {
 
 constexpr int kSqWarps = 4;  // warps per block
 
+// Lane roles. With two groups per warp (11 <= S <= 16) each group takes its
+// own half-warp (lanes 16 gi + t, t < S): a 64-bit shared-memory request is
+// served per half-warp, so the groups' accesses never share a bank cycle.
+// Smaller S pack 32 / S groups of S consecutive lanes.
 template <int S>
 struct SqLane {
-  static constexpr int G = 32 / S;  // line groups per warp
+  static constexpr int G = 32 / S;                  // line groups per warp
+  static constexpr int W = G == 2 ? 16 : S;         // lane stride of the groups
   int warp, gi, t;
-  bool live;  // lane belongs to a group (the last 32 - G S lanes idle)
+  bool live;  // lane belongs to a group (the other lanes idle)
   __device__ __forceinline__ SqLane() {
     const int lane = threadIdx.x & 31;
     warp = threadIdx.x >> 5;
-    gi = lane / S;
-    t = lane - gi * S;
-    live = gi < G;
-    if (!live) gi = 0;
+    gi = lane / W;
+    t = lane - gi * W;
+    live = gi < G && t < S;
+    if (!live) {
+      gi = 0;
+      t = 0;
+    }
   }
 };
 
@@ -70,11 +78,13 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_zinv_sq(Geo g, const C* __res
     for (int fi = 0; fi < 6; ++fi) {
       const double2* f = zinv_field(src, set * 6 + fi);
       C x[S], xz[S];
+      // K < N / 2: positions below N / 2 hold kz >= 0 modes, those above kz < 0
 #pragma unroll
       for (int m = 0; m < S; ++m) {
         const int p = ln.t + S * m;
-        const bool lo = p <= K, hi = p >= N - K;
-        const int kz = lo ? p : p - N;
+        const bool below = S * m + S - 1 < N / 2, above = S * m >= N / 2;
+        const bool lo = !above && p <= K, hi = !below && p >= N - K;
+        const int kz = below ? p : above ? p - N : lo ? p : p - N;
         const C v = (act && (lo || hi)) ? to_c<C>(sym_at(g, f, y, kx, kz)) : cmake<C>(0, 0);
         x[m] = v;
         xz[m] = cmul_ik(v, (Rl)(kz * g.az));
@@ -174,17 +184,48 @@ size_t zfwd_sq_smem() {
 // ---------------------------------------------------------------------------
 // x pass with the products
 // ---------------------------------------------------------------------------
+// Shared-memory layout of the x pass, chosen so that every 64-bit request is
+// served at the minimum number of wavefronts:
+//   input tile [field][zl][kx], row stride KP: the staging copies (8 z columns
+//     x 2 rows per half-warp) need KP = 2 mod 16 when ZC = 8; with more columns
+//     per block an odd KP;
+//   output tile [row][zl] with the 8 z columns of a row swizzled by
+//     (row / 2) mod 8: the lanes of a group write 14 consecutive rows of one
+//     column, the store reads 2 rows of 8 columns per half-warp;
+//   twiddles lane-major (sq_tw_stride).
+template <int ZC>
+__host__ __device__ __forceinline__ int xsq_kp(int k1) {
+  return ZC == 8 ? k1 + ((2 - k1) % 16 + 16) % 16 : k1 | 1;
+}
+
 template <typename C, int S>
 struct XmidSq {
   static constexpr int G = SqLane<S>::G;
   static constexpr int ZC = kSqWarps * G;  // z columns per block
-  static __host__ __device__ int kp(int k1) { return k1 | 1; }  // odd row stride of the input tile
+  static __host__ __device__ int kp(int k1) { return xsq_kp<ZC>(k1); }
+  static constexpr int twn = (S - 1) * sq_tw_stride(S);  // twiddle table entries
   static size_t smem(const Geo& g, int nfields) {
     const int K1 = g.kx_max + 1;
     return sizeof(C) * ((size_t)nfields * ZC * kp(K1) + 3 * (size_t)K1 * ZC + (size_t)kSqWarps * G * sq_xbuf<S>() +
-                        (size_t)S * S);
+                        (size_t)twn);
   }
 };
+
+// slot of (row, z column) in the output tile
+template <int ZC>
+__device__ __forceinline__ int xsq_oslot(int row, int zl) {
+  return ZC == 8 ? row * 8 + (zl ^ ((row >> 1) & 7)) : row * ZC + zl;
+}
+
+// Block-wide: the lane-major twiddle table from the table w_N^e, e = 0..N-1.
+template <typename C, int S>
+__device__ __forceinline__ void xsq_twiddle_table(C* stab, const C* __restrict__ twtab) {
+  constexpr int TS = sq_tw_stride(S);
+  for (int e = threadIdx.x; e < XmidSq<C, S>::twn; e += blockDim.x) {
+    const int j = e / TS + 1, t = e - (j - 1) * TS;
+    stab[e] = t < S ? twtab[t * j] : cmake<C>(0, 0);
+  }
+}
 
 // 8- or 16-byte asynchronous copy global -> shared (zero fill when !ok)
 template <typename C>
@@ -202,7 +243,7 @@ template <typename C, int ZC>
 __device__ __forceinline__ void xsq_stage_tile(const Geo& g, const C* __restrict__ inter, C* tile, int nfields,
                                                int y, int z0) {
   constexpr int RSTEP = kSqWarps * 32 / ZC;  // tile rows per pass of the block
-  const int K1 = g.kx_max + 1, KP = K1 | 1;
+  const int K1 = g.kx_max + 1, KP = xsq_kp<ZC>(K1);
   if (threadIdx.x < RSTEP * ZC) {
     const int zl = threadIdx.x % ZC;
     const int z = z0 + zl;
@@ -233,19 +274,23 @@ __device__ __forceinline__ void xsq_fill(const Geo& g, const C* tile, int zl, in
   const int K = g.kx_max, KP = XmidSq<C, S>::kp(K + 1);
   const C* ta = tile + (fa * ZC + zl) * KP;
   const C* tb = tile + (fb * ZC + zl) * KP;
+  // K < N / 2, so positions below N / 2 can only be kx >= 0 modes and those
+  // above only kx < 0 modes: after unrolling, each m but a straddling one
+  // needs one bound check and no select of the packing
 #pragma unroll
   for (int m = 0; m < S; ++m) {
     const int p = t + S * m;
-    const bool lo = p <= K, hi = p >= N - K;
+    const bool below = S * m + S - 1 < N / 2, above = S * m >= N / 2;
+    const bool lo = !above && p <= K, hi = !below && p >= N - K;
     C out = cmake<C>(0, 0);
     if (live && (lo || hi)) {
-      const int kx = lo ? p : N - p;
+      const int kx = below ? p : above ? N - p : lo ? p : N - p;
       C A = ta[kx], B = tb[kx];
       const Rl k = (Rl)(kx * g.ax);
       if (dxa) A = cmul_ik(A, k);
       if (dxb) B = cmul_ik(B, k);
-      if (p == 0) out = cmake<C>(A.x, B.x);
-      else if (lo) out = cmake<C>(A.x - B.y, A.y + B.x);
+      if (m == 0 && p == 0) out = cmake<C>(A.x, B.x);
+      else if (below || (!above && lo)) out = cmake<C>(A.x - B.y, A.y + B.x);
       else out = cmake<C>(A.x + B.y, B.x - A.y);
     }
     x[m] = out;
@@ -267,7 +312,7 @@ __device__ __forceinline__ void xsq_forward(const Geo& g, const C* tab, C* xb, C
     for (int m = 0; m < S; ++m) {
       xb[t + S * m] = z01[m];
       const int p = t + S * m;
-      if (p <= K) otile[(2 * K1 + p) * ZC + zl] = z2[m];
+      if (p <= K) otile[xsq_oslot<ZC>(2 * K1 + p, zl)] = z2[m];
     }
   }
   __syncwarp();
@@ -277,8 +322,8 @@ __device__ __forceinline__ void xsq_forward(const Geo& g, const C* tab, C* xb, C
       const C a = xb[kx];
       const C b = xb[kx == 0 ? 0 : N - kx];
       // H0 = (Z[k] + conj Z[-k]) / 2, H1 = (Z[k] - conj Z[-k]) / (2 i)
-      otile[(0 * K1 + kx) * ZC + zl] = cmake<C>(half * (a.x + b.x), half * (a.y - b.y));
-      otile[(1 * K1 + kx) * ZC + zl] = cmake<C>(half * (a.y + b.y), -half * (a.x - b.x));
+      otile[xsq_oslot<ZC>(0 * K1 + kx, zl)] = cmake<C>(half * (a.x + b.x), half * (a.y - b.y));
+      otile[xsq_oslot<ZC>(1 * K1 + kx, zl)] = cmake<C>(half * (a.y + b.y), -half * (a.x - b.x));
     }
   }
 }
@@ -297,7 +342,7 @@ __device__ __forceinline__ void xsq_store(const Geo& g, const C* otile, C* __res
   int row = threadIdx.x / ZC;
   int f = row / K1, kx = row - (row / K1) * K1;
   for (; row < 3 * K1; row += RSTEP) {
-    base[f * fstride + (size_t)kx * g.pz] = otile[row * ZC + zl];
+    base[f * fstride + (size_t)kx * g.pz] = otile[xsq_oslot<ZC>(row, zl)];
     kx += RSTEP;
     while (kx >= K1) {
       kx -= K1;
@@ -334,9 +379,9 @@ __global__ void __launch_bounds__(kSqWarps * 32, xsq_min_blocks<C>()) k_xmid_sq(
   const Rl dub = dubase ? (Rl)dubase[y / g.nb] : (Rl)0;
   const Rl c = (Rl)g.c_inv, lam = (Rl)lam_d, half = (Rl)0.5;
   xsq_stage_tile<C, ZC>(g, inter, tile, kZinvLines, y, z0);
-  // twiddle table w_N^e in shared memory (read by stage 1 of every transform)
+  // twiddle table in shared memory (read by stage 1 of every transform)
   C* stab = otile + 3 * K1 * ZC + kSqWarps * G * XB;
-  for (int e = threadIdx.x; e < S * S; e += blockDim.x) stab[e] = twtab[e];
+  xsq_twiddle_table<C, S>(stab, twtab);
   cp_async_wait<0>();
   __syncthreads();
   const bool live = ln.live;
@@ -428,9 +473,9 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_xmid_dual_sq(Geo g, const C* 
   const Rl dub = (Rl)dubase[y / g.nb];
   const Rl c = (Rl)g.c_inv, q4 = (Rl)0.25;
   xsq_stage_tile<C, ZC>(g, inter, tile, 2 * kZinvLines, y, z0);
-  // twiddle table w_N^e in shared memory (read by stage 1 of every transform)
+  // twiddle table in shared memory (read by stage 1 of every transform)
   C* stab = otile + 3 * K1 * ZC + kSqWarps * G * XB;
-  for (int e = threadIdx.x; e < S * S; e += blockDim.x) stab[e] = twtab[e];
+  xsq_twiddle_table<C, S>(stab, twtab);
   cp_async_wait<0>();
   __syncthreads();
   const bool live = ln.live;
@@ -647,8 +692,8 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_xmid_h2(Geo g, const C* __res
     for (int kx = h * S + t; kx <= K; kx += 2 * S) {
       const C a = xb[kx];
       const C b = xb[kx == 0 ? 0 : N - kx];
-      otile[(0 * K1 + kx) * ZC + zl] = cmake<C>(half * (a.x + b.x), half * (a.y - b.y));
-      otile[(1 * K1 + kx) * ZC + zl] = cmake<C>(half * (a.y + b.y), -half * (a.x - b.x));
+      otile[xsq_oslot<ZC>(0 * K1 + kx, zl)] = cmake<C>(half * (a.x + b.x), half * (a.y - b.y));
+      otile[xsq_oslot<ZC>(1 * K1 + kx, zl)] = cmake<C>(half * (a.y + b.y), -half * (a.x - b.x));
     }
   }
   __syncthreads();

@@ -44,7 +44,7 @@ JSD_PRECISION_MIXED = 1
 
 
 EXPORTED = (
-    "jsd_plan_create", "jsd_plan_destroy", "jsd_step", "jsd_set_history",
+    "jsd_plan_create", "jsd_plan_destroy", "jsd_step", "jsd_set_history", "jsd_set_source",
     "jsd_correct_mass_flux", "jsd_energy", "jsd_flow_rate", "jsd_nonlinear_terms",
     "jsd_workspace_bytes", "jsd_launches_per_step", "jsd_last_error", "jsd_abi_version",
     "jsd_profile_enable", "jsd_profile_read", "jsd_energy_noalloc", "jsd_step_trajectory",
@@ -56,7 +56,7 @@ EXPORTED = (
     "jsd_set_wait_limit", "jsd_wait_limit", "jsd_step_adjoint", "jsd_energy_grad",
 )
 
-ABI_VERSION = 3  # JSD_ABI_VERSION of include/jsd.h this binding is written for
+ABI_VERSION = 4  # JSD_ABI_VERSION of include/jsd.h this binding is written for
 
 # status codes (enum jsd_status)
 JSD_ERR_ARG, JSD_ERR_CUDA, JSD_ERR_NOMEM, JSD_ERR_STATE, JSD_ERR_NONFINITE = -1, -2, -3, -4, -5
@@ -99,6 +99,7 @@ def load(path: str = LIB_PATH):
     lib.jsd_plan_destroy.argtypes = [vp]
     lib.jsd_step.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp]
     lib.jsd_set_history.argtypes = [vp, vp, ctypes.c_int]
+    lib.jsd_set_source.argtypes = [vp, vp, vp, vp]
     lib.jsd_step_trajectory.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp]
     lib.jsd_correct_mass_flux.argtypes = [vp, vp, vp, vp]
     lib.jsd_energy.argtypes = [vp, vp, vp, vp]

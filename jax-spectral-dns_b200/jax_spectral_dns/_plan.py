@@ -247,6 +247,25 @@ class StepPlan:
             _native.check(self.lib.jsd_set_history(self.handle, ctypes.c_void_p(states.data_ptr()),
                                                    int(states.shape[0])), "jsd_set_history")
 
+    def set_source(self, hv: Optional[torch.Tensor] = None, hg: Optional[torch.Tensor] = None,
+                   s00: Optional[torch.Tensor] = None):
+        """Source terms added in every stage of the following steps: hv, hg
+        (Ny, Mx, Mz) complex to the nonlinear terms h_v, h_g and s00 (2 Ny,)
+        complex (x then z) to the mean-flow forcing; no arguments switch them
+        off. The plan keeps the tensors alive until the next call."""
+        if hv is None:
+            self._source = None
+            _native.check(self.lib.jsd_set_source(self.handle, None, None, None), "jsd_set_source")
+            return
+        src = tuple(t.contiguous() for t in (hv, hg, s00))
+        for t in src:
+            assert t.dtype == torch.complex128 and t.is_cuda
+        assert src[0].numel() == src[1].numel() == self.modes[1] * self.modes[0] * self.modes[2]
+        assert src[2].numel() == 2 * self.modes[1]
+        self._source = src
+        _native.check(self.lib.jsd_set_source(self.handle, *(ctypes.c_void_p(t.data_ptr()) for t in src)),
+                      "jsd_set_source")
+
     def energy(self, state: torch.Tensor) -> torch.Tensor:
         out = torch.empty(1, dtype=torch.float64, device=state.device)
         _native.check(self.lib.jsd_energy(self.handle, ctypes.c_void_p(state.data_ptr()),

@@ -27,7 +27,8 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
     _kind = _native.JSD_KIND_DUAL
     # objectives (..._dual.py:388-400): the gain E(T)/E(0); the gain of the part
     # of u(T) with kx != 0 (gain_3d); the gain of u(T) without its (kx, kz) =
-    # (0, 0) mode (gain_no_00); the time-averaged dissipation (not supported)
+    # (0, 0) mode (gain_no_00); the time-averaged dissipation, whose dual starts
+    # from zero and is driven by a source from the forward history
     optimisation_modes = ("gain", "gain_3d", "dissipation", "gain_no_00")
 
     @staticmethod
@@ -38,17 +39,16 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
         out = data.clone()
         if mode == "gain_3d":
             out[:, 0] = 0.0  # minus field_2d(0): the kx = 0 modes
-        else:
+        elif mode == "gain_no_00":
             out[:, 0, :, 0] = 0.0  # minus field_2d(0).field_2d(2): the (0, 0) mode
+        else:
+            out.zero_()  # dissipation: the dual starts from zero
         return out
 
     def __init__(self, velocity_field: Optional[VectorField], forward_equation: NavierStokesVelVortPerturbation,
                  **params: Any):
         self.epsilon = params.get("epsilon", 1e-5)
         mode = params.get("optimisation_mode", "gain")
-        if mode == "dissipation":
-            raise NotImplementedError("optimisation_mode='dissipation' (a source term from the forward history in "
-                                      "every dual step) is not supported")
         if mode not in self.optimisation_modes:
             raise ValueError(f"unknown optimisation mode {mode!r}. Valid choices are {self.optimisation_modes}")
         self.optimisation_mode = mode
@@ -92,6 +92,41 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
         spec["dt_explicit"] = self.get_dt()
         spec["constant_mass_flux"] = False
         return spec
+
+    def _time_dependent(self) -> bool:
+        return self.optimisation_mode == "dissipation" or super()._time_dependent()
+
+    def _prepare_step(self, plan, time_step: int) -> None:
+        super()._prepare_step(plan, time_step)
+        if self.optimisation_mode == "dissipation":
+            plan.set_source(*self._dissipation_source(time_step))
+
+    def _dissipation_source(self, time_step: int):
+        """Source of the dissipation objective's dual step `time_step`
+        (..._dual.py:962-990): s = -lap(u) / |Re_tau T| of the forward state
+        u = history[-1 - time_step], composed as the reference's step adds it
+        (navier_stokes.py:1697-1703): with C = (curl s)_y, h_v gains
+        i kz C[kx index 0] - i kx_1 C[kx index 2] and h_g gains C[kx index 1],
+        each plane added at every kx; the mean flow gains (s_x, s_z) at
+        (0, 0) (navier_stokes.py:1461-1491). Returns (h_v, h_g) in the
+        device's (Ny, Mx, Mz) layout and the (2 Ny,) mean-flow source."""
+        traj = self.forward_equation._trajectory_device
+        if traj is None:
+            raise RuntimeError("run the forward calculation before the dissipation dual step")
+        u = traj[traj.shape[0] - 1 - time_step].permute(0, 2, 1, 3)  # (3, Mx, Ny, Mz)
+        dom = self.get_domain()
+        scale = -1.0 / abs(self.get_Re_tau() * self.end_time)
+        s = torch.stack([(dom.diff(u[i], 0, 2) + dom.diff(u[i], 1, 2) + dom.diff(u[i], 2, 2)) * scale
+                         for i in range(3)])
+        C = dom.curl(s)[1]
+        kx = torch.as_tensor(dom.grid[0], dtype=torch.float64, device=u.device)
+        kz = torch.as_tensor(dom.grid[2], dtype=torch.float64, device=u.device)
+        hv_plane = 1j * kz * C[0] - 1j * kx[1] * C[2]  # (Ny, Mz)
+        mx = u.shape[1]
+        hv = hv_plane.unsqueeze(1).expand(-1, mx, -1).contiguous()
+        hg = C[1].unsqueeze(1).expand(-1, mx, -1).contiguous()
+        s00 = torch.cat([s[0][0, :, 0], s[2][0, :, 0]]).contiguous()
+        return hv, hg, s00
 
     def _prepare_plan_history(self, plan) -> None:
         if self.linearise(0):
@@ -172,7 +207,27 @@ class NavierStokesVelVortPerturbationDual(NavierStokesVelVortPerturbation):
         """Energy of u(T) without its (0, 0) mode over E(0) (..._dual.py:1079-1091)."""
         return self._gain_of("gain_no_00")
 
+    def get_dissipation_average(self) -> float:
+        """(1 / |Re_tau n|) sum over the n stored forward states of
+        sum_ij (d_j u_i)^2, the squares taken of the spectral coefficients,
+        then no_hat and the volume integral (..._dual.py:1089-1104)."""
+        self.run_forward_calculation()
+        traj = self.forward_equation._trajectory_device
+        dom = self.get_domain()
+        acc = None
+        for t in range(traj.shape[0]):
+            u = traj[t].permute(0, 2, 1, 3)
+            for i in range(3):
+                for j in range(3):
+                    d = dom.diff(u[i], j) ** 2
+                    acc = d if acc is None else acc + d
+        acc = acc / abs(self.get_Re_tau() * traj.shape[0])
+        return FourierField(self.get_physical_domain(), acc).no_hat().volume_integral()
+
     def get_objective_fun(self) -> float:
+        if self.optimisation_mode == "dissipation":
+            self.gain = self.get_gain()
+            return self.get_dissipation_average()
         return self._gain_of(self.optimisation_mode)
 
     def get_objective_fun_name(self) -> str:

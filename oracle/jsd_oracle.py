@@ -179,6 +179,11 @@ class Grid:
             total += self.lx / self.px * iy.sum() / vol
         return float(total)
 
+    def volume_integral(self, f: np.ndarray) -> float:
+        """PhysicalField.volume_integral (field.py:1456-1466): z, then y, then x."""
+        iz = self.lz / self.pz * f.sum(axis=2)
+        return float(self.lx / self.px * (iz @ self.y_weights()).sum())
+
     def flow_rate(self, u_hat: np.ndarray) -> float:
         """NavierStokesVelVort.get_flow_rate (navier_stokes.py:709-722):
         y-integral of the streamwise velocity at the grid point x = z = 0."""
@@ -316,6 +321,7 @@ class Stepper:
         self.base_hat = base_hat
         self.flow_rate_target = flow_rate_target
         self.u_history = None  # dual: callable t -> forward state
+        self.source = None  # callable t -> (3, Mx, Ny, Mz) source or None (get_source_term)
         # time-dependent base flow t -> base_hat (NavierStokesVelVortPerturbationInstationary);
         # linearise / coupling_term may also be callables t -> bool (the *_switch parameters)
         self.base_fn = None
@@ -419,8 +425,17 @@ class Stepper:
         g = self.g
         dt_e = self.dt_explicit
         hv_old = hg_old = conv_old = None
+        src = self.source(time_step) if self.source is not None else None
         for st in range(3):
             h_v, h_g, vort, conv = self._nonlinear(vel_hat, time_step)
+            if src is not None:
+                # navier_stokes.py:1697-1703, indexing as written there: the y
+                # component C of curl(source) is (Mx, Ny, Mz); C[0], C[2] are
+                # its kx index 0 and 2 planes, whose x/z derivatives broadcast
+                # over kx before [1] picks the kx index 1 plane again
+                C = g.curl(src)[1]
+                h_v = h_v + (1j * g.KZ * C[0][None] - 1j * g.KX * C[2][None])[1][None]
+                h_g = h_g + C[1][None]
             if st == 0:
                 hv_old = np.zeros_like(h_v)
                 hg_old = np.zeros_like(h_g)
@@ -451,19 +466,21 @@ class Stepper:
             u_new = (-1j * g.KX * vy + 1j * g.KZ * om_new) / k2s
             w_new = (-1j * g.KZ * vy - 1j * g.KX * om_new) / k2s
             # (0,0) mean flow (rk_00)
-            u00, w00 = self._mean_flow(st, vel_hat, conv, conv_old, dpdx, time_step)
+            u00, w00 = self._mean_flow(st, vel_hat, conv, conv_old, dpdx, time_step, src)
             u_new[0, :, 0] = u00
             w_new[0, :, 0] = w00
             hv_old, hg_old, conv_old = h_v, h_g, conv
             vel_hat = set_bc(np.array([u_new, v_new, w_new]))
         return self._mass_flux(vel_hat, dpdx)
 
-    def _mean_flow(self, st, vel_hat, conv, conv_old, dpdx, time_step):
+    def _mean_flow(self, st, vel_hat, conv, conv_old, dpdx, time_step, source=None):
         g, n = self.g, self.g.ny
         v_hat = np.concatenate([vel_hat[0][0, :, 0], vel_hat[2][0, :, 0]])
         scale = ((g.px * (2 * np.pi / g.lx) ** 2) * (g.pz * (2 * np.pi / g.lz) ** 2)) ** 0.5
         dp = dpdx * scale
         src = np.concatenate([-dp * np.ones(n), np.zeros(n)])
+        if source is not None:  # navier_stokes.py:1461-1491
+            src = src + np.concatenate([source[0][0, :, 0], source[2][0, :, 0]])
         N_new = np.concatenate([-conv[0][0, :, 0], -conv[2][0, :, 0]]) + src
         N_old = np.concatenate([-conv_old[0][0, :, 0], -conv_old[2][0, :, 0]]) + src
         out = self.lhs_inv_ns[st] @ (self.rhs_ns[st] @ v_hat + (self.dt_explicit * RK_GAMMA[st]) * N_new
@@ -541,6 +558,43 @@ def run(stepper: Stepper, u0: np.ndarray, n_steps: int, dpdx: float = 0.0, histo
         if history:
             hist.append(u)
     return u, dpdx, hist
+
+
+def dissipation_average(g: Grid, hist, re_tau: float) -> float:
+    """get_dissipation_average (navier_stokes_perturbation_dual.py:1089-1104):
+    sum over the stored states of sum_ij (d_j u_i)^2, squares of the spectral
+    coefficients, over |Re_tau n|, then no_hat and the volume integral. The x-z
+    integral leaves the (0, 0) mode of that sum."""
+    acc = np.zeros(hist[0].shape[1:], dtype=complex)
+    for u in hist:
+        for i in range(3):
+            for j in range(3):
+                acc += g.diff(u[i], j) ** 2
+    acc /= abs(re_tau * len(hist))
+    return float(g.volume_integral(g.no_hat(acc)))
+
+
+def dissipation_gradient(shape, lx, lz, re, dt, n_steps, u0, linearise, u_max=1.0):
+    """The dual's dissipation objective (navier_stokes_perturbation_dual.py:
+    904-990, 1089-1120): the dual starts from zero and every step t adds the
+    source -lap(u(T - t)) / |Re_tau T| of the forward state it pairs with;
+    grad = (u0 - v0) / E0. Returns (grad, value, v0)."""
+    re_tau = re / u_max
+    fwd = make_stepper("perturbation", shape, lx, lz, re_tau, dt, linearise=linearise, u_max=u_max)
+    _, _, hist = run(fwd, u0, n_steps, history=True)
+    g = fwd.g
+    dual = Stepper(g, re_tau, dt, kind="dual", linearise=linearise, base_hat=fwd.base_hat, dt_explicit=-dt)
+    dual.u_history = lambda t: hist[-1 - t]
+    end_time = n_steps * dt
+
+    def source(t):
+        u = hist[-1 - t]
+        lap = np.array([g.diff(u[i], 0, 2) + g.diff(u[i], 1, 2) + g.diff(u[i], 2, 2) for i in range(3)])
+        return -1.0 / abs(re_tau * end_time) * lap
+
+    dual.source = source
+    v0, _, _ = run(dual, np.zeros_like(u0), n_steps)
+    return (u0 - v0) / g.energy(u0), dissipation_average(g, hist, re_tau), v0
 
 
 def dual_gradient(shape, lx, lz, re, dt, n_steps, u0, linearise, u_max=1.0):

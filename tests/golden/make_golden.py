@@ -267,16 +267,23 @@ def case_cg_opt():
 
 
 def case_dual_modes():
-    """Reference continuous-adjoint gradients for the objectives gain_3d and
-    gain_no_00 (..._dual.py:388-400, 904-937, 1065-1091): linearised, 9x33x9
-    modes, Re=3000, Lx=2pi, Lz=pi, E0=1e-6, |kx|,|kz| <= 4, dt=0.01, T=0.1."""
+    """Reference continuous-adjoint gradients for the objectives gain_3d,
+    gain_no_00 and dissipation (..._dual.py:388-400, 904-990, 1065-1104):
+    linearised, 9x33x9 modes, Re=3000, Lx=2pi, Lz=pi, E0=1e-6, |kx|,|kz| <= 4,
+    dt=0.01, T=0.1. The dissipation objective only sees the (0, 0) mode (the
+    x-z integral of the squared spectral gradients), which the seeded field
+    leaves at zero, so its case adds a streamwise mean-flow perturbation
+    1e-3 (1 - y^2) to make the value more than the transforms' round-off."""
     shape, lx, lz = (8, 33, 8), 2 * math.pi, math.pi
     re, dt, n = 3000.0, 0.01, 10
     dom = _domain(shape, lx, lz)
     u0 = seeds.seeded_velocity_hat(shape, (lx, lz), (4, 4), 1e-6, seed=12)
-    out = {}
-    for mode in ("gain_3d", "gain_no_00"):
-        nse = NavierStokesVelVortPerturbation(_vf(dom, u0), Re=re, dt=dt, end_time=n * dt, linearise=True)
+    u0_diss = u0.copy()
+    u0_diss[0, 0, :, 0] += 1e-3 * (1.0 - seeds.cheb_points(u0.shape[2]) ** 2)
+    out = {"dissipation_u0": u0_diss}
+    for mode in ("gain_3d", "gain_no_00", "dissipation"):
+        start = u0_diss if mode == "dissipation" else u0
+        nse = NavierStokesVelVortPerturbation(_vf(dom, start), Re=re, dt=dt, end_time=n * dt, linearise=True)
         nse.activate_jit()
         dual = NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(
             nse, checkpointing=False, optimisation_mode=mode)

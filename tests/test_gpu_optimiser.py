@@ -33,22 +33,28 @@ def test_cg_gain_ascent_matches_reference(cuda):
     assert rel(solver.current_guess.get_data().cpu().numpy(), d["final_guess"]) < 1e-8
 
 
-def _problem(d, mode="gain", end_scale=1):
+def _problem(d, mode="gain", end_scale=1, u0_key="u0"):
     shape, (lx, lz) = tuple(int(x) for x in d["shape"]), d["lengths"]
     n, dt = int(d["n_steps"]), float(d["dt"])
     dom = PhysicalDomain.create(shape, (True, False, True), scale_factors=(lx, 1.0, lz), aliasing=3 / 2)
-    u0 = VectorField.FromData(FourierField, dom, torch.as_tensor(d["u0"], device="cuda"), name="velocity_hat")
+    u0 = VectorField.FromData(FourierField, dom, torch.as_tensor(d[u0_key], device="cuda"), name="velocity_hat")
     nse = NavierStokesVelVortPerturbation(u0, Re=float(d["re"]), dt=dt, end_time=end_scale * n * dt, linearise=True)
     return NavierStokesVelVortPerturbationDual.FromNavierStokesVelVortPerturbation(nse, optimisation_mode=mode)
 
 
-@pytest.mark.parametrize("mode", ["gain_3d", "gain_no_00"])
+@pytest.mark.parametrize("mode", ["gain_3d", "gain_no_00", "dissipation"])
 def test_dual_objectives_match_reference(cuda, mode):
-    """gain_3d (u(T) without its kx = 0 part) and gain_no_00 (without its
-    (0, 0) mode): objective value and dual gradient against the reference's
-    dual solver (navier_stokes_perturbation_dual.py:388-400, 904-937, 1065-1091)."""
+    """gain_3d (u(T) without its kx = 0 part), gain_no_00 (without its (0, 0)
+    mode) and dissipation (the time average of the squared velocity gradients,
+    whose dual starts from zero and is driven by a source from the forward
+    history in every step): objective value and dual gradient against the
+    reference's dual solver (navier_stokes_perturbation_dual.py:388-400,
+    904-990, 1065-1104; the source enters at navier_stokes.py:1461-1491,
+    1697-1703)."""
     d = golden("dual_modes_9x33x9")
-    dual = _problem(d, mode)
+    # the dissipation case starts with a mean-flow perturbation: the objective
+    # only sees the (0, 0) mode
+    dual = _problem(d, mode, u0_key="dissipation_u0" if mode == "dissipation" else "u0")
     value = dual.get_objective_fun()
     assert abs(value / float(d[mode + "_value"]) - 1) < 1e-10
     grad = dual.get_grad().cpu().numpy()

@@ -46,7 +46,7 @@ def test_binding_covers_header(lib):
 def test_abi_version_and_error_strings(lib):
     from jax_spectral_dns import _native
 
-    assert lib.jsd_abi_version() == _native.ABI_VERSION == 3
+    assert lib.jsd_abi_version() == _native.ABI_VERSION == 4
     assert isinstance(lib.jsd_last_error(), bytes)
 
 
@@ -65,6 +65,12 @@ def test_wait_limit_argument_checks_without_gpu(lib):
     """jsd_set_wait_limit validates before touching a plan."""
     assert lib.jsd_set_wait_limit(None, 10) == -1
     assert lib.jsd_wait_limit(None) == 0
+
+
+def test_set_source_argument_checks_without_gpu(lib):
+    """jsd_set_source rejects a missing plan before touching it."""
+    assert lib.jsd_set_source(None, None, None, None) == -1
+    assert b"plan" in lib.jsd_last_error()
 
 
 def test_plan_create_rejects_bad_descriptor_without_gpu(lib):

@@ -61,6 +61,18 @@ def test_dual_gradient(name, lin):
     assert abs(gain / float(d["gain"]) - 1) < 1e-13
 
 
+def test_dissipation_objective():
+    """The dual's dissipation objective (navier_stokes_perturbation_dual.py:
+    904-990, 1089-1120): the source from the forward history in every dual
+    step, composed with the reference's indexing (navier_stokes.py:1461-1491,
+    1697-1703), and the time-averaged value."""
+    d = golden("dual_modes_9x33x9")
+    grad, value, _ = O.dissipation_gradient(tuple(d["shape"]), *d["lengths"], float(d["re"]), float(d["dt"]),
+                                            int(d["n_steps"]), d["dissipation_u0"], True)
+    assert rel(grad, d["dissipation_grad"]) < 1e-12
+    assert abs(value / float(d["dissipation_value"]) - 1) < 1e-10
+
+
 def test_transient_growth_energy_history():
     """E(t) over the first 100 steps of the pseudo-2D linear case."""
     d = golden("lin_pert_9x65x5")
