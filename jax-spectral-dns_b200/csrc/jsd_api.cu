@@ -774,6 +774,10 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     rc = launch_eig(p, b, ni, kSiteEigIn, s);
     if (rc) return rc;
   }
+  if (p->src_hv) {
+    k_add_source00<<<1, 128, 0, s>>>(g, p->Vinv, p->lda, p->src_hv, p->X1);
+    JSD_LAUNCHED("k_add_source00");
+  }
   {
     EigTables t{p->lam, p->c0, p->cN, p->sgn, p->w0, p->wN, p->re_run};
     StageCoef sc{kAlpha[st], kBeta[st], kGamma[st], kXi[st], p->desc.dt, p->desc.dt_explicit, p->desc.re_tau,
@@ -1306,7 +1310,8 @@ int jsd_launches_per_step(const jsd_plan* plan) {
   // kernel), 2 GEMMs, eigen update, mean flow and reconstruct; omega_y is carried
   // too, except after the mass-flux correction (3 launches) changed u
   const bool coupling_off = !plan->coupling && plan->desc.kind != JSD_KIND_NS;
-  const int per_stage = (linear ? 6 : 9) + (coupling_off ? 1 : 0);
+  // a source (jsd_set_source) adds k_add_source and k_add_source00 per stage
+  const int per_stage = (linear ? 6 : 9) + (coupling_off ? 1 : 0) + (plan->src_hv ? 2 : 0);
   const bool cmf = plan->desc.constant_mass_flux != 0;
   return 3 * per_stage + (cmf ? 3 + 1 : 0);
 }

@@ -390,6 +390,30 @@ __global__ void k_add_source(Geo g, const double2* __restrict__ hv, const double
   }
 }
 
+// The (0, 0) column of an h_v source. There h_v = -D q - k^2 H1 reduces to
+// -D q, and D has a constant null space, so the source cannot enter through q
+// or H1; its interior part goes into the eigen coordinates instead:
+// X1(:, (0,0)) -= V^-1 hv(interior, (0,0)). The reference adds the source to
+// h_v at every wavenumber, (0, 0) included, and solves the v equation there
+// as at every other wavenumber (navier_stokes.py:1697-1703). One thread per
+// eigen row; single-run plans (the source is one field).
+__global__ void k_add_source00(Geo g, const double* __restrict__ vinv, int lda, const double2* __restrict__ hv,
+                               double* __restrict__ X1) {
+  const int n = g.ny - 2;
+  const size_t N = 2 * (size_t)g.nk * g.nb;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double a = vinv[(size_t)i * lda + j];
+      const double2 h = hv[(size_t)(j + 1) * g.nk];
+      re += a * h.x;
+      im += a * h.y;
+    }
+    X1[(size_t)i * N] -= re;
+    X1[(size_t)i * N + 1] -= im;
+  }
+}
+
 // forward z pass: block (kx in [0, K], y).
 template <typename C>
 __global__ void k_zfwd(Geo g, FftDesc fz, const C* __restrict__ tw, const C* __restrict__ out3,
