@@ -419,7 +419,8 @@ def run_ours(args):
                 per_kernel[k]["gbs"] = round(v["work"] / (v["ms"] / 1e3) / 1e9, 1)
         # side legs and kernel choices on their own lines, before the headline
         details = {pr: {"gemm_configs": {site: cfg for site, (cfg, _) in plans[pr].gemm_configs().items()},
-                        "split_kernel": plans[pr].split_kernel(), "xmid_variant": plans[pr].xmid_variant(),
+                        "split_kernel": plans[pr].split_kernel(), "split_eig_in": plans[pr].split_eig_in(),
+                        "xmid_variant": plans[pr].xmid_variant(),
                         "eig_kernels": {site: plans[pr].eig_kernel(i) for i, site in ((1, "eig_in"), (2, "eig_out"))}}
                    for pr in plans}
         print(json.dumps({"leg": "kernel_choices", "forms": details, "kernels": per_kernel}), flush=True)

@@ -28,8 +28,8 @@
 extern "C" {
 #endif
 
-#define JSD_ABI_VERSION 4  /* 2: jsd_desc gained n_batch, re_tau_batch; 3: JSD_ERR_NONFINITE, wait limit;
-                               4: jsd_set_source */
+#define JSD_ABI_VERSION 5  /* 2: jsd_desc gained n_batch, re_tau_batch; 3: JSD_ERR_NONFINITE, wait limit;
+                               4: jsd_set_source; 5: jsd_split_eig_in */
 
 enum jsd_status {
   JSD_OK = 0,
@@ -253,12 +253,23 @@ int jsd_xmid_variant(const jsd_plan* plan, float* times_ms);
  * plan's FFT length, precision or equation). No counterpart in the reference. */
 int jsd_set_xmid_variant(jsd_plan* plan, int variant);
 
-/* Split-TF32 y-derivative kernel of a mixed-precision plan: 0 mma.sync
- * (k_sgemm3), 1 tcgen05 with the accumulator in tensor memory
- * (k_tc05_dfield, Ny <= 129, the default); -1 for FP64 plans. times_ms (2 floats, may be
+/* Split-TF32 product kernel of a mixed-precision plan (y-derivatives, and
+ * the eigenbasis-in products of the nonlinear terms when those are split):
+ * 0 mma.sync (k_sgemm3), 1 tcgen05 with the accumulator in tensor memory
+ * (k_tc05_split, Ny <= 129, the default); -1 for FP64 plans. times_ms (2 floats, may be
  * null) receives the autotuner's timings. No counterpart in the reference. */
 int jsd_split_kernel(const jsd_plan* plan, float* times_ms);
 int jsd_set_split_kernel(jsd_plan* plan, int kernel);
+
+/* Eigenbasis-in products of the nonlinear terms (V^-1 D q, V^-1 H1,
+ * V^-1 h_g) of a mixed-precision plan: 1 in split TF32 on the split kernel
+ * (the default: the terms themselves come out of FP32 transforms and
+ * products), 0 FP64-accurate (DMMA or int8 Ozaki, as jsd_eig_kernel says);
+ * -1 for FP64 plans. The state's own eigenbasis products (V^-1 v, V^-1
+ * omega_y, V and D V back) stay FP64-accurate either way.
+ * No counterpart in the reference. */
+int jsd_split_eig_in(const jsd_plan* plan);
+int jsd_set_split_eig_in(jsd_plan* plan, int on);
 
 /* Eigenbasis product kernel of a plan at GEMM site 1 (eigenbasis in) or 2
  * (eigenbasis out): 0 FP64 DMMA (the default of FP64 plans), 1

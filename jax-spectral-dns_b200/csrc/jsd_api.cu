@@ -169,8 +169,14 @@ struct jsd_plan {
   // steady-state stages may do), packed D parts, kernel choice, error flag
   int tc_rows = 0;
   float *tc_ahi = nullptr, *tc_alo = nullptr;
-  double* tc_xrow = nullptr;  // Ny = 129: the last row of D (FP64, applied beside the tensor part)
-  int split_kernel = 0;         // 0: k_sgemm3 (mma.sync), 1: k_tc05_dfield (tcgen05)
+  double* tc_xrow = nullptr;  // Ny = 129: the last row of D (FP64, applied beside the tensor part; zero padded)
+  int split_kernel = 0;         // 0: k_sgemm3 (mma.sync), 1: k_tc05_split (tcgen05)
+  // split-TF32 eigenbasis-in products of the mixed form's FP32-accurate
+  // nonlinear terms: tcgen05 packs (index 0: V^-1 D, 1: V^-1) and row-major
+  // TF32 hi / lo parts padded to lda (k_sgemm3); off: FP64-accurate products
+  bool split_eig_in = false;
+  float *tc_ei_hi[2] = {}, *tc_ei_lo[2] = {};
+  float *ei_hi[2] = {}, *ei_lo[2] = {};
   int* errflag = nullptr;       // set by kernels whose bounded waits expired
   int num_sms = 148;
   float split_ms[2] = {};       // autotuner timings of the two split kernels
@@ -321,32 +327,92 @@ int launch_gemm(const jsd_plan* p, const GemmBatch& b, int max_m, GemmSite site,
 GemmBatch gemm_batch(const jsd_plan* p);
 void add_entry(GemmBatch& b, const double* A, const double* B, double* C, int M, int K, double alpha = 1.0);
 
-// y-derivatives D * f of up to kGemmMaxBatch fields: FP64 DMMA, or 3xTF32 in
-// the mixed-precision mode
-// Split-TF32 y-derivatives on tcgen05 (rows 0 .. tc_rows-1 of D).
+// 2-D tensor map of a row-major FP64 matrix (defined below)
 int oz_tensor_map(jsd_plan* p, const double* B, int N, int rows, int ldb, int box_cols, int box_rows, bool swizzle128,
                   CUtensorMap* out);
 
-// Split-TF32 y-derivatives on tcgen05 (all Ny <= 129 rows of D; row 128 in FP64).
-int launch_tc05(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
+// Split-TF32 products on tcgen05: dst[i] = A_op[i] src[i] (K[i] rows of
+// src, M <= 129 rows of the operators; row 128 of operator 0 in FP64 from
+// xrow), operators given as tc05_pack_a parts; c_f32: dst holds floats.
+int launch_tc05(jsd_plan* p, const float* const* a_hi, const float* const* a_lo, const int* op,
+                const double* const* src, const int* K, double* const* dst, int count, int M, const double* xrow,
+                cudaStream_t s, bool c_f32 = false) {
+  if (count < 1 || count > kGemmMaxBatch || M < 1 || M > kTcM + 1 || (M > kTcM && !xrow))
+    return fail(JSD_ERR_ARG, "tcgen05 split product: bad batch");
   Tc05Batch b;
   memset(&b, 0, sizeof(b));
   b.N = 2 * p->g.nk * p->g.nb;
-  b.M = p->tc_rows;
-  b.K = p->g.ny;
+  b.M = M;
   b.ldb = b.ldc = b.N;
-  b.xrow = p->tc_xrow;
+  b.xrow = xrow;
+  b.c_f32 = c_f32 ? 1 : 0;
+  b.prefetch = (b.ldb % 2) == 0 ? 1 : 0;
+  double flops = 0.0;
   for (int i = 0; i < count; ++i) {
-    if (reinterpret_cast<uintptr_t>(src[i]) % 16) return fail(JSD_ERR_STATE, "tcgen05 y-derivative needs 16-byte aligned rows");
-    int rc = oz_tensor_map(p, src[i], b.N, b.K, b.ldb, 32, kTcKp, false, &b.map[b.count]);
-    if (rc) return rc;
-    b.C[b.count++] = dst[i];
+    if (op[i] < 0 || op[i] >= kTcMaxOps || K[i] < 1 || K[i] > kTcKp || !a_hi[op[i]] || !a_lo[op[i]])
+      return fail(JSD_ERR_ARG, "tcgen05 split product: bad entry");
+    b.B[i] = src[i];
+    b.C[i] = dst[i];
+    b.K[i] = K[i];
+    b.op[i] = op[i];
+    if (reinterpret_cast<uintptr_t>(src[i]) % 16) b.prefetch = 0;
+    flops += 2.0 * M * (double)K[i] * b.N;
   }
+  for (int o = 0; o < kTcMaxOps; ++o) {
+    b.a_hi[o] = a_hi[o];
+    b.a_lo[o] = a_lo[o];
+  }
+  b.count = count;
   const int tiles = (b.N + kTcN - 1) / kTcN * b.count;
-  ProfScope ps(p, JSD_PROF_SGEMM, 2.0 * b.M * (double)b.K * b.N * count, s);
-  k_tc05_dfield<<<tiles < p->num_sms ? tiles : p->num_sms, kTcThreads, kTcSmem, s>>>(p->tc_ahi, p->tc_alo, b,
-                                                                                      p->errflag, p->wait_limit);
-  JSD_LAUNCHED("k_tc05_dfield");
+  ProfScope ps(p, JSD_PROF_SGEMM, flops, s);
+  k_tc05_split<<<tiles < p->num_sms ? tiles : p->num_sms, kTcThreads, kTcSmem, s>>>(b, p->errflag, p->wait_limit);
+  JSD_LAUNCHED("k_tc05_split");
+  return 0;
+}
+
+// D * f on tcgen05 (all Ny <= 129 rows of D; row 128 in FP64)
+int launch_tc05_dfield(jsd_plan* p, const double* const* src, double* const* dst, int count, cudaStream_t s) {
+  const float* hi[kTcMaxOps] = {p->tc_ahi, p->tc_ahi};
+  const float* lo[kTcMaxOps] = {p->tc_alo, p->tc_alo};
+  int op[kGemmMaxBatch] = {}, K[kGemmMaxBatch] = {};
+  for (int i = 0; i < count && i < kGemmMaxBatch; ++i) K[i] = p->g.ny;
+  return launch_tc05(p, hi, lo, op, src, K, dst, count, p->tc_rows, p->tc_xrow, s);
+}
+
+// Split-TF32 eigenbasis-in products of the nonlinear terms (mixed form):
+// X1 = V^-1 D q, T_0 = V^-1 H1, T_1 = V^-1 h_g (interior rows, stored in
+// FP32), on tcgen05 or k_sgemm3 as the plan's split-kernel choice says.
+int launch_split_eig_in(jsd_plan* p, cudaStream_t s) {
+  const int ny = p->g.ny, ni = ny - 2;
+  const size_t E = p->edoubles, rowd = 2 * (size_t)p->g.nk * p->g.nb;
+  const double* src[3] = {(const double*)p->q, (const double*)p->H1 + rowd, (const double*)p->hg + rowd};
+  double* dst[3] = {p->X1, p->T, p->T + E};
+  const int K[3] = {ny, ni, ni};
+  const int op[3] = {0, 1, 1};
+  if (p->split_kernel == 1 && p->tc_rows)
+    return launch_tc05(p, p->tc_ei_hi, p->tc_ei_lo, op, src, K, dst, 3, ni, nullptr, s, true);
+  SplitGemmBatch b;
+  memset(&b, 0, sizeof(b));
+  b.c_f32 = 1;
+  b.N = 2 * p->g.nk * p->g.nb;
+  b.lda = p->lda;
+  b.ldb = b.N;
+  b.ldc = b.N;
+  double flops = 0.0;
+  for (int i = 0; i < 3; ++i) {
+    SplitGemmEntry& e = b.e[b.count++];
+    e.Ahi = p->ei_hi[op[i]];
+    e.Alo = p->ei_lo[op[i]];
+    e.B = src[i];
+    e.C = dst[i];
+    e.M = ni;
+    e.K = K[i];
+    flops += 2.0 * ni * (double)K[i] * b.N;
+  }
+  ProfScope ps(p, JSD_PROF_SGEMM, flops, s);
+  const dim3 grid((b.N + Sgemm3Smem::BN - 1) / Sgemm3Smem::BN, 1, b.count);
+  k_sgemm3<<<grid, Sgemm3Smem::THREADS, Sgemm3Smem::BYTES, s>>>(b);
+  JSD_LAUNCHED("k_sgemm3");
   return 0;
 }
 
@@ -364,7 +430,7 @@ int launch_dfield(jsd_plan* p, const double* const* src, double* const* dst, int
   }
   const int kernel = force_split >= 0 ? force_split : p->split_kernel;
   (void)walls_free;  // the tcgen05 kernel computes every row, the y = -1 wall row in FP64
-  if (kernel == 1 && p->tc_rows) return launch_tc05(p, src, dst, count, s);
+  if (kernel == 1 && p->tc_rows) return launch_tc05_dfield(p, src, dst, count, s);
   SplitGemmBatch b;
   memset(&b, 0, sizeof(b));
   b.N = 2 * p->g.nk * p->g.nb;
@@ -548,7 +614,6 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
   const double2* u = state;
   const double2* v = state + fs;
   const double2* w = state + 2 * fs;
-  const int ny = g.ny;
   double2* conv = p->conv + (size_t)stage * 2 * gp.ny;
   const bool linear = p->desc.linearise && p->desc.kind != JSD_KIND_NS;
   if (p->desc.kind == JSD_KIND_DUAL && !linear && !uhist)
@@ -573,7 +638,6 @@ int nonlinear(jsd_plan* p, const double2* state, const double2* uhist, int stage
     return 0;
   }
   const bool dual = p->desc.kind == JSD_KIND_DUAL;
-  const int nsets = dual ? 2 : 1;
   {
     const double* src[6];
     double* dst[6];
@@ -761,21 +825,37 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
     k_omega<<<grid_for(fs, blk), blk, 0, s>>>(gp, u, w, p->om);
     JSD_LAUNCHED("k_omega");
   }
-  // eigenbasis transforms
+  // eigenbasis transforms. In the mixed form the nonlinear terms q, H1, h_g
+  // are FP32-accurate (FP32 transforms and products), so their products run
+  // in split TF32 like the y-derivatives and are kept in FP32 (X1, T_0, T_1
+  // and the previous stage's terms); V^-1 v and V^-1 omega_y of the state
+  // (first stage of a call) stay FP64-accurate. The linearised terms are
+  // formed in FP64 and keep FP64-accurate products.
+  const bool split_in = p->split_eig_in && !(p->desc.linearise && p->desc.kind != JSD_KIND_NS);
   {
     GemmBatch b = gemm_batch(p);
     const size_t E = p->edoubles;
     const size_t rowd = 2 * (size_t)g.nk * g.nb;  // doubles per Chebyshev row
-    add_entry(b, p->VinvD, (const double*)p->q, p->X1, ni, ny);
-    add_entry(b, p->Vinv, (const double*)p->H1 + rowd, p->T + 0 * E, ni, ni);
-    add_entry(b, p->Vinv, (const double*)p->hg + rowd, p->T + 1 * E, ni, ni);
+    if (split_in) {
+      rc = launch_split_eig_in(p, s);
+      if (rc) return rc;
+    } else {
+      add_entry(b, p->VinvD, (const double*)p->q, p->X1, ni, ny);
+      add_entry(b, p->Vinv, (const double*)p->H1 + rowd, p->T + 0 * E, ni, ni);
+      add_entry(b, p->Vinv, (const double*)p->hg + rowd, p->T + 1 * E, ni, ni);
+    }
     if (!p->ev_valid) add_entry(b, p->Vinv, (const double*)v + rowd, p->T + 2 * E, ni, ni);
     if (!p->om_valid) add_entry(b, p->Vinv, (const double*)p->om + rowd, p->T + 3 * E, ni, ni);
-    rc = launch_eig(p, b, ni, kSiteEigIn, s);
-    if (rc) return rc;
+    if (b.count) {
+      rc = launch_eig(p, b, ni, kSiteEigIn, s);
+      if (rc) return rc;
+    }
   }
   if (p->src_hv) {
-    k_add_source00<<<1, 128, 0, s>>>(g, p->Vinv, p->lda, p->src_hv, p->X1);
+    if (split_in)
+      k_add_source00<float><<<1, 128, 0, s>>>(g, p->Vinv, p->lda, p->src_hv, reinterpret_cast<float*>(p->X1));
+    else
+      k_add_source00<double><<<1, 128, 0, s>>>(g, p->Vinv, p->lda, p->src_hv, p->X1);
     JSD_LAUNCHED("k_add_source00");
   }
   {
@@ -784,27 +864,34 @@ int stage(jsd_plan* p, double2* state, double* dpdx, int st, int time_step, cuda
                  st == 0 ? 1 : 0};
     const int N = 2 * g.nk * g.nb;
     const size_t E = p->edoubles;
-    // reads X1, 4 transformed fields, 2 old terms; writes 2 old terms, v~ twice, om~
-    ProfScope ps(p, JSD_PROF_EIGEN, sizeof(double) * 13.0 * (double)E, s);
+    // reads X1, 4 transformed fields, 2 old terms; writes 2 old terms, v~, om~
+    // (X1, T_0, T_1 and the old terms in FP32 when split)
+    ProfScope ps(p, JSD_PROF_EIGEN, sizeof(double) * (split_in ? 7.5 : 11.0) * (double)E, s);
     // v~ and om~ carried from the last stage are read from vnt / omnt and the
     // update goes to their ping-pong partners, which then become vnt / omnt
     const double* vt = p->ev_valid ? p->vnt : p->T + 2 * E;
     const double* omt = p->om_valid ? p->omnt : p->T + 3 * E;
     if (p->ev_valid) std::swap(p->vnt, p->vnt_alt);
     if (p->om_valid) std::swap(p->omnt, p->omnt_alt);
-    k_eigen_update<<<(N + kEigCols - 1) / kEigCols, kEigCols * kEigParts, 0, s>>>(
-        g, t, sc, p->X1, p->T, p->T + E, vt, omt, (const double*)v, p->hv_old, p->hg_old, p->vnt, p->omnt);
+    const int blocks = (N + kEigCols - 1) / kEigCols, rpp = eigen_update_rpp(ny);
+    const size_t sm = eigen_update_smem(ny);
+    if (split_in)
+      k_eigen_update<float><<<blocks, kEigCols * kEigParts, sm, s>>>(
+          g, t, sc, reinterpret_cast<const float*>(p->X1), reinterpret_cast<const float*>(p->T),
+          reinterpret_cast<const float*>(p->T + E), vt, omt, (const double*)v, reinterpret_cast<float*>(p->hv_old),
+          reinterpret_cast<float*>(p->hg_old), p->vnt, p->omnt, rpp);
+    else
+      k_eigen_update<double><<<blocks, kEigCols * kEigParts, sm, s>>>(
+          g, t, sc, p->X1, p->T, p->T + E, vt, omt, (const double*)v, p->hv_old, p->hg_old, p->vnt, p->omnt, rpp);
     JSD_LAUNCHED("k_eigen_update");
   }
   {
     const size_t n2 = 2 * (size_t)ny;
-    const double* rns = p->rhs_ns + (size_t)st * n2 * n2;
     const double* lns = p->lhs_inv_ns + (size_t)st * n2 * n2;
     const double2* conv = p->conv + (size_t)st * 2 * gp.ny;
     const double2* conv_old = st == 0 ? nullptr : p->conv + (size_t)(st - 1) * 2 * gp.ny;
     const double dte = p->desc.dt_explicit;
     // per-run matrices: lr / lns point at run 0's stage-st matrices, the kernel offsets by run
-    (void)rns;
     const double* lr = p->lr_ns + (size_t)st * n2 * n2;
     const dim3 grid((unsigned)((n2 + kMeanFlowRows - 1) / kMeanFlowRows), (unsigned)g.nb);
     k_mean_flow_rows<<<grid, 32 * kMeanFlowRows, sizeof(double2) * 2 * n2, s>>>(
@@ -942,7 +1029,9 @@ int set_smem_limits() {
   }
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   JSD_CUDA(cudaFuncSetAttribute(k_mean_flow_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  JSD_CUDA(cudaFuncSetAttribute(k_tc05_dfield, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
+  JSD_CUDA(cudaFuncSetAttribute(k_eigen_update<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_eigen_update<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  JSD_CUDA(cudaFuncSetAttribute(k_tc05_split, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmem));
   JSD_CUDA(cudaFuncSetAttribute(k_oz8_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kOzSmem));
   cudaError_t err = cudaSuccess;
   for (int sd : kSquareSides)
@@ -1152,16 +1241,28 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
       }
     }
   }
-  // split-TF32 y-derivative kernels (mixed plans): the steady-state call on u and w
+  // split-TF32 product kernels (mixed plans)
   if (rc == 0 && plan->mixed && plan->tc_rows) {
     const double* src[2] = {(const double*)plan->q, (const double*)plan->H1};
     double* dst[2] = {(double*)plan->Dfld, (double*)(plan->Dfld + 2 * fs)};
     float best = 3.0e38f;
+    // both calls of a steady stage that use the kernel: D on u and w, and
+    // the split eigenbasis-in products when the plan splits them
+    const int keep = plan->split_kernel;
+    auto run = [&](int k) {
+      int r = launch_dfield(plan, src, dst, 2, s, true, k);
+      if (r == 0 && plan->split_eig_in) {
+        plan->split_kernel = k;
+        r = launch_split_eig_in(plan, s);
+        plan->split_kernel = keep;
+      }
+      return r;
+    };
     for (int k = 0; k < 2 && rc == 0; ++k) {
-      rc = launch_dfield(plan, src, dst, 2, s, true, k);  // warm-up
+      rc = run(k);  // warm-up
       if (rc) break;
       if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(JSD_ERR_CUDA, "cudaEventRecord");
-      for (int r = 0; r < 5 && rc == 0; ++r) rc = launch_dfield(plan, src, dst, 2, s, true, k);
+      for (int r = 0; r < 5 && rc == 0; ++r) rc = run(k);
       if (rc) break;
       float ms = 0.f;
       if (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
@@ -1221,6 +1322,19 @@ int jsd_set_split_kernel(jsd_plan* plan, int kernel) {
   if (!plan->mixed || kernel < 0 || kernel > 1 || (kernel == 1 && !plan->tc_rows))
     return fail(JSD_ERR_ARG, "split-TF32 kernel not available for this plan");
   plan->split_kernel = kernel;
+  return 0;
+}
+
+int jsd_split_eig_in(const jsd_plan* plan) {
+  if (!plan) return -1;
+  return plan->mixed ? (plan->split_eig_in ? 1 : 0) : -1;
+}
+
+int jsd_set_split_eig_in(jsd_plan* plan, int on) {
+  if (!plan) return fail(JSD_ERR_ARG, "null plan");
+  if (!plan->mixed || !plan->ei_hi[0] || (on != 0 && on != 1))
+    return fail(JSD_ERR_ARG, "split eigenbasis-in products need a mixed-precision plan (Ny - 2 <= 144)");
+  plan->split_eig_in = on == 1;
   return 0;
 }
 
@@ -1449,13 +1563,39 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
       }
     JSD_TRY(upload(p, &p->Dhi, hi.data(), hi.size()));
     JSD_TRY(upload(p, &p->Dlo, lo.data(), lo.size()));
-    if (ny <= kTcM + 1 && tensor_map_encoder()) {
+    // V^-1 D and V^-1 split the same way (eigenbasis-in products of the
+    // FP32-accurate nonlinear terms)
+    const double* eiA[2] = {VinvD.data(), d->Vinv};
+    const int eiK[2] = {ny, ni};
+    for (int k = 0; k < 2; ++k) {
+      std::vector<float> eh((size_t)ni * p->lda, 0.f), el((size_t)ni * p->lda, 0.f);
+      for (int r = 0; r < ni; ++r)
+        for (int c = 0; c < eiK[k]; ++c) {
+          const double x = eiA[k][(size_t)r * eiK[k] + c];
+          const float h = tf32_round((float)x);
+          eh[(size_t)r * p->lda + c] = h;
+          el[(size_t)r * p->lda + c] = tf32_round((float)(x - (double)h));
+        }
+      JSD_TRY(upload(p, &p->ei_hi[k], eh.data(), eh.size()));
+      JSD_TRY(upload(p, &p->ei_lo[k], el.data(), el.size()));
+    }
+    p->split_eig_in = ni <= Sgemm3Smem::BM;
+    if (ny <= kTcM + 1) {
       p->tc_rows = ny;
       std::vector<float> ahi, alo;
       tc05_pack_a(d->D, ny, ny, ny, tf32_round, ahi, alo);
       JSD_TRY(upload(p, &p->tc_ahi, ahi.data(), ahi.size()));
       JSD_TRY(upload(p, &p->tc_alo, alo.data(), alo.size()));
-      if (ny > kTcM) JSD_TRY(upload(p, &p->tc_xrow, d->D + (size_t)kTcM * ny, (size_t)ny));
+      for (int k = 0; k < 2; ++k) {
+        tc05_pack_a(eiA[k], ni, eiK[k], eiK[k], tf32_round, ahi, alo);
+        JSD_TRY(upload(p, &p->tc_ei_hi[k], ahi.data(), ahi.size()));
+        JSD_TRY(upload(p, &p->tc_ei_lo[k], alo.data(), alo.size()));
+      }
+      if (ny > kTcM) {
+        std::vector<double> xr(kTcKp, 0.0);
+        for (int c = 0; c < ny; ++c) xr[c] = d->D[(size_t)kTcM * ny + c];
+        JSD_TRY(upload(p, &p->tc_xrow, xr.data(), xr.size()));
+      }
       // the tcgen05 kernel is the default (58 us per call against 86 us for
       // k_sgemm3 at 128 x 129 x 128); the autotuner re-decides per plan
       p->split_kernel = 1;

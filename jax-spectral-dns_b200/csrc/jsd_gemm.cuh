@@ -221,6 +221,7 @@ struct SplitGemmBatch {
   SplitGemmEntry e[kGemmMaxBatch];
   int count;
   int N, lda, ldb, ldc;
+  int c_f32;  // C holds floats (same element offsets)
 };
 
 __device__ __forceinline__ unsigned tf32_bits(float x) {
@@ -340,9 +341,14 @@ __global__ void __launch_bounds__(Sgemm3Smem::THREADS) k_sgemm3(SplitGemmBatch b
 #pragma unroll
       for (int j = 0; j < TN; ++j) {
         const int col = n0 + wn + j * 8 + 2 * t;
-        if (col < N)
-          *reinterpret_cast<double2*>(e.C + (size_t)r * ldc + col) =
-              make_double2((double)acc[i][j][2 * h], (double)acc[i][j][2 * h + 1]);
+        if (col < N) {
+          if (batch.c_f32)
+            *reinterpret_cast<float2*>(reinterpret_cast<float*>(e.C) + (size_t)r * ldc + col) =
+                make_float2(acc[i][j][2 * h], acc[i][j][2 * h + 1]);
+          else
+            *reinterpret_cast<double2*>(e.C + (size_t)r * ldc + col) =
+                make_double2((double)acc[i][j][2 * h], (double)acc[i][j][2 * h + 1]);
+        }
       }
     }
   }

@@ -397,8 +397,9 @@ __global__ void k_add_source(Geo g, const double2* __restrict__ hv, const double
 // h_v at every wavenumber, (0, 0) included, and solves the v equation there
 // as at every other wavenumber (navier_stokes.py:1697-1703). One thread per
 // eigen row; single-run plans (the source is one field).
+template <typename TI>
 __global__ void k_add_source00(Geo g, const double* __restrict__ vinv, int lda, const double2* __restrict__ hv,
-                               double* __restrict__ X1) {
+                               TI* __restrict__ X1) {
   const int n = g.ny - 2;
   const size_t N = 2 * (size_t)g.nk * g.nb;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -409,8 +410,8 @@ __global__ void k_add_source00(Geo g, const double* __restrict__ vinv, int lda, 
       re += a * h.x;
       im += a * h.y;
     }
-    X1[(size_t)i * N] -= re;
-    X1[(size_t)i * N + 1] -= im;
+    X1[(size_t)i * N] = (TI)((double)X1[(size_t)i * N] - re);
+    X1[(size_t)i * N + 1] = (TI)((double)X1[(size_t)i * N + 1] - im);
   }
 }
 
@@ -595,12 +596,23 @@ constexpr int kEigCols = 32;    // columns per block (one warp-wide row segment)
 constexpr int kEigParts = 4;    // warps per block, each walking a quarter of the eigen rows
 constexpr int kEigBatch = 4;    // rows whose loads are issued together (loads in flight per thread: 7 x batch)
 
+// Rows of a block's part: j1 - j0 <= ceil((Ny - 2) / kEigParts). The first
+// pass keeps v_p~ of its rows in shared memory for the second (rpp rows per
+// part, dynamic shared memory of eigen_update_smem bytes).
+inline int eigen_update_rpp(int ny) { return (ny - 2 + kEigParts - 1) / kEigParts; }
+inline size_t eigen_update_smem(int ny) { return sizeof(double) * kEigParts * eigen_update_rpp(ny) * kEigCols; }
+
+// TI: storage of the nonlinear terms (X1, H1~, h_g~ and the previous stage's
+// h_v~, h_g~): double, or float where they come out of FP32 transforms and
+// products (the mixed form)
+template <typename TI>
 __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
-    Geo g, EigTables t, StageCoef sc, const double* __restrict__ X1, const double* __restrict__ H1t,
-    const double* __restrict__ hgt, const double* __restrict__ vt, const double* __restrict__ omt,
-    const double* __restrict__ vfield, double* __restrict__ hv_old, double* __restrict__ hg_old,
-    double* __restrict__ vnt, double* __restrict__ omnt) {
+    Geo g, EigTables t, StageCoef sc, const TI* __restrict__ X1, const TI* __restrict__ H1t,
+    const TI* __restrict__ hgt, const double* __restrict__ vt, const double* __restrict__ omt,
+    const double* __restrict__ vfield, TI* __restrict__ hv_old, TI* __restrict__ hg_old,
+    double* __restrict__ vnt, double* __restrict__ omnt, int rpp) {
   __shared__ double red[kEigParts][6][kEigCols];
+  extern __shared__ double vps_all[];
   const int N = 2 * g.nk * g.nb;  // columns: real and imaginary parts of every mode of every run
   const int lane = threadIdx.x % kEigCols;
   const int part = threadIdx.x / kEigCols;
@@ -608,6 +620,7 @@ __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
   const bool active = c < N;
   const int n = g.ny - 2;
   const int j0 = (n * part) / kEigParts, j1 = (n * (part + 1)) / kEigParts;
+  double* vps = vps_all + (size_t)part * rpp * kEigCols + lane;  // v_p~ of row j at vps[(j - j0) * kEigCols]
   double k2 = 0.0, v0 = 0.0, vN = 0.0, re = sc.re;
   if (active) {
     const int run = (c >> 1) / g.nk;
@@ -623,14 +636,17 @@ __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
   const double br = sc.beta * sc.dt / re;
   double d0p = 0, dNp = 0, d0a = 0, dNa = 0, d0b = 0, dNb = 0;
   if (active) {
-    for (int jb = j0; jb < j1; jb += kEigBatch) {
+    // rows whose loads are in flight together: more when the terms are FP32
+    constexpr int NB = sizeof(TI) == 4 ? 2 * kEigBatch : kEigBatch;
+    for (int jb = j0; jb < j1; jb += NB) {
       // all loads of the batch first (independent rows), then the arithmetic
-      double x1[kEigBatch], h1[kEigBatch], hg[kEigBatch], vv[kEigBatch], om[kEigBatch], hvo[kEigBatch],
-          hgo[kEigBatch];
+      TI x1[NB], h1[NB], hg[NB], hvo[NB], hgo[NB];
+      double vv[NB], om[NB];
 #pragma unroll
-      for (int b = 0; b < kEigBatch; ++b) {
+      for (int b = 0; b < NB; ++b) {
         const int j = jb + b;
-        x1[b] = h1[b] = hg[b] = vv[b] = om[b] = hvo[b] = hgo[b] = 0.0;
+        x1[b] = h1[b] = hg[b] = hvo[b] = hgo[b] = (TI)0;
+        vv[b] = om[b] = 0.0;
         if (j < j1) {
           const size_t o = (size_t)j * N + c;
           x1[b] = X1[o];
@@ -645,18 +661,18 @@ __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
         }
       }
 #pragma unroll
-      for (int b = 0; b < kEigBatch; ++b) {
+      for (int b = 0; b < NB; ++b) {
         const int j = jb + b;
         if (j >= j1) break;
         const size_t o = (size_t)j * N + c;
         const double L = t.lam[j] - k2;
         const double R = 1.0 + ar * L;
         const double H = 1.0 - br * L;
-        const double ih = 1.0 / H;
-        const double ihl = ih / L;
-        const double hv = -x1[b] - k2 * h1[b];
+        const double ihl = 1.0 / (H * L);  // one reciprocal: 1 / H = L / (H L)
+        const double ih = L * ihl;
+        const double hv = -(double)x1[b] - k2 * (double)h1[b];
         const double phi = L * vv[b] + t.c0[j] * v0 + t.cN[j] * vN;
-        const double vp = (R * phi + sc.dt_e * (sc.gamma * hv + sc.xi * hvo[b])) * ihl;
+        const double vp = (R * phi + sc.dt_e * (sc.gamma * hv + sc.xi * (double)hvo[b])) * ihl;
         const double va = br * t.c0[j] * ihl;
         const double w0 = t.w0[j], wN = t.wN[j], sg = t.sgn[j];
         d0p += w0 * vp;
@@ -665,9 +681,9 @@ __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
         dNa += wN * va;
         d0b += w0 * sg * va;
         dNb += wN * sg * va;
-        vnt[o] = vp;
-        hv_old[o] = hv;
-        omnt[o] = (R * om[b] + sc.dt_e * (sc.gamma * hg[b] + sc.xi * hgo[b])) * ih;
+        vps[(j - j0) * kEigCols] = vp;
+        hv_old[o] = (TI)hv;
+        omnt[o] = (R * om[b] + sc.dt_e * (sc.gamma * (double)hg[b] + sc.xi * (double)hgo[b])) * ih;
         hg_old[o] = hg[b];
       }
     }
@@ -692,20 +708,11 @@ __global__ void __launch_bounds__(kEigCols * kEigParts, 4) k_eigen_update(
   const double ra = -sum[0], rb = -sum[1];
   const double a = (sum[5] * ra - sum[4] * rb) / det;
   const double b = (-sum[3] * ra + sum[2] * rb) / det;
-  for (int jb = j0; jb < j1; jb += kEigBatch) {
-    double vp[kEigBatch];
-#pragma unroll
-    for (int q = 0; q < kEigBatch; ++q)
-      vp[q] = (jb + q < j1) ? vnt[(size_t)(jb + q) * N + c] : 0.0;
-#pragma unroll
-    for (int q = 0; q < kEigBatch; ++q) {
-      const int j = jb + q;
-      if (j >= j1) break;
-      const double L = t.lam[j] - k2;
-      const double H = 1.0 - br * L;
-      const double va = br * t.c0[j] / (H * L);
-      vnt[(size_t)j * N + c] = vp[q] + (a + b * t.sgn[j]) * va;
-    }
+  for (int j = j0; j < j1; ++j) {
+    const double L = t.lam[j] - k2;
+    const double H = 1.0 - br * L;
+    const double va = br * t.c0[j] * (1.0 / (H * L));
+    vnt[(size_t)j * N + c] = vps[(j - j0) * kEigCols] + (a + b * t.sgn[j]) * va;
   }
 }
 

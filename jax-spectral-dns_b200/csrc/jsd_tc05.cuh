@@ -1,30 +1,37 @@
 // tcgen05 building blocks (shared-memory descriptors, mbarriers with bounded
-// waits, bulk and TMA copies, tensor-memory loads) and the split-TF32
-// y-derivative kernel on the 5th-generation tensor cores.
+// waits, bulk and TMA copies, tensor-memory loads) and the split-TF32 product
+// kernel on the 5th-generation tensor cores.
 //
-// k_tc05_dfield: C (M x N, FP64) = D (M x K) * B (K x N, FP64) for the
-// Chebyshev derivative matrix D (M = K = Ny <= 129), as three TF32 products
-// D_hi B_hi + D_lo B_hi + D_hi B_lo with FP32 accumulation in tensor memory
-// (the same 3xTF32 scheme as k_sgemm3). One persistent CTA of 27 warps per SM,
-// each CTA a contiguous range of 32-column tiles:
-//   * warp 26 (producer): one 2-D TMA load (cp.async.bulk.tensor, mbarrier
-//     completion) of the tile's 136 x 32 FP64 block of B into a staging buffer
-//     (rows past K and columns past N arrive as zeros);
-//   * warps 0-16 (converters, warp w = rows 8w..8w+7, lane = column): split the
-//     staged values into TF32 hi and lo and store them as one 64-row K-major
-//     operand (hi rows 0-31, lo rows 32-63); for Ny = 129 they also form the
-//     FP64 dot products of D's last row (y = -1) with their rows;
-//   * warp 25 (issuer): keeps D_hi / D_lo resident (bulk copy once), issues per
-//     K step of 8 two tcgen05.mma.kind::tf32 (M = 128): D_hi x [B_hi; B_lo]
-//     (N = 64: hi*hi into columns 0-31, hi*lo into 32-63) and D_lo x B_hi
-//     (N = 32, into columns 0-31), into one of two 64-column accumulator sets;
+// k_tc05_split: C_i (M x N, FP64) = A_op(i) (M x K_i) * B_i (K_i x N, FP64) for
+// a batch of fields B_i and at most two operators A (M <= 129 rows, K <= 136),
+// as three TF32 products A_hi B_hi + A_lo B_hi + A_hi B_lo with FP32
+// accumulation in tensor memory (the same 3xTF32 scheme as k_sgemm3): the
+// Chebyshev derivative D on the state (y-derivatives), and V^-1 D, V^-1 on the
+// nonlinear terms (eigenbasis-in products of FP32-accurate data in the mixed
+// form). One persistent CTA of 26 warps per SM, each CTA a contiguous range of
+// 32-column tiles (entry-major):
+//   * warps 0-16 (converters, warp w = rows 8w..8w+7, lane = column): load the
+//     tile's values straight from global memory (coalesced 256-byte rows,
+//     rows past K_i and columns past N as zeros), one tile ahead: the loads of
+//     tile i + 1 are issued before tile i is stored, so they land while tile i
+//     is multiplied; split the values into TF32 hi and lo and store them as
+//     one 64-row K-major operand (hi rows 0-31, lo rows 32-63) in one of two
+//     operand buffers; for M = 129 they also form the FP64 dot products of
+//     the operator's last row with their rows;
+//   * warp 25 (issuer): keeps A_hi / A_lo of the current operator resident
+//     (bulk copy; reloaded when the entry's operator changes, after the MMAs
+//     issued so far completed), issues per K step of 8 two
+//     tcgen05.mma.kind::tf32 (M = 128): A_hi x [B_hi; B_lo] (N = 64: hi*hi
+//     into columns 0-31, hi*lo into 32-63) and A_lo x B_hi (N = 32, into
+//     columns 0-31), into one of two 64-column accumulator sets;
 //   * warps 17-24 (epilogue, TMEM lane quadrant = warp % 4, half of the
 //     columns each): read both accumulators (tcgen05.ld), add them in FP64 and
-//     store; the last row (Ny = 129) from the converters' partial dots.
+//     store rows < min(M, 128); row 128 (M = 129) from the converters' dots.
 // Every mbarrier wait has an iteration limit (a kernel argument); on expiry the
 // kernel raises the error flag, every role stops at its next tile, the issuer
-// waits (bounded) for its operand copy and its last MMAs, the producer for its
-// last staged load, and the CTA frees its TMEM and returns.
+// waits (bounded) for its operand copy and its last MMAs, and the CTA frees
+// its TMEM and returns (the converters' loads go to registers: nothing of
+// theirs is in flight into shared memory).
 //
 // Canonical K-major layout without swizzle (units of 16 bytes = 4 TF32): a core
 // matrix is 8 rows x 16 bytes stored contiguously; core matrix (row group g,
@@ -55,23 +62,29 @@ constexpr int kTcN = 32;                       // columns per tile
 constexpr int kTcASize = kTcM * kTcKp * 4;     // bytes of one A part (69632)
 constexpr int kTcBRows = 2 * kTcN;             // stacked B operand rows (hi, lo)
 constexpr int kTcBSize = kTcBRows * kTcKp * 4;  // 34816
-constexpr int kTcStageBytes = kTcKp * kTcN * 8;  // 34816
 constexpr int kTcConvWarps = kTcKp / 8, kTcEpiWarps = 8;
-constexpr int kTcIssuerWarp = kTcConvWarps + kTcEpiWarps, kTcProducerWarp = kTcIssuerWarp + 1;
-constexpr int kTcThreads = 32 * (kTcProducerWarp + 1);  // 864
-constexpr int kTcSideDoubles = kTcConvWarps * kTcN;      // partial dots of the last row
-constexpr int kTcTmemCols = 2 * 2 * kTcN;                // two sets of (hi*hi + lo*hi, hi*lo)
-constexpr size_t kTcSmem =
-    2 * (size_t)kTcASize + kTcBSize + kTcStageBytes + 2 * sizeof(double) * kTcSideDoubles + 128;
+constexpr int kTcIssuerWarp = kTcConvWarps + kTcEpiWarps;
+constexpr int kTcThreads = 32 * (kTcIssuerWarp + 1);  // 832
+constexpr int kTcSideDoubles = kTcConvWarps * kTcN;   // partial dots of the last row
+constexpr int kTcTmemCols = 2 * 2 * kTcN;             // two sets of (hi*hi + lo*hi, hi*lo)
+constexpr int kTcMaxOps = 2;                          // operators per launch
+constexpr size_t kTcSmem = 2 * (size_t)kTcASize + 2 * (size_t)kTcBSize + 2 * sizeof(double) * kTcSideDoubles + 128;
 
-// map: 2-D tensor map of B[i] (inner N doubles, outer K rows, row stride
-// ldb), box 32 x 136
+// B[i]: K[i] x N FP64 (row stride ldb), multiplied by operator op[i]; the
+// operator parts are packed by tc05_pack_a; xrow: the FP64 row 128 of
+// operator 0 when M = 129 (kTcKp values, zero padded), else null
 struct Tc05Batch {
-  CUtensorMap map[kGemmMaxBatch];
+  const double* B[kGemmMaxBatch];
   double* C[kGemmMaxBatch];
-  const double* xrow;  // M = 129: row 128 of D (K values), else null
+  int K[kGemmMaxBatch];
+  int op[kGemmMaxBatch];
+  const float* a_hi[kTcMaxOps];
+  const float* a_lo[kTcMaxOps];
+  const double* xrow;
   int count;
-  int M, N, K, ldb, ldc;
+  int M, N, ldb, ldc;
+  int c_f32;     // C holds floats (same element offsets)
+  int prefetch;  // every B[i] is 16-byte aligned: rows may be bulk-prefetched into L2
 };
 
 // byte offset of element (row r, k) of an R-row TF32 operand in the core-matrix layout
@@ -170,28 +183,53 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
       : "r"(taddr));
 }
 
+// 16 TMEM lanes x 4 repetitions of 256 bits (8 columns): thread (lane % 4,
+// lane / 4) receives rows lane / 4 and lane / 4 + 8, columns 8 p + 2 (lane % 4)
+// and + 1 of repetition p, in registers 4 p + {0, 1} and 4 p + {2, 3}
+__device__ __forceinline__ void tc_ld16x256b_x4(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.16x256b.x4.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+
 __device__ __forceinline__ float tf32_round_dev(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
 }
+
+// `bytes` (a multiple of 16) from a 16-byte aligned global address into L2
+__device__ __forceinline__ void tc_prefetch_l2(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// *p when c, else 0; volatile, so a prefetch is issued where it stands and is
+// waited for only where its value is first used
+__device__ __forceinline__ double tc_load_if(const double* p, bool c) {
+  double x = 0.0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %2, 0;\n\t@p ld.global.nc.L1::no_allocate.f64 %0, [%1];\n\t}\n"
+      : "+d"(x)
+      : "l"(p), "r"((int)c));
+  return x;
+}
 #endif
 
-__global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __restrict__ a_hi,
-                                                               const float* __restrict__ a_lo,
-                                                               const __grid_constant__ Tc05Batch b,
-                                                               int* __restrict__ err, int spin) {
+__global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_constant__ Tc05Batch b,
+                                                              int* __restrict__ err, int spin) {
 #if defined(__CUDA_ARCH__)
   extern __shared__ __align__(1024) unsigned char tsm[];
   unsigned char* sAh = tsm;
   unsigned char* sAl = tsm + kTcASize;
-  unsigned char* sB = tsm + 2 * kTcASize;                       // stacked hi / lo operand
-  double* stage = reinterpret_cast<double*>(sB + kTcBSize);      // staged FP64 tile, row k at 32 k
-  double* side = stage + kTcKp * kTcN;                          // two tile buffers of partial dots
+  unsigned char* sB0 = tsm + 2 * kTcASize;                      // two stacked hi / lo operands
+  double* side = reinterpret_cast<double*>(sB0 + 2 * kTcBSize);  // two tile buffers of partial dots
   uint64_t* bars = reinterpret_cast<uint64_t*>(side + 2 * kTcSideDoubles);
   // bars: 0,1 full (B operand + partial dots of tile parity); 2,3 mma done;
-  // 4,5 epilogue done; 6 A loaded; 7 staged tile ready; 8 staging released
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 9);
+  // 4,5 epilogue done; 6 A loaded
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 7);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto bar = [&](int i) { return tc_smem(&bars[i]); };
@@ -203,8 +241,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
     mbar_init(bar(4), 32 * kTcEpiWarps);
     mbar_init(bar(5), 32 * kTcEpiWarps);
     mbar_init(bar(6), 1);
-    mbar_init(bar(7), 1);
-    mbar_init(bar(8), 32 * kTcConvWarps);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -223,7 +259,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
   const int t_begin = (int)(total * blockIdx.x / gridDim.x);
   const int t_end = (int)(total * (blockIdx.x + 1) / gridDim.x);
   const int nt = t_end - t_begin;
-  const int ksteps = (b.K + 7) / 8;  // <= kTcKp / 8
   auto fail_now = [&]() {
     *abort_flag = 1;
     atomicOr(err, kErrWaitExpired);
@@ -232,55 +267,96 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
   if (warp < kTcConvWarps) {
     // ---------------------------------------------------------------- converters
     const int n = lane, k0 = 8 * warp;
-    for (int i = 0; i < nt && !*abort_flag; ++i) {
-      const int buf = i & 1;
+    double xa[8], xb[8];  // two tiles in flight: the loads of tile i + 2 are issued once tile i is stored
+    auto fetch = [&](int i, double(&x)[8]) {
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
-      const bool cv = n0 + n < b.N;
-      bool ok = mbar_wait(bar(7), i & 1, spin);
-      if (!__all_sync(0xffffffffu, ok)) {
-        fail_now();
-        break;
-      }
-      double x[8];
+      const double* B = b.B[0];
+      int K = b.K[0];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) x[j] = cv ? stage[(k0 + j) * kTcN + n] : 0.0;  // rows >= K arrive as zeros
-      tc_arrive(bar(8));  // staging may be refilled
+      for (int q = 1; q < kGemmMaxBatch; ++q)
+        if (e == q) {
+          B = b.B[q];
+          K = b.K[q];
+        }
+      const bool cv = n0 + n < b.N;
+      const double* src = B + (size_t)k0 * b.ldb + n0 + n;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) x[j] = tc_load_if(src + (size_t)j * b.ldb, cv && k0 + j < K);
+    };
+    // the 8 rows of this warp of tile i into L2 (lane j < 8: row k0 + j, one
+    // bulk prefetch of the tile's 256-byte row segment or the part inside N)
+    auto prefetch = [&](int i) {
+      if (!b.prefetch || lane >= 8) return;
+      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
+      const double* B = b.B[0];
+      int K = b.K[0];
+#pragma unroll
+      for (int q = 1; q < kGemmMaxBatch; ++q)
+        if (e == q) {
+          B = b.B[q];
+          K = b.K[q];
+        }
+      const int cols = b.N - n0 < kTcN ? b.N - n0 : kTcN;  // even: N and n0 are
+      if (k0 + lane < K) tc_prefetch_l2(B + (size_t)(k0 + lane) * b.ldb + n0, (uint32_t)cols * 8u);
+    };
+    // tile i from registers x into operand buffer i % 2; then x takes the
+    // loads of tile i + 2 (from L2: prefetched a tile earlier), which land
+    // while tiles i and i + 1 are multiplied
+    auto body = [&](int i, double(&x)[8]) -> bool {
+      const int buf = i & 1;
       double dot = 0.0;
       if (b.M > kTcM) {
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
-          if (k0 + j < b.K) dot = fma(__ldg(b.xrow + k0 + j), x[j], dot);
+        for (int j = 0; j < 8; ++j) dot = fma(__ldg(b.xrow + k0 + j), x[j], dot);  // xrow is zero padded
       }
-      uint32_t hi[8], lo[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const float h = tf32_round_dev((float)x[j]);
-        hi[j] = __float_as_uint(h);
-        lo[j] = __float_as_uint(tf32_round_dev((float)(x[j] - (double)h)));
-      }
-      // the B operand is free once the previous tile's MMAs completed; the
-      // partial dots once the epilogue of the tile two back is done
-      ok = (i < 1 || mbar_wait(bar(2 + ((i - 1) & 1)), ((i - 1) >> 1) & 1, spin)) &&
-           (i < 2 || mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1, spin));
+      // operand buffer `buf` is free once the MMAs of tile i - 2 completed, its
+      // partial dots once the epilogue of tile i - 2 is done
+      const bool ok = i < 2 || (mbar_wait(bar(2 + buf), ((i - 2) >> 1) & 1, spin) &&
+                                mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1, spin));
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
-        break;
+        return false;
       }
+      unsigned char* sB = sB0 + buf * kTcBSize;
+      // one FP64 conversion per value: hi + lo keep 22 of the FP32 value's 24
+      // bits, and f - hi is exact in FP32
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
-        *reinterpret_cast<uint4*>(sB + tc05_offset(kTcBRows, n, k0 + 4 * c)) =
-            make_uint4(hi[4 * c], hi[4 * c + 1], hi[4 * c + 2], hi[4 * c + 3]);
+        uint32_t hi[4], lo[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const float f = (float)x[4 * c + j];
+          const float h = tf32_round_dev(f);
+          hi[j] = __float_as_uint(h);
+          lo[j] = __float_as_uint(tf32_round_dev(f - h));
+        }
+        *reinterpret_cast<uint4*>(sB + tc05_offset(kTcBRows, n, k0 + 4 * c)) = make_uint4(hi[0], hi[1], hi[2], hi[3]);
         *reinterpret_cast<uint4*>(sB + tc05_offset(kTcBRows, kTcN + n, k0 + 4 * c)) =
-            make_uint4(lo[4 * c], lo[4 * c + 1], lo[4 * c + 2], lo[4 * c + 3]);
+            make_uint4(lo[0], lo[1], lo[2], lo[3]);
       }
       side[buf * kTcSideDoubles + warp * kTcN + n] = dot;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
       tc_arrive(bar(buf));
+      if (i + 2 < nt) fetch(i + 2, x);
+      if (i + 3 < nt) prefetch(i + 3);
+      return true;
+    };
+    if (nt > 0) fetch(0, xa);
+    if (nt > 1) fetch(1, xb);
+    if (nt > 2) prefetch(2);
+    for (int i = 0; i < nt && !*abort_flag; i += 2) {
+      if (!body(i, xa)) break;
+      if (i + 1 < nt && !*abort_flag && !body(i + 1, xb)) break;
     }
   } else if (warp < kTcConvWarps + kTcEpiWarps) {
     // ----------------------------------------------------------------- epilogue
-    const int ew = warp - kTcConvWarps, quad = warp & 3, half = ew >> 2;
-    const int row = 32 * quad + lane, c0 = 16 * half;
+    // warp: TMEM lane quadrant warp % 4 (the lanes it may access), 16-lane
+    // half lh of it; tcgen05.ld 16x256b: thread (t0, t1) = (lane % 4, lane / 4)
+    // holds rows t1 and t1 + 8 of the half, columns 8p + 2 t0 and + 1 of
+    // repetition p, so a quad of threads stores 64 contiguous bytes of a row
+    const int ew = warp - kTcConvWarps, quad = warp & 3, lh = ew >> 2;
+    const int t0 = lane & 3, t1 = lane >> 2;
+    const int rowA = 32 * quad + 16 * lh + t1, rowB = rowA + 8;
     const int mt = b.M < kTcM ? b.M : kTcM;
     for (int i = 0; i < nt && !*abort_flag; ++i) {
       const int buf = i & 1;
@@ -295,24 +371,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
 #pragma unroll
       for (int q = 1; q < kGemmMaxBatch; ++q)
         if (e == q) C = b.C[q];
-      const uint32_t tbase = tmem + ((uint32_t)(32 * quad) << 16) + (uint32_t)(buf * 2 * kTcN + c0);
+      const uint32_t tbase = tmem + ((uint32_t)(32 * quad + 16 * lh) << 16) + (uint32_t)(buf * 2 * kTcN);
       uint32_t s0[16], s1[16];
-      tc_ld16(tbase, s0);           // hi*hi + lo*hi
-      tc_ld16(tbase + kTcN, s1);    // hi*lo
+      tc_ld16x256b_x4(tbase, s0);         // hi*hi + lo*hi
+      tc_ld16x256b_x4(tbase + kTcN, s1);  // hi*lo
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-      if (row < mt) {
-        double* out = C + (size_t)row * b.ldc + n0 + c0;
-        if (n0 + c0 + 16 <= b.N) {
 #pragma unroll
-          for (int j = 0; j < 16; j += 2)
-            *reinterpret_cast<double2*>(out + j) =
-                make_double2((double)__uint_as_float(s0[j]) + (double)__uint_as_float(s1[j]),
-                             (double)__uint_as_float(s0[j + 1]) + (double)__uint_as_float(s1[j + 1]));
-        } else {
+      for (int p = 0; p < 4; ++p) {
+        const int col = n0 + 8 * p + 2 * t0;  // even, and N is even: the pair is in range with its first entry
+        if (col < b.N) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j)
-            if (n0 + c0 + j < b.N) out[j] = (double)__uint_as_float(s0[j]) + (double)__uint_as_float(s1[j]);
+          for (int h = 0; h < 2; ++h) {
+            const int row = h ? rowB : rowA;
+            if (row >= mt) continue;
+            // FP32 sum of the two accumulators (the products are FP32-accurate)
+            const float x0 = __uint_as_float(s0[4 * p + 2 * h]) + __uint_as_float(s1[4 * p + 2 * h]);
+            const float x1 = __uint_as_float(s0[4 * p + 2 * h + 1]) + __uint_as_float(s1[4 * p + 2 * h + 1]);
+            if (b.c_f32)
+              *reinterpret_cast<float2*>(reinterpret_cast<float*>(C) + (size_t)row * b.ldc + col) =
+                  make_float2(x0, x1);
+            else
+              *reinterpret_cast<double2*>(C + (size_t)row * b.ldc + col) = make_double2((double)x0, (double)x1);
+          }
         }
       }
       if (b.M > kTcM && ew == 0 && n0 + lane < b.N) {
@@ -324,29 +405,50 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
       }
       tc_arrive(bar(4 + buf));
     }
-  } else if (warp == kTcIssuerWarp) {
+  } else {
     // ------------------------------------------------------------------- issuer
     if (lane == 0) {
-      int issued = 0;
-      tc_expect_tx(bar(6), (uint32_t)(2 * kTcASize));
-      tc_bulk_g2s(sAh, a_hi, (uint32_t)kTcASize, bar(6));
-      tc_bulk_g2s(sAl, a_lo, (uint32_t)kTcASize, bar(6));
-      if (!mbar_wait(bar(6), 0, spin)) {
-        fail_now();
-        // the operand copy may still be writing shared memory: let it land
-        if (!mbar_wait(bar(6), 0, kDrainPolls)) atomicOr(err, kErrWaitExpired);
-      }
+      int issued = 0, a_loads = 0, cur_op = -1;
       constexpr uint32_t lbo_a = kTcM * 16, lbo_b = kTcBRows * 16;
       const uint64_t dah = tc05_desc(tc_smem(sAh), lbo_a, 128), dal = tc05_desc(tc_smem(sAl), lbo_a, 128);
-      const uint64_t db = tc05_desc(tc_smem(sB), lbo_b, 128);
+      const uint64_t db0 = tc05_desc(tc_smem(sB0), lbo_b, 128);
+      const uint64_t db1 = tc05_desc(tc_smem(sB0 + kTcBSize), lbo_b, 128);
       for (int i = 0; i < nt && !*abort_flag; ++i) {
         const int buf = i & 1;
+        const int t = t_begin + i, e = t / tiles_n;
+        int op = b.op[0], K = b.K[0];
+#pragma unroll
+        for (int q = 1; q < kGemmMaxBatch; ++q)
+          if (e == q) {
+            op = b.op[q];
+            K = b.K[q];
+          }
+        if (op != cur_op) {
+          // the resident operator is read by every MMA issued so far: let them complete
+          if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, spin)) {
+            fail_now();
+            break;
+          }
+          tc_expect_tx(bar(6), (uint32_t)(2 * kTcASize));
+          tc_bulk_g2s(sAh, b.a_hi[op], (uint32_t)kTcASize, bar(6));
+          tc_bulk_g2s(sAl, b.a_lo[op], (uint32_t)kTcASize, bar(6));
+          ++a_loads;
+          if (!mbar_wait(bar(6), (a_loads - 1) & 1, spin)) {
+            fail_now();
+            // the operand copy may still be writing shared memory: let it land
+            if (!mbar_wait(bar(6), (a_loads - 1) & 1, kDrainPolls)) atomicOr(err, kErrWaitExpired);
+            break;
+          }
+          cur_op = op;
+        }
         if (!mbar_wait(bar(buf), (i >> 1) & 1, spin)) {
           fail_now();
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         const uint32_t acc = tmem + (uint32_t)(buf * 2 * kTcN);
+        const uint64_t db = buf ? db1 : db0;
+        const int ksteps = (K + 7) / 8;  // <= kTcKp / 8
         // K step s moves the start-address field (address / 16) by a constant
 #pragma unroll
         for (int s = 0; s < kTcKp / 8; ++s) {
@@ -363,26 +465,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
       // no MMA may still run when the CTA frees its tensor memory
       if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, kDrainPolls)) fail_now();
     }
-  } else {
-    // ----------------------------------------------------------------- producer
-    int loads = 0;
-    for (int i = 0; i < nt && !*abort_flag; ++i) {
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
-      const bool ok = i < 1 || mbar_wait(bar(8), (i - 1) & 1, spin);
-      if (!__all_sync(0xffffffffu, ok)) {
-        fail_now();
-        break;
-      }
-      if (lane == 0) {
-        tc_expect_tx(bar(7), (uint32_t)kTcStageBytes);
-        tc_tma_load_2d(stage, &b.map[e], n0, 0, bar(7));
-      }
-      ++loads;
-    }
-    // one staged load at most is in flight (the next is issued only after the
-    // converters read the previous one): wait for it before the CTA's shared
-    // memory is released (returns at once when every load was consumed)
-    if (lane == 0 && loads > 0 && !mbar_wait(bar(7), (loads - 1) & 1, kDrainPolls)) atomicOr(err, kErrWaitExpired);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
@@ -393,8 +475,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_dfield(const float* __re
 #endif
 }
 
-// Host: rows 0..M-1 of D (row-major, ld = ldd) split into TF32 hi / lo in the
-// core-matrix layout of a 128-row operand (rows >= M and K >= k zero).
+// Host: rows 0..M-1 of an operator (row-major, ld = ldd) split into TF32 hi /
+// lo in the core-matrix layout of a 128-row operand (rows >= M and K >= k zero).
 inline void tc05_pack_a(const double* D, int M, int K, int ldd, float (*tf32)(float), std::vector<float>& hi,
                         std::vector<float>& lo) {
   hi.assign(kTcASize / 4, 0.f);

@@ -51,12 +51,12 @@ EXPORTED = (
     "jsd_launches_first_step_extra", "jsd_autotune", "jsd_gemm_config",
     "jsd_set_gemm_config", "jsd_xmid_variant", "jsd_set_xmid_variant",
     "jsd_energy_runs", "jsd_set_batch_active", "jsd_batch_active",
-    "jsd_split_kernel", "jsd_set_split_kernel", "jsd_device_error",
+    "jsd_split_kernel", "jsd_set_split_kernel", "jsd_split_eig_in", "jsd_set_split_eig_in", "jsd_device_error",
     "jsd_set_coupling_term", "jsd_set_base_flow", "jsd_eig_kernel", "jsd_set_eig_kernel",
     "jsd_set_wait_limit", "jsd_wait_limit", "jsd_step_adjoint", "jsd_energy_grad",
 )
 
-ABI_VERSION = 4  # JSD_ABI_VERSION of include/jsd.h this binding is written for
+ABI_VERSION = 5  # JSD_ABI_VERSION of include/jsd.h this binding is written for
 
 # status codes (enum jsd_status)
 JSD_ERR_ARG, JSD_ERR_CUDA, JSD_ERR_NOMEM, JSD_ERR_STATE, JSD_ERR_NONFINITE = -1, -2, -3, -4, -5
@@ -120,6 +120,8 @@ def load(path: str = LIB_PATH):
     lib.jsd_energy_runs.argtypes = [vp, vp, vp, vp]
     lib.jsd_split_kernel.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_set_split_kernel.argtypes = [vp, ctypes.c_int]
+    lib.jsd_split_eig_in.argtypes = [vp]
+    lib.jsd_set_split_eig_in.argtypes = [vp, ctypes.c_int]
     lib.jsd_eig_kernel.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
     lib.jsd_set_eig_kernel.argtypes = [vp, ctypes.c_int, ctypes.c_int]
     lib.jsd_device_error.argtypes = [vp, vp]

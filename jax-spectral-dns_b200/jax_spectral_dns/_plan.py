@@ -159,6 +159,14 @@ class StepPlan:
     def set_split_kernel(self, kernel: int) -> None:
         _native.check(self.lib.jsd_set_split_kernel(self.handle, int(kernel)), "jsd_set_split_kernel")
 
+    def split_eig_in(self) -> int:
+        """1 when the mixed form's eigenbasis-in products of the nonlinear
+        terms run in split TF32, 0 when FP64-accurate, -1 for FP64 plans."""
+        return int(self.lib.jsd_split_eig_in(self.handle))
+
+    def set_split_eig_in(self, on: bool) -> None:
+        _native.check(self.lib.jsd_set_split_eig_in(self.handle, int(bool(on))), "jsd_set_split_eig_in")
+
     def eig_kernel(self, site: int):
         """(eigenbasis product kernel at GEMM site 1 or 2: 0 FP64 DMMA, 1 Ozaki
         int8 tensor cores; [autotune ms of the best DMMA tile and of Ozaki])."""

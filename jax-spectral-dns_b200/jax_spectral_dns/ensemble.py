@@ -192,11 +192,16 @@ class BatchedEnsemble:
                     continue
                 plan.set_batch_active(active)
                 view = buf[: 3 * ny * active * mx * mz].view(3, ny, active, mx, mz)
+                # the graphs' eager warm-up steps a copy of the view: give it
+                # the phase's own layout of valid states (its first runs)
+                view.copy_(init[:, :, :active])
                 full, rem = divmod(n_steps, chunk)
                 if full:
                     graphs.append((GraphedSteps(plan, view, dp, 0, chunk), full))
                 if rem:
                     graphs.append((GraphedSteps(plan, view, dp, 0, rem), 1))
+            buf.copy_(init.reshape(-1))
+            plan.check_device_errors()  # the warm-up steps ran on valid states
             self.groups.append({"idx": idx, "plan": plan, "init": init, "buf": buf, "dp": dp, "phases": phases,
                                 "dims": (ny, mx, mz), "final": torch.zeros_like(init)})
         torch.cuda.synchronize(self.device)

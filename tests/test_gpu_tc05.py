@@ -1,9 +1,13 @@
-"""Split-TF32 y-derivatives on tcgen05 (k_tc05_dfield) in the mixed form.
+"""Split-TF32 products on tcgen05 (k_tc05_split) in the mixed form: the
+y-derivatives, and the eigenbasis-in products of the nonlinear terms.
 
 The tcgen05 kernel (accumulator in tensor memory) must agree with the
 mma.sync split kernel to FP32-accumulation level and with the FP64 form to the
 mixed form's own level, for Ny <= 128 and for Ny = 129 (the y = -1 wall row
 in FP64 beside the 128-row tensor part); its bounded waits must never expire.
+Splitting the eigenbasis-in products (their inputs come out of FP32
+transforms and products) must leave the state at the same level as
+FP64-accurate products of the same terms.
 """
 import numpy as np
 import pytest
@@ -51,6 +55,28 @@ def test_tcgen05_split_kernel(cuda, shape):
     hv_b, hg_b = b.nonlinear_terms(st)
     assert rel(hv_a.cpu().numpy(), hv_b.cpu().numpy()) < 1e-5 and rel(hg_a.cpu().numpy(), hg_b.cpu().numpy()) < 1e-5
     a.check_device_errors()
+
+
+@pytest.mark.parametrize("shape", [(16, 65, 16), (16, 129, 16), (32, 97, 16)])
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_split_eigenbasis_in(cuda, shape, kernel):
+    """V^-1 D q, V^-1 H1, V^-1 h_g in split TF32 (the mixed default; two
+    operators in one tcgen05 launch) against FP64-accurate products."""
+    u0 = seeded_velocity_hat(shape, (LX, LZ), (6, 6), 1e-3, seed=12)
+    a = _plan(shape, "mixed")
+    a.set_split_kernel(kernel)
+    assert a.split_eig_in() == 1
+    out_split = _run(a, u0, 6)
+    a.check_device_errors()
+    b = _plan(shape, "mixed")
+    b.set_split_kernel(kernel)
+    b.set_split_eig_in(False)
+    assert b.split_eig_in() == 0
+    out_exact = _run(b, u0, 6)
+    out_64 = _run(_plan(shape, "fp64"), u0, 6)
+    assert rel(out_split, out_exact) < 1e-6
+    assert rel(out_split, out_64) < 1e-5
+    assert _plan(shape, "fp64").split_eig_in() == -1
 
 
 def test_autotune_picks_a_split_kernel(cuda):

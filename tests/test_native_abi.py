@@ -46,7 +46,7 @@ def test_binding_covers_header(lib):
 def test_abi_version_and_error_strings(lib):
     from jax_spectral_dns import _native
 
-    assert lib.jsd_abi_version() == _native.ABI_VERSION == 4
+    assert lib.jsd_abi_version() == _native.ABI_VERSION == 5
     assert isinstance(lib.jsd_last_error(), bytes)
 
 
