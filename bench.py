@@ -399,6 +399,18 @@ def run_ours(args):
                                            "entry in MEASURED_PEAKS.json)",
                             "cublas_same_shape_tflops": same_shape,
                             "traffic": _ncu_traffic("k_dgemm", head), "share_of_kernel_time": k["ms"] / total_k}
+            elif dom == "sgemm":
+                # split-TF32 products (y-derivatives, eigenbasis-in of the
+                # nonlinear terms): three TF32 tensor products per FP32-level
+                # product, against the dense TF32 rate (half the bf16 rate)
+                achieved = 3 * k["work"] / (k["ms"] / 1e3) / 1e12
+                tf32_peak = peaks["bf16_tflops"] / 2
+                roofline = {"kernel": "k_tc05_split (split-TF32 products on tcgen05)", "bound": "tensor",
+                            "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s (TF32)",
+                            "frac": achieved / tf32_peak,
+                            "peak_source": peak_src + " (MEASURED_PEAKS.json bf16_tflops / 2)",
+                            "traffic": _ncu_traffic("k_tc05_split", head),
+                            "share_of_kernel_time": k["ms"] / total_k}
             else:
                 achieved = k["work"] / (k["ms"] / 1e3) / 1e9
                 roofline = {"kernel": KERNEL_NAMES[dom], "bound": "hbm", "achieved": achieved,

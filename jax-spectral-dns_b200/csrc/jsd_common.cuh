@@ -74,6 +74,13 @@ __host__ __device__ __forceinline__ size_t sidx(const Geo& g, int y, int ix, int
   return ((size_t)y * g.mx + ix) * g.mz + iz;
 }
 
+// `bytes` (a multiple of 16) from a 16-byte aligned global address into L2
+__device__ __forceinline__ void l2_prefetch(const void* p, unsigned bytes) {
+#if defined(__CUDA_ARCH__)
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
+#endif
+}
+
 // Hermitian part of X at the signed mode (kx, kz): (X(k) + conj X(-k)) / 2.
 __host__ __device__ __forceinline__ double2 sym_at(const Geo& g, const double2* __restrict__ f, int y, int kx, int kz) {
   double2 a = f[sidx(g, y, mode_pos(kx, g.mx), mode_pos(kz, g.mz))];

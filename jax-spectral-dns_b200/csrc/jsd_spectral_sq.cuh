@@ -72,11 +72,23 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_zinv_sq(Geo g, const C* __res
   const int kx = act ? pair - y * K1 : 0;
   C tw[S - 1];
   sq_twiddles<S>(tw, twtab, ln.t);
+  // the group's two rows (kx and -kx) of field `i` into L2: the loads of a
+  // field then wait for L2, not DRAM (one field ahead; rows are 16-byte
+  // aligned and mz * 16 bytes long)
+  auto prefetch = [&](int i) {
+    if (act && ln.t == 0 && i < 6 * src.nsets) {
+      const double2* f = zinv_field(src, i);
+      l2_prefetch(f + sidx(g, y, kx, 0), (unsigned)(g.mz * sizeof(double2)));
+      if (kx) l2_prefetch(f + sidx(g, y, g.mx - kx, 0), (unsigned)(g.mz * sizeof(double2)));
+    }
+  };
+  prefetch(1);
 #pragma unroll 1
   for (int set = 0; set < src.nsets; ++set) {
 #pragma unroll 1
     for (int fi = 0; fi < 6; ++fi) {
       const double2* f = zinv_field(src, set * 6 + fi);
+      prefetch(set * 6 + fi + 2);
       C x[S], xz[S];
       // K < N / 2: positions below N / 2 hold kz >= 0 modes, those above kz < 0
 #pragma unroll
