@@ -541,6 +541,7 @@ int launch_ozaki(const jsd_plan* pc, const GemmBatch& b, cudaStream_t s) {
   o.N = b.N;
   o.ldb = b.ldb;
   o.ldc = b.ldc;
+  o.prefetch = (b.ldb % 2) == 0 ? 1 : 0;
   for (int i = 0; i < b.count; ++i) {
     const GemmEntry& g = b.e[i];
     int k = 0;
@@ -560,6 +561,7 @@ int launch_ozaki(const jsd_plan* pc, const GemmBatch& b, cudaStream_t s) {
     e.C = g.C;
     e.M = g.M;
     e.K = g.K;
+    if (reinterpret_cast<uintptr_t>(g.B) % 16) o.prefetch = 0;
   }
   const long long tiles = (long long)((o.N + kOzN - 1) / kOzN) * o.count;
   ProfScope ps(const_cast<jsd_plan*>(p), JSD_PROF_GEMM, gemm_flops(b), s);

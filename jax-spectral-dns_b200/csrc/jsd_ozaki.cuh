@@ -214,6 +214,7 @@ struct OzBatch {
   OzEntry e[kGemmMaxBatch];
   int count;
   int N, ldb, ldc;
+  int prefetch;  // every B is 16-byte aligned and ldb even: rows may be bulk-prefetched into L2
 };
 
 // one field of entry e by selects (a runtime index into the kernel parameter
@@ -357,6 +358,14 @@ __global__ void __launch_bounds__(kOzThreads, 1) k_oz8_gemm(const __grid_constan
           Kn = oz_K(b, en);
           Bn = oz_B(b, en);
         }
+      }
+      // the tile after the one just loaded into L2, so that its loads wait
+      // for L2 rather than DRAM: lane j < 8 prefetches row k0 + j (warp 0
+      // lane 8 row 128), its 256-byte segment or the part inside N
+      if (b.prefetch && en < b.count) {
+        const int cols = b.N - n0n < kOzN ? b.N - n0n : kOzN;  // even: N and n0n are
+        const int row = lane < kOzConvRows ? k0 + lane : (warp == 0 && lane == kOzConvRows ? kOzK : -1);
+        if (row >= 0 && row < Kn) l2_prefetch(Bn + (size_t)row * b.ldb + n0n, (unsigned)cols * 8u);
       }
     };
     if (nt > 0) load_next();
