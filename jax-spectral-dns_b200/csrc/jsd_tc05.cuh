@@ -66,9 +66,17 @@ constexpr int kTcConvWarps = kTcKp / 8, kTcEpiWarps = 8;
 constexpr int kTcIssuerWarp = kTcConvWarps + kTcEpiWarps;
 constexpr int kTcThreads = 32 * (kTcIssuerWarp + 1);  // 832
 constexpr int kTcSideDoubles = kTcConvWarps * kTcN;   // partial dots of the last row
-constexpr int kTcTmemCols = 2 * 2 * kTcN;             // two sets of (hi*hi + lo*hi, hi*lo)
+constexpr int kTcNB = 4;                               // operand buffers (tiles converted ahead of the MMAs)
+// tensor memory: two accumulator sets of (hi*hi + lo*hi, hi*lo) at columns 0
+// and 64, the operator's TF32 parts (A from tensor memory, lane = row, one K
+// element per column) at 128 and 288 (32-column aligned)
+constexpr int kTcTmemCols = 512;
+constexpr int kTcAccCols = 2 * kTcN;
+constexpr int kTcAHiCol = 2 * kTcAccCols, kTcALoCol = kTcAHiCol + 160;
+static_assert(kTcALoCol + kTcKp <= kTcTmemCols, "tensor-memory columns");
 constexpr int kTcMaxOps = 2;                          // operators per launch
-constexpr size_t kTcSmem = 2 * (size_t)kTcASize + 2 * (size_t)kTcBSize + 2 * sizeof(double) * kTcSideDoubles + 128;
+constexpr int kTcBars = 3 * kTcNB + 2 * 2 + 1;         // full, b free, side free; mma done, epilogue done; A ready
+constexpr size_t kTcSmem = kTcNB * (size_t)kTcBSize + kTcNB * sizeof(double) * kTcSideDoubles + 8 * kTcBars + 16;
 
 // B[i]: K[i] x N FP64 (row stride ldb), multiplied by operator op[i]; the
 // operator parts are packed by tc05_pack_a; xrow: the FP64 row 128 of
@@ -108,6 +116,22 @@ __device__ __forceinline__ uint64_t tc05_desc(uint32_t saddr, uint32_t lbo, uint
 // F32 accumulator, TF32 A and B, both K-major, M = 128, N as given
 __host__ __device__ constexpr uint32_t tc_idesc_tf32(int n) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kTcM >> 4) << 24);
+}
+
+// A from tensor memory (lane = row, column = K element), B from shared memory
+__device__ __forceinline__ void tc_mma_tf32_ts(uint32_t tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc,
+                                               uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(tmem),
+      "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc), "r"(0u));
+}
+
+// 32 TMEM lanes (the warp's quadrant) x 8 columns: thread = lane, 8 consecutive columns
+__device__ __forceinline__ void tc_st32x8(uint32_t taddr, const uint32_t* v) {
+  // (no memory clobber: tensor memory only, so global loads may move above it)
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};\n" ::"r"(taddr),
+               "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]));
 }
 
 __device__ __forceinline__ void tc_mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
@@ -222,25 +246,30 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
                                                               int* __restrict__ err, int spin) {
 #if defined(__CUDA_ARCH__)
   extern __shared__ __align__(1024) unsigned char tsm[];
-  unsigned char* sAh = tsm;
-  unsigned char* sAl = tsm + kTcASize;
-  unsigned char* sB0 = tsm + 2 * kTcASize;                      // two stacked hi / lo operands
-  double* side = reinterpret_cast<double*>(sB0 + 2 * kTcBSize);  // two tile buffers of partial dots
-  uint64_t* bars = reinterpret_cast<uint64_t*>(side + 2 * kTcSideDoubles);
-  // bars: 0,1 full (B operand + partial dots of tile parity); 2,3 mma done;
-  // 4,5 epilogue done; 6 A loaded
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 7);
+  unsigned char* sB0 = tsm;                                            // kTcNB stacked hi / lo operands
+  double* side = reinterpret_cast<double*>(sB0 + kTcNB * kTcBSize);    // kTcNB buffers of partial dots
+  uint64_t* bars = reinterpret_cast<uint64_t*>(side + kTcNB * kTcSideDoubles);
+  // bars: [0, NB) full (operand + dots of buffer b); [NB, 2NB) operand b read
+  // by its MMAs; [2NB, 3NB) dots b read by the epilogue; 3NB + s MMAs of
+  // accumulator set s done; 3NB + 2 + s epilogue of set s done; 3NB + 4 A in
+  // tensor memory
+  constexpr int kFull = 0, kBFree = kTcNB, kSFree = 2 * kTcNB, kMDone = 3 * kTcNB, kEDone = 3 * kTcNB + 2,
+                kAReady = 3 * kTcNB + 4;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kTcBars);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto bar = [&](int i) { return tc_smem(&bars[i]); };
   if (tid == 0) {
-    mbar_init(bar(0), 32 * kTcConvWarps);
-    mbar_init(bar(1), 32 * kTcConvWarps);
-    mbar_init(bar(2), 1);
-    mbar_init(bar(3), 1);
-    mbar_init(bar(4), 32 * kTcEpiWarps);
-    mbar_init(bar(5), 32 * kTcEpiWarps);
-    mbar_init(bar(6), 1);
+    for (int q = 0; q < kTcNB; ++q) {
+      mbar_init(bar(kFull + q), 32 * kTcConvWarps);
+      mbar_init(bar(kBFree + q), 1);
+      mbar_init(bar(kSFree + q), 32 * kTcEpiWarps / 2);
+    }
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(bar(kMDone + q), 1);
+      mbar_init(bar(kEDone + q), 32 * kTcEpiWarps / 2);
+    }
+    mbar_init(bar(kAReady), 32 * kTcEpiWarps / 2);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
@@ -263,6 +292,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
     *abort_flag = 1;
     atomicOr(err, kErrWaitExpired);
   };
+  // entry fields of tile i of this CTA by selects over the parameter arrays
+  auto entry_of = [&](int i) { return (t_begin + i) / tiles_n; };
+  auto op_of = [&](int e) {
+    int op = b.op[0];
+#pragma unroll
+    for (int q = 1; q < kGemmMaxBatch; ++q)
+      if (e == q) op = b.op[q];
+    return op;
+  };
+  auto k_of = [&](int e) {
+    int K = b.K[0];
+#pragma unroll
+    for (int q = 1; q < kGemmMaxBatch; ++q)
+      if (e == q) K = b.K[q];
+    return K;
+  };
 
   if (warp < kTcConvWarps) {
     // ---------------------------------------------------------------- converters
@@ -271,13 +316,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
     auto fetch = [&](int i, double(&x)[8]) {
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
       const double* B = b.B[0];
-      int K = b.K[0];
 #pragma unroll
       for (int q = 1; q < kGemmMaxBatch; ++q)
-        if (e == q) {
-          B = b.B[q];
-          K = b.K[q];
-        }
+        if (e == q) B = b.B[q];
+      const int K = k_of(e);
       const bool cv = n0 + n < b.N;
       const double* src = B + (size_t)k0 * b.ldb + n0 + n;
 #pragma unroll
@@ -289,35 +331,31 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
       if (!b.prefetch || lane >= 8) return;
       const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
       const double* B = b.B[0];
-      int K = b.K[0];
 #pragma unroll
       for (int q = 1; q < kGemmMaxBatch; ++q)
-        if (e == q) {
-          B = b.B[q];
-          K = b.K[q];
-        }
+        if (e == q) B = b.B[q];
+      const int K = k_of(e);
       const int cols = b.N - n0 < kTcN ? b.N - n0 : kTcN;  // even: N and n0 are
       if (k0 + lane < K) tc_prefetch_l2(B + (size_t)(k0 + lane) * b.ldb + n0, (uint32_t)cols * 8u);
     };
-    // tile i from registers x into operand buffer i % 2; then x takes the
-    // loads of tile i + 2 (from L2: prefetched a tile earlier), which land
-    // while tiles i and i + 1 are multiplied
+    // tile i from registers x into operand buffer i % NB; then x takes the
+    // loads of tile i + 2 (from L2: prefetched a tile earlier)
     auto body = [&](int i, double(&x)[8]) -> bool {
-      const int buf = i & 1;
+      const int bq = i % kTcNB;
       double dot = 0.0;
       if (b.M > kTcM) {
 #pragma unroll
         for (int j = 0; j < 8; ++j) dot = fma(__ldg(b.xrow + k0 + j), x[j], dot);  // xrow is zero padded
       }
-      // operand buffer `buf` is free once the MMAs of tile i - 2 completed, its
-      // partial dots once the epilogue of tile i - 2 is done
-      const bool ok = i < 2 || (mbar_wait(bar(2 + buf), ((i - 2) >> 1) & 1, spin) &&
-                                mbar_wait(bar(4 + buf), ((i - 2) >> 1) & 1, spin));
+      // buffer bq is free once the MMAs of tile i - NB read its operand and
+      // the epilogue of tile i - NB read its dots
+      const int ph = ((i / kTcNB) - 1) & 1;
+      const bool ok = i < kTcNB || (mbar_wait(bar(kBFree + bq), ph, spin) && mbar_wait(bar(kSFree + bq), ph, spin));
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         return false;
       }
-      unsigned char* sB = sB0 + buf * kTcBSize;
+      unsigned char* sB = sB0 + bq * kTcBSize;
       // one FP64 conversion per value: hi + lo keep 22 of the FP32 value's 24
       // bits, and f - hi is exact in FP32
 #pragma unroll
@@ -334,9 +372,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
         *reinterpret_cast<uint4*>(sB + tc05_offset(kTcBRows, kTcN + n, k0 + 4 * c)) =
             make_uint4(lo[0], lo[1], lo[2], lo[3]);
       }
-      side[buf * kTcSideDoubles + warp * kTcN + n] = dot;
+      side[bq * kTcSideDoubles + warp * kTcN + n] = dot;
       asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-      tc_arrive(bar(buf));
+      tc_arrive(bar(kFull + bq));
       if (i + 2 < nt) fetch(i + 2, x);
       if (i + 3 < nt) prefetch(i + 3);
       return true;
@@ -350,120 +388,160 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
     }
   } else if (warp < kTcConvWarps + kTcEpiWarps) {
     // ----------------------------------------------------------------- epilogue
-    // warp: TMEM lane quadrant warp % 4 (the lanes it may access), 16-lane
-    // half lh of it; tcgen05.ld 16x256b: thread (t0, t1) = (lane % 4, lane / 4)
-    // holds rows t1 and t1 + 8 of the half, columns 8p + 2 t0 and + 1 of
-    // repetition p, so a quad of threads stores 64 contiguous bytes of a row
-    const int ew = warp - kTcConvWarps, quad = warp & 3, lh = ew >> 2;
+    // two groups of 4 warps (one per TMEM lane quadrant, warp % 4), group g
+    // taking the tiles i with i % 2 = g (accumulator set g), so each group has
+    // two tile periods for its tile. tcgen05.ld 16x256b: thread (t0, t1) =
+    // (lane % 4, lane / 4) holds rows t1 and t1 + 8 of a 16-lane half,
+    // columns 8p + 2 t0 and + 1 of repetition p, so a quad of threads stores
+    // 64 contiguous bytes of a row. The group of the first tile of each
+    // operator also copies that operator's TF32 parts into tensor memory.
+    const int ew = warp - kTcConvWarps, quad = warp & 3, gq = ew >> 2;
     const int t0 = lane & 3, t1 = lane >> 2;
-    const int rowA = 32 * quad + 16 * lh + t1, rowB = rowA + 8;
     const int mt = b.M < kTcM ? b.M : kTcM;
-    for (int i = 0; i < nt && !*abort_flag; ++i) {
-      const int buf = i & 1;
-      const bool ok = mbar_wait(bar(2 + buf), (i >> 1) & 1, spin) && mbar_wait(bar(buf), (i >> 1) & 1, spin);
+    // columns [c_begin, c_end) (multiples of 8) of both TF32 parts of the
+    // operator into this warp's lane quadrant of tensor memory
+    auto load_a = [&](int op, int c_begin, int c_end) {
+      const int row = 32 * quad + lane;
+      const float* hi = (op ? b.a_hi[1] : b.a_hi[0]) + (size_t)row * kTcKp;
+      const float* lo = (op ? b.a_lo[1] : b.a_lo[0]) + (size_t)row * kTcKp;
+      const uint32_t lanes = (uint32_t)(32 * quad) << 16;
+#pragma unroll 3
+      for (int c = c_begin; c < c_end; c += 8) {
+        uint32_t v[8];
+        const float4 h0 = __ldg(reinterpret_cast<const float4*>(hi + c));
+        const float4 h1 = __ldg(reinterpret_cast<const float4*>(hi + c + 4));
+        v[0] = __float_as_uint(h0.x), v[1] = __float_as_uint(h0.y), v[2] = __float_as_uint(h0.z);
+        v[3] = __float_as_uint(h0.w), v[4] = __float_as_uint(h1.x), v[5] = __float_as_uint(h1.y);
+        v[6] = __float_as_uint(h1.z), v[7] = __float_as_uint(h1.w);
+        tc_st32x8(tmem + lanes + (uint32_t)(kTcAHiCol + c), v);
+        const float4 l0 = __ldg(reinterpret_cast<const float4*>(lo + c));
+        const float4 l1 = __ldg(reinterpret_cast<const float4*>(lo + c + 4));
+        v[0] = __float_as_uint(l0.x), v[1] = __float_as_uint(l0.y), v[2] = __float_as_uint(l0.z);
+        v[3] = __float_as_uint(l0.w), v[4] = __float_as_uint(l1.x), v[5] = __float_as_uint(l1.y);
+        v[6] = __float_as_uint(l1.z), v[7] = __float_as_uint(l1.w);
+        tc_st32x8(tmem + lanes + (uint32_t)(kTcALoCol + c), v);
+      }
+      asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+    };
+    constexpr int kASplit = 72;  // the two groups' halves of the first load (9 and 8 chunks of 8 columns)
+    if (nt > 0) {
+      load_a(op_of(entry_of(0)), gq ? kASplit : 0, gq ? kTcKp : kASplit);
+      asm volatile("bar.sync 1, %0;\n" ::"n"(32 * kTcEpiWarps) : "memory");  // both halves stored
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      if (gq == 0) tc_arrive(bar(kAReady));
+    }
+    for (int i = gq; i < nt && !*abort_flag; i += 2) {
+      const int e = entry_of(i), op = op_of(e);
+      if (i > 0 && op_of(entry_of(i - 1)) != op) {
+        // the previous operator is read by every MMA up to tile i - 1
+        const bool ok = mbar_wait(bar(kMDone + ((i - 1) & 1)), ((i - 1) >> 1) & 1, spin);
+        if (!__all_sync(0xffffffffu, ok)) {
+          fail_now();
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        load_a(op, 0, kTcKp);
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        tc_arrive(bar(kAReady));
+      }
+      const int set = i & 1, bq = i % kTcNB;
+      bool ok = mbar_wait(bar(kMDone + set), (i >> 1) & 1, spin);
+      if (ok && b.M > kTcM) ok = mbar_wait(bar(kFull + bq), (i / kTcNB) & 1, spin);  // the dots
       if (!__all_sync(0xffffffffu, ok)) {  // tcgen05.ld below needs the whole warp
         fail_now();
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      const int t = t_begin + i, e = t / tiles_n, n0 = (t - e * tiles_n) * kTcN;
+      const int n0 = (t_begin + i - e * tiles_n) * kTcN;
       double* C = b.C[0];
 #pragma unroll
       for (int q = 1; q < kGemmMaxBatch; ++q)
         if (e == q) C = b.C[q];
-      const uint32_t tbase = tmem + ((uint32_t)(32 * quad + 16 * lh) << 16) + (uint32_t)(buf * 2 * kTcN);
-      uint32_t s0[16], s1[16];
-      tc_ld16x256b_x4(tbase, s0);         // hi*hi + lo*hi
-      tc_ld16x256b_x4(tbase + kTcN, s1);  // hi*lo
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
 #pragma unroll
-      for (int p = 0; p < 4; ++p) {
-        const int col = n0 + 8 * p + 2 * t0;  // even, and N is even: the pair is in range with its first entry
-        if (col < b.N) {
+      for (int hv = 0; hv < 2; ++hv) {
+        const uint32_t tbase = tmem + ((uint32_t)(32 * quad + 16 * hv) << 16) + (uint32_t)(set * kTcAccCols);
+        uint32_t s0[16], s1[16];
+        tc_ld16x256b_x4(tbase, s0);         // hi*hi + lo*hi
+        tc_ld16x256b_x4(tbase + kTcN, s1);  // hi*lo
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        const int rowA = 32 * quad + 16 * hv + t1;
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const int row = h ? rowB : rowA;
-            if (row >= mt) continue;
-            // FP32 sum of the two accumulators (the products are FP32-accurate)
-            const float x0 = __uint_as_float(s0[4 * p + 2 * h]) + __uint_as_float(s1[4 * p + 2 * h]);
-            const float x1 = __uint_as_float(s0[4 * p + 2 * h + 1]) + __uint_as_float(s1[4 * p + 2 * h + 1]);
-            if (b.c_f32)
-              *reinterpret_cast<float2*>(reinterpret_cast<float*>(C) + (size_t)row * b.ldc + col) =
-                  make_float2(x0, x1);
-            else
-              *reinterpret_cast<double2*>(C + (size_t)row * b.ldc + col) = make_double2((double)x0, (double)x1);
+        for (int p = 0; p < 4; ++p) {
+          const int col = n0 + 8 * p + 2 * t0;  // even, and N is even: the pair is in range with its first entry
+          if (col < b.N) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const int row = rowA + 8 * h;
+              if (row >= mt) continue;
+              // FP32 sum of the two accumulators (the products are FP32-accurate)
+              const float x0 = __uint_as_float(s0[4 * p + 2 * h]) + __uint_as_float(s1[4 * p + 2 * h]);
+              const float x1 = __uint_as_float(s0[4 * p + 2 * h + 1]) + __uint_as_float(s1[4 * p + 2 * h + 1]);
+              if (b.c_f32)
+                *reinterpret_cast<float2*>(reinterpret_cast<float*>(C) + (size_t)row * b.ldc + col) =
+                    make_float2(x0, x1);
+              else
+                *reinterpret_cast<double2*>(C + (size_t)row * b.ldc + col) = make_double2((double)x0, (double)x1);
+            }
           }
         }
       }
-      if (b.M > kTcM && ew == 0 && n0 + lane < b.N) {
-        const double* sd = side + buf * kTcSideDoubles;
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      if (b.M > kTcM && quad == 0 && n0 + lane < b.N) {
+        const double* sd = side + bq * kTcSideDoubles;
         double x = sd[lane];
 #pragma unroll
         for (int w = 1; w < kTcConvWarps; ++w) x += sd[w * kTcN + lane];
         C[(size_t)kTcM * b.ldc + n0 + lane] = x;
       }
-      tc_arrive(bar(4 + buf));
+      tc_arrive(bar(kSFree + bq));
+      tc_arrive(bar(kEDone + set));
     }
   } else {
     // ------------------------------------------------------------------- issuer
     if (lane == 0) {
       int issued = 0, a_loads = 0, cur_op = -1;
-      constexpr uint32_t lbo_a = kTcM * 16, lbo_b = kTcBRows * 16;
-      const uint64_t dah = tc05_desc(tc_smem(sAh), lbo_a, 128), dal = tc05_desc(tc_smem(sAl), lbo_a, 128);
+      constexpr uint32_t lbo_b = kTcBRows * 16;
       const uint64_t db0 = tc05_desc(tc_smem(sB0), lbo_b, 128);
-      const uint64_t db1 = tc05_desc(tc_smem(sB0 + kTcBSize), lbo_b, 128);
       for (int i = 0; i < nt && !*abort_flag; ++i) {
-        const int buf = i & 1;
-        const int t = t_begin + i, e = t / tiles_n;
-        int op = b.op[0], K = b.K[0];
-#pragma unroll
-        for (int q = 1; q < kGemmMaxBatch; ++q)
-          if (e == q) {
-            op = b.op[q];
-            K = b.K[q];
-          }
-        if (op != cur_op) {
-          // the resident operator is read by every MMA issued so far: let them complete
-          if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, spin)) {
-            fail_now();
-            break;
-          }
-          tc_expect_tx(bar(6), (uint32_t)(2 * kTcASize));
-          tc_bulk_g2s(sAh, b.a_hi[op], (uint32_t)kTcASize, bar(6));
-          tc_bulk_g2s(sAl, b.a_lo[op], (uint32_t)kTcASize, bar(6));
+        const int set = i & 1, bq = i % kTcNB;
+        const int e = entry_of(i), op = op_of(e), K = k_of(e);
+        if (op != cur_op) {  // the epilogue group of tile i copies the operator into tensor memory
           ++a_loads;
-          if (!mbar_wait(bar(6), (a_loads - 1) & 1, spin)) {
+          if (!mbar_wait(bar(kAReady), (a_loads - 1) & 1, spin)) {
             fail_now();
-            // the operand copy may still be writing shared memory: let it land
-            if (!mbar_wait(bar(6), (a_loads - 1) & 1, kDrainPolls)) atomicOr(err, kErrWaitExpired);
             break;
           }
           cur_op = op;
         }
-        if (!mbar_wait(bar(buf), (i >> 1) & 1, spin)) {
+        if (!mbar_wait(bar(kFull + bq), (i / kTcNB) & 1, spin) ||
+            (i >= 2 && !mbar_wait(bar(kEDone + set), ((i - 2) >> 1) & 1, spin))) {
           fail_now();
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const uint32_t acc = tmem + (uint32_t)(buf * 2 * kTcN);
-        const uint64_t db = buf ? db1 : db0;
+        const uint32_t acc = tmem + (uint32_t)(set * kTcAccCols);
+        // operand buffer bq's descriptor: the start-address field moves by its offset / 16
+        const uint64_t db = db0 + (uint64_t)((bq * kTcBSize) >> 4);
         const int ksteps = (K + 7) / 8;  // <= kTcKp / 8
-        // K step s moves the start-address field (address / 16) by a constant
 #pragma unroll
         for (int s = 0; s < kTcKp / 8; ++s) {
           if (s >= ksteps) break;
-          const uint64_t oa = (2u * s * lbo_a) >> 4, ob = (2u * s * lbo_b) >> 4;
-          tc_mma_tf32(acc, dah + oa, db + ob, tc_idesc_tf32(2 * kTcN), s > 0 ? 1u : 0u);  // hi x [hi; lo]
-          tc_mma_tf32(acc, dal + oa, db + ob, tc_idesc_tf32(kTcN), 1u);                 // lo x hi
+          const uint64_t ob = (2u * s * lbo_b) >> 4;
+          tc_mma_tf32_ts(acc, tmem + (uint32_t)(kTcAHiCol + 8 * s), db + ob, tc_idesc_tf32(2 * kTcN),
+                         s > 0 ? 1u : 0u);                                                              // hi x [hi; lo]
+          tc_mma_tf32_ts(acc, tmem + (uint32_t)(kTcALoCol + 8 * s), db + ob, tc_idesc_tf32(kTcN), 1u);  // lo x hi
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                         bar(2 + buf))
+                         bar(kMDone + set))
+                     : "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         bar(kBFree + bq))
                      : "memory");
         issued = i + 1;
       }
       // no MMA may still run when the CTA frees its tensor memory
-      if (issued > 0 && !mbar_wait(bar(2 + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, kDrainPolls)) fail_now();
+      if (issued > 0 && !mbar_wait(bar(kMDone + ((issued - 1) & 1)), ((issued - 1) >> 1) & 1, kDrainPolls))
+        fail_now();
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -476,7 +554,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
 }
 
 // Host: rows 0..M-1 of an operator (row-major, ld = ldd) split into TF32 hi /
-// lo in the core-matrix layout of a 128-row operand (rows >= M and K >= k zero).
+// lo, 128 rows x kTcKp (rows >= M and K >= k zero), row-major: the layout the
+// kernel copies into tensor memory (lane = row).
 inline void tc05_pack_a(const double* D, int M, int K, int ldd, float (*tf32)(float), std::vector<float>& hi,
                         std::vector<float>& lo) {
   hi.assign(kTcASize / 4, 0.f);
@@ -485,7 +564,7 @@ inline void tc05_pack_a(const double* D, int M, int K, int ldd, float (*tf32)(fl
     for (int k = 0; k < K && k < kTcKp; ++k) {
       const double x = D[(size_t)r * ldd + k];
       const float h = tf32((float)x);
-      const int off = tc05_offset(kTcM, r, k) >> 2;
+      const int off = r * kTcKp + k;
       hi[off] = h;
       lo[off] = tf32((float)(x - (double)h));
     }
