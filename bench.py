@@ -83,7 +83,7 @@ def _peaks():
 
 
 # kernel class -> summary file stem under profiles/ (<stem>_channel_128x129x128.md)
-KERNEL_NAMES = {"gemm": "k_dgemm", "sgemm": "k_sgemm3", "zinv": "k_zinv_sq", "xmid": "k_xmid", "zfwd": "k_zfwd_sq",
+KERNEL_NAMES = {"gemm": "k_dgemm", "sgemm": "k_tc05_split", "zinv": "k_zinv_sq", "xmid": "k_xmid", "zfwd": "k_zfwd_sq",
                 "eigen": "k_eigen_update"}
 
 

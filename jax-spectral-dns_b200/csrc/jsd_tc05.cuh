@@ -12,26 +12,30 @@
 // 32-column tiles (entry-major):
 //   * warps 0-16 (converters, warp w = rows 8w..8w+7, lane = column): load the
 //     tile's values straight from global memory (coalesced 256-byte rows,
-//     rows past K_i and columns past N as zeros), one tile ahead: the loads of
-//     tile i + 1 are issued before tile i is stored, so they land while tile i
-//     is multiplied; split the values into TF32 hi and lo and store them as
-//     one 64-row K-major operand (hi rows 0-31, lo rows 32-63) in one of two
-//     operand buffers; for M = 129 they also form the FP64 dot products of
-//     the operator's last row with their rows;
-//   * warp 25 (issuer): keeps A_hi / A_lo of the current operator resident
-//     (bulk copy; reloaded when the entry's operator changes, after the MMAs
-//     issued so far completed), issues per K step of 8 two
-//     tcgen05.mma.kind::tf32 (M = 128): A_hi x [B_hi; B_lo] (N = 64: hi*hi
-//     into columns 0-31, hi*lo into 32-63) and A_lo x B_hi (N = 32, into
-//     columns 0-31), into one of two 64-column accumulator sets;
-//   * warps 17-24 (epilogue, TMEM lane quadrant = warp % 4, half of the
-//     columns each): read both accumulators (tcgen05.ld), add them in FP64 and
-//     store rows < min(M, 128); row 128 (M = 129) from the converters' dots.
-// Every mbarrier wait has an iteration limit (a kernel argument); on expiry the
+//     rows past K_i and columns past N as zeros) two tiles ahead in registers,
+//     with the tile after those brought into L2 by bulk prefetches; split the
+//     values into TF32 hi and lo and store them as one 64-row K-major operand
+//     (hi rows 0-31, lo rows 32-63) in one of four operand buffers; for
+//     M = 129 they also form the FP64 dot products of the operator's last row
+//     with their rows;
+//   * warp 25 (issuer): issues per K step of 8 two tcgen05.mma.kind::tf32
+//     (M = 128) with the operator from tensor memory: A_hi x [B_hi; B_lo]
+//     (N = 64: hi*hi into columns 0-31, hi*lo into 32-63) and A_lo x B_hi
+//     (N = 32, into columns 0-31), into one of two 64-column accumulator sets;
+//   * warps 17-24 (epilogue, two groups of four warps, one per TMEM lane
+//     quadrant; group g takes the tiles of accumulator set g): read both
+//     accumulators (tcgen05.ld 16x256b), add them in FP32 and store rows
+//     < min(M, 128) in FP64 or FP32; row 128 (M = 129) from the converters'
+//     dots. They also copy the operator's TF32 parts into tensor memory
+//     (tcgen05.st; lane = row, one K element per column): both groups for the
+//     first tile, and the group of the first tile of the second operator
+//     after the MMAs of the first have completed.
+// Every buffer hand-off has its own mbarrier, so no waiter can fall two phases
+// behind. Every wait has an iteration limit (a kernel argument); on expiry the
 // kernel raises the error flag, every role stops at its next tile, the issuer
-// waits (bounded) for its operand copy and its last MMAs, and the CTA frees
-// its TMEM and returns (the converters' loads go to registers: nothing of
-// theirs is in flight into shared memory).
+// waits (bounded) for its last MMAs, and the CTA frees its TMEM and returns
+// (the converters' loads go to registers and the operator copies are
+// synchronous: nothing else is in flight into shared or tensor memory).
 //
 // Canonical K-major layout without swizzle (units of 16 bytes = 4 TF32): a core
 // matrix is 8 rows x 16 bytes stored contiguously; core matrix (row group g,
@@ -187,15 +191,6 @@ __device__ __forceinline__ void tc_bulk_g2s(void* dst, const void* src, uint32_t
                    tc_smem(dst)),
                "l"(src), "r"(bytes), "r"(bar)
                : "memory");
-}
-
-// 2-D TMA load of the box at (x, y) (x: innermost, a multiple of 16 bytes)
-__device__ __forceinline__ void tc_tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
-          tc_smem(dst)),
-      "l"(map), "r"(x), "r"(y), "r"(bar)
-      : "memory");
 }
 
 __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
