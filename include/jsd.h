@@ -263,8 +263,10 @@ int jsd_set_split_kernel(jsd_plan* plan, int kernel);
 
 /* Eigenbasis-in products of the nonlinear terms (V^-1 D q, V^-1 H1,
  * V^-1 h_g) of a mixed-precision plan: 1 in split TF32 on the split kernel
- * (the default: the terms themselves come out of FP32 transforms and
- * products), 0 FP64-accurate (DMMA or int8 Ozaki, as jsd_eig_kernel says);
+ * (the default for the Navier-Stokes equations: the terms themselves come
+ * out of FP32 transforms and products), 0 FP64-accurate (DMMA or int8
+ * Ozaki, as jsd_eig_kernel says; the default with a base flow, whose
+ * coupling terms are part of these products);
  * -1 for FP64 plans. The state's own eigenbasis products (V^-1 v, V^-1
  * omega_y, V and D V back) stay FP64-accurate either way.
  * No counterpart in the reference. */

@@ -1581,7 +1581,12 @@ int jsd_plan_create(const jsd_desc* d, jsd_plan** out) {
       JSD_TRY(upload(p, &p->ei_hi[k], eh.data(), eh.size()));
       JSD_TRY(upload(p, &p->ei_lo[k], el.data(), el.size()));
     }
-    p->split_eig_in = ni <= Sgemm3Smem::BM;
+    // on by default for the Navier-Stokes equations; with a base flow
+    // (perturbation, dual) its coupling terms are part of these products, and
+    // over 2000 steps at 48 x 65 x 48 splitting them raised the mixed form's
+    // energy-history error against FP64 from 2e-7 to 1.2e-6, so such plans
+    // keep FP64-accurate products unless asked (jsd_set_split_eig_in)
+    p->split_eig_in = ni <= Sgemm3Smem::BM && d->kind == JSD_KIND_NS;
     if (ny <= kTcM + 1) {
       p->tc_rows = ny;
       std::vector<float> ahi, alo;

@@ -79,7 +79,7 @@ constexpr int kTcAccCols = 2 * kTcN;
 constexpr int kTcAHiCol = 2 * kTcAccCols, kTcALoCol = kTcAHiCol + 160;
 static_assert(kTcALoCol + kTcKp <= kTcTmemCols, "tensor-memory columns");
 constexpr int kTcMaxOps = 2;                          // operators per launch
-constexpr int kTcBars = 3 * kTcNB + 2 * 2 + 1;         // full, b free, side free; mma done, epilogue done; A ready
+constexpr int kTcBars = 2 * kTcNB + 2 * 2 + 1;         // full, buffer free; mma done, epilogue done; A ready
 constexpr size_t kTcSmem = kTcNB * (size_t)kTcBSize + kTcNB * sizeof(double) * kTcSideDoubles + 8 * kTcBars + 16;
 
 // B[i]: K[i] x N FP64 (row stride ldb), multiplied by operator op[i]; the
@@ -244,12 +244,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
   unsigned char* sB0 = tsm;                                            // kTcNB stacked hi / lo operands
   double* side = reinterpret_cast<double*>(sB0 + kTcNB * kTcBSize);    // kTcNB buffers of partial dots
   uint64_t* bars = reinterpret_cast<uint64_t*>(side + kTcNB * kTcSideDoubles);
-  // bars: [0, NB) full (operand + dots of buffer b); [NB, 2NB) operand b read
-  // by its MMAs; [2NB, 3NB) dots b read by the epilogue; 3NB + s MMAs of
-  // accumulator set s done; 3NB + 2 + s epilogue of set s done; 3NB + 4 A in
-  // tensor memory
-  constexpr int kFull = 0, kBFree = kTcNB, kSFree = 2 * kTcNB, kMDone = 3 * kTcNB, kEDone = 3 * kTcNB + 2,
-                kAReady = 3 * kTcNB + 4;
+  // bars: [0, NB) full (operand + dots of buffer b); [NB, 2NB) buffer b
+  // released by the epilogue of its tile (which waited for that tile's MMAs,
+  // so the operand has been read too); 2NB + s MMAs of accumulator set s
+  // done; 2NB + 2 + s epilogue of set s done; 2NB + 4 A in tensor memory
+  constexpr int kFull = 0, kSFree = kTcNB, kMDone = 2 * kTcNB, kEDone = 2 * kTcNB + 2, kAReady = 2 * kTcNB + 4;
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kTcBars);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tslot + 1);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -257,7 +256,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
   if (tid == 0) {
     for (int q = 0; q < kTcNB; ++q) {
       mbar_init(bar(kFull + q), 32 * kTcConvWarps);
-      mbar_init(bar(kBFree + q), 1);
       mbar_init(bar(kSFree + q), 32 * kTcEpiWarps / 2);
     }
     for (int q = 0; q < 2; ++q) {
@@ -342,10 +340,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
 #pragma unroll
         for (int j = 0; j < 8; ++j) dot = fma(__ldg(b.xrow + k0 + j), x[j], dot);  // xrow is zero padded
       }
-      // buffer bq is free once the MMAs of tile i - NB read its operand and
-      // the epilogue of tile i - NB read its dots
+      // buffer bq is free once the epilogue of tile i - NB is done with it: it
+      // read the dots, after the MMAs that read the operand had completed
       const int ph = ((i / kTcNB) - 1) & 1;
-      const bool ok = i < kTcNB || (mbar_wait(bar(kBFree + bq), ph, spin) && mbar_wait(bar(kSFree + bq), ph, spin));
+      const bool ok = i < kTcNB || mbar_wait(bar(kSFree + bq), ph, spin);
       if (!__all_sync(0xffffffffu, ok)) {
         fail_now();
         return false;
@@ -528,9 +526,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                          bar(kMDone + set))
-                     : "memory");
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                         bar(kBFree + bq))
                      : "memory");
         issued = i + 1;
       }

@@ -60,11 +60,14 @@ def test_tcgen05_split_kernel(cuda, shape):
 @pytest.mark.parametrize("shape", [(16, 65, 16), (16, 129, 16), (32, 97, 16)])
 @pytest.mark.parametrize("kernel", [0, 1])
 def test_split_eigenbasis_in(cuda, shape, kernel):
-    """V^-1 D q, V^-1 H1, V^-1 h_g in split TF32 (the mixed default; two
-    operators in one tcgen05 launch) against FP64-accurate products."""
+    """V^-1 D q, V^-1 H1, V^-1 h_g in split TF32 (two operators in one
+    tcgen05 launch; the mixed default without a base flow, selected here for a
+    perturbation plan) against FP64-accurate products."""
     u0 = seeded_velocity_hat(shape, (LX, LZ), (6, 6), 1e-3, seed=12)
     a = _plan(shape, "mixed")
     a.set_split_kernel(kernel)
+    assert a.split_eig_in() == 0  # the default with a base flow
+    a.set_split_eig_in(True)
     assert a.split_eig_in() == 1
     out_split = _run(a, u0, 6)
     a.check_device_errors()
