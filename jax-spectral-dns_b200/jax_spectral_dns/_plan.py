@@ -218,6 +218,62 @@ class StepPlan:
                                         ctypes.c_void_p(dpdx.data_ptr()), int(first_step), int(n_steps),
                                         _stream_ptr()), "jsd_step")
 
+    def step_host_stream(self, host_in, host_out, dpdx: torch.Tensor, first_step: int = 0, n_steps: int = 1):
+        """Advance host states: each pinned host_in[k] (reference layout
+        (3, Mx, Ny, Mz), complex128) by n_steps, the result into the pinned
+        host_out[k]. The host->device copy of state k + 1 and the device->host
+        copy of state k - 1 run on two copy streams (one per direction, so
+        they overlap each other too) while state k steps on the current stream
+        (two device buffers each way), so the transfers overlap the steps.
+        dpdx is shared and advanced by every state in turn.
+        Returns once everything is enqueued; the current stream waits for the
+        last copy."""
+        n = len(host_in)
+        assert len(host_out) == n
+        if n == 0:
+            return
+        dev = dpdx.device
+        main = torch.cuda.current_stream(dev)
+        if getattr(self, "_copy_streams", None) is None or self._copy_streams[0].device != dev:
+            self._copy_streams = (torch.cuda.Stream(device=dev), torch.cuda.Stream(device=dev))
+        copy, back = self._copy_streams
+        shape = tuple(host_in[0].shape)
+        din = [torch.empty(shape, dtype=torch.complex128, device=dev) for _ in range(2)]
+        dout = [torch.empty(shape, dtype=torch.complex128, device=dev) for _ in range(2)]
+        ev = {key: [torch.cuda.Event() for _ in range(2)] for key in ("loaded", "consumed", "computed", "drained")}
+        copy.wait_stream(main)  # the buffers were allocated on the current stream
+        back.wait_stream(main)
+
+        def load(k):
+            b = k % 2
+            with torch.cuda.stream(copy):
+                if k >= 2:
+                    copy.wait_event(ev["consumed"][b])  # state k - 2 has left din[b]
+                din[b].copy_(host_in[k], non_blocking=True)
+                ev["loaded"][b].record(copy)
+
+        load(0)
+        if n > 1:
+            load(1)
+        for k in range(n):
+            b = k % 2
+            main.wait_event(ev["loaded"][b])
+            st = din[b].transpose(-3, -2).contiguous()
+            ev["consumed"][b].record(main)
+            if k + 2 < n:
+                load(k + 2)
+            self.step(st, dpdx, first_step, n_steps)
+            if k >= 2:
+                main.wait_event(ev["drained"][b])  # state k - 2 has left dout[b]
+            dout[b].copy_(st.transpose(-3, -2))
+            ev["computed"][b].record(main)
+            with torch.cuda.stream(back):
+                back.wait_event(ev["computed"][b])
+                host_out[k].copy_(dout[b], non_blocking=True)
+                ev["drained"][b].record(back)
+        main.wait_stream(copy)
+        main.wait_stream(back)
+
     def step_trajectory(self, state: torch.Tensor, dpdx: torch.Tensor, first_step: int, n_steps: int
                         ) -> torch.Tensor:
         """Advance in place and return all states (n_steps + 1, 3, Ny, Mx, Mz)."""
