@@ -21,14 +21,14 @@ namespace jsd {
 
 constexpr int kSqWarps = 4;  // warps per block
 
-// Lane roles. With two groups per warp (11 <= S <= 16) each group takes its
-// own half-warp (lanes 16 gi + t, t < S): a 64-bit shared-memory request is
-// served per half-warp, so the groups' accesses never share a bank cycle.
-// Smaller S pack 32 / S groups of S consecutive lanes.
-template <int S>
+// Lane roles. HW: with two groups per warp (11 <= S <= 16) each group takes
+// its own half-warp (lanes 16 gi + t, t < S): a 64-bit shared-memory request
+// is served per half-warp, so the groups' accesses never share a bank cycle.
+// Otherwise 32 / S groups of S consecutive lanes, the last 32 - G S idle.
+template <int S, bool HW = true>
 struct SqLane {
-  static constexpr int G = 32 / S;                  // line groups per warp
-  static constexpr int W = G == 2 ? 16 : S;         // lane stride of the groups
+  static constexpr int G = 32 / S;                        // line groups per warp
+  static constexpr int W = (HW && G == 2) ? 16 : S;       // lane stride of the groups
   int warp, gi, t;
   bool live;  // lane belongs to a group (the other lanes idle)
   __device__ __forceinline__ SqLane() {
@@ -39,7 +39,7 @@ struct SqLane {
     live = gi < G && t < S;
     if (!live) {
       gi = 0;
-      t = 0;
+      if (HW) t = 0;
     }
   }
 };
@@ -62,8 +62,15 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_zinv_sq(Geo g, const C* __res
                                                            C* __restrict__ inter) {
   using Rl = typename real_of<C>::type;
   constexpr int N = S * S, XB = sq_xbuf<S>();
+  // The two forms keep their best measured shapes: FP32 lines on half-warp
+  // groups with the next field's rows prefetched into L2 and per-position
+  // bound tests resolved at compile time; FP64 lines on consecutive-lane
+  // groups with plain bound tests and no prefetch (the compiler then keeps
+  // all 2 S loads of a line in flight; with the FP32 shape the FP64 pass
+  // took 175 us instead of 109 us cold at 128 x 129 x 128).
+  constexpr bool F32 = sizeof(C) == sizeof(float2);
   extern __shared__ __align__(16) unsigned char sq_raw[];
-  const SqLane<S> ln;
+  const SqLane<S, F32> ln;
   C* xb = reinterpret_cast<C*>(sq_raw) + (ln.warp * SqLane<S>::G + ln.gi) * XB;
   const int K1 = g.kx_max + 1, K = g.kz_max;
   const int pair = (blockIdx.x * kSqWarps + ln.warp) * SqLane<S>::G + ln.gi;
@@ -76,7 +83,7 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_zinv_sq(Geo g, const C* __res
   // field then wait for L2, not DRAM (one field ahead; rows are 16-byte
   // aligned and mz * 16 bytes long)
   auto prefetch = [&](int i) {
-    if (act && ln.t == 0 && i < 6 * src.nsets) {
+    if (F32 && act && ln.t == 0 && i < 6 * src.nsets) {
       const double2* f = zinv_field(src, i);
       l2_prefetch(f + sidx(g, y, kx, 0), (unsigned)(g.mz * sizeof(double2)));
       if (kx) l2_prefetch(f + sidx(g, y, g.mx - kx, 0), (unsigned)(g.mz * sizeof(double2)));
@@ -94,7 +101,7 @@ __global__ void __launch_bounds__(kSqWarps * 32) k_zinv_sq(Geo g, const C* __res
 #pragma unroll
       for (int m = 0; m < S; ++m) {
         const int p = ln.t + S * m;
-        const bool below = S * m + S - 1 < N / 2, above = S * m >= N / 2;
+        const bool below = F32 && S * m + S - 1 < N / 2, above = F32 && S * m >= N / 2;
         const bool lo = !above && p <= K, hi = !below && p >= N - K;
         const int kz = below ? p : above ? p - N : lo ? p : p - N;
         const C v = (act && (lo || hi)) ? to_c<C>(sym_at(g, f, y, kx, kz)) : cmake<C>(0, 0);
