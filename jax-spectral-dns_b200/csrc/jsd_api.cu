@@ -1199,9 +1199,16 @@ int jsd_autotune(jsd_plan* plan, void* stream) {
       add_entry(b, plan->Dm, (const double*)plan->q, (double*)plan->Dfld, ny, ny);
       add_entry(b, plan->Dm, (const double*)plan->H1, (double*)(plan->Dfld + 2 * fs), ny, ny);
     } else if (site == kSiteEigIn) {
-      add_entry(b, plan->VinvD, (const double*)plan->q, plan->X1, ni, ny);
-      add_entry(b, plan->Vinv, (const double*)plan->H1 + rowd, plan->T, ni, ni);
-      add_entry(b, plan->Vinv, (const double*)plan->hg + rowd, plan->T + E, ni, ni);
+      const bool linear = plan->desc.linearise && plan->desc.kind != JSD_KIND_NS;
+      if (plan->split_eig_in && !linear) {
+        // the nonlinear terms go to the split kernel: what stays on this site
+        // is V^-1 omega_y at the first stage after a mass-flux correction
+        add_entry(b, plan->Vinv, (const double*)plan->H1 + rowd, plan->T + 3 * E, ni, ni);
+      } else {
+        add_entry(b, plan->VinvD, (const double*)plan->q, plan->X1, ni, ny);
+        add_entry(b, plan->Vinv, (const double*)plan->H1 + rowd, plan->T, ni, ni);
+        add_entry(b, plan->Vinv, (const double*)plan->hg + rowd, plan->T + E, ni, ni);
+      }
       max_m = ni;
     } else {
       add_entry(b, plan->Vfull, plan->vnt, (double*)plan->tmp, ny, ni);
