@@ -138,13 +138,6 @@ __device__ __forceinline__ void tc_st32x8(uint32_t taddr, const uint32_t* v) {
                "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]));
 }
 
-__device__ __forceinline__ void tc_mma_tf32(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u));
-}
-
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
 }
@@ -193,15 +186,6 @@ __device__ __forceinline__ void tc_bulk_g2s(void* dst, const void* src, uint32_t
                : "memory");
 }
 
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t* r) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-}
-
 // 16 TMEM lanes x 4 repetitions of 256 bits (8 columns): thread (lane % 4,
 // lane / 4) receives rows lane / 4 and lane / 4 + 8, columns 8 p + 2 (lane % 4)
 // and + 1 of repetition p, in registers 4 p + {0, 1} and 4 p + {2, 3}
@@ -218,11 +202,6 @@ __device__ __forceinline__ float tf32_round_dev(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
-}
-
-// `bytes` (a multiple of 16) from a 16-byte aligned global address into L2
-__device__ __forceinline__ void tc_prefetch_l2(const void* p, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(p), "r"(bytes) : "memory");
 }
 
 // *p when c, else 0; volatile, so a prefetch is issued where it stands and is
@@ -329,7 +308,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_tc05_split(const __grid_const
         if (e == q) B = b.B[q];
       const int K = k_of(e);
       const int cols = b.N - n0 < kTcN ? b.N - n0 : kTcN;  // even: N and n0 are
-      if (k0 + lane < K) tc_prefetch_l2(B + (size_t)(k0 + lane) * b.ldb + n0, (uint32_t)cols * 8u);
+      if (k0 + lane < K) l2_prefetch(B + (size_t)(k0 + lane) * b.ldb + n0, (unsigned)cols * 8u);
     };
     // tile i from registers x into operand buffer i % NB; then x takes the
     // loads of tile i + 2 (from L2: prefetched a tile earlier)
