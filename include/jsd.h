@@ -268,7 +268,8 @@ int jsd_set_split_kernel(jsd_plan* plan, int kernel);
  * Ozaki, as jsd_eig_kernel says; the default with a base flow, whose
  * coupling terms are part of these products);
  * -1 for FP64 plans. The state's own eigenbasis products (V^-1 v, V^-1
- * omega_y, V and D V back) stay FP64-accurate either way.
+ * omega_y, V and D V back) stay FP64-accurate either way, and so do the
+ * products of linearised terms (formed in FP64, not by FP32 transforms).
  * No counterpart in the reference. */
 int jsd_split_eig_in(const jsd_plan* plan);
 int jsd_set_split_eig_in(jsd_plan* plan, int on);
